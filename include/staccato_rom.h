@@ -1,0 +1,129 @@
+/*
+ * staccato_rom.h -- C ABI of the B200 reduced-order frequency sweep.
+ *
+ * The library replaces the ROM-projection and frequency-sweep bodies of STACCATO's
+ * Krylov-substructure class (src/analysis/KrylovROMSubstructure.{h,cpp}) and the batched
+ * sweeps of its GPU/CPU test programs.  Conventions follow the reference:
+ *   - complex numbers are interleaved {re, im} doubles, the layout of MKL_Complex16 /
+ *     STACCATOComplexDouble (src/tools/AuxiliaryParameters.h:52) and cuDoubleComplex;
+ *   - dense matrices are column-major (LAPACK_COL_MAJOR, KrylovROMSubstructure.cpp:1428);
+ *   - the caller owns every buffer; all pointers are device pointers unless named h_*;
+ *   - every call returns an int status (SROM_OK = 0) instead of exit(EXIT_FAILURE)
+ *     (the reference's error path, KrylovROMSubstructure.cpp:654-700);
+ *   - a handle binds one device and one stream and is not thread-safe; distinct handles are.
+ * No torch or CUDA types appear in the signatures; a CUDA stream is passed as void*.
+ */
+#ifndef STACCATO_ROM_H
+#define STACCATO_ROM_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SROM_API __attribute__((visibility("default")))
+#else
+#define SROM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct srom_handle srom_handle;
+
+/* Layout-compatible with MKL_Complex16 / STACCATOComplexDouble / cuDoubleComplex. */
+typedef struct {
+    double re, im;
+} srom_complex;
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define SROM_OK 0
+#define SROM_ERR_INVALID 1     /* bad argument (null pointer, size out of range, ...) */
+#define SROM_ERR_CUDA 2        /* a CUDA runtime call failed; see srom_last_error */
+#define SROM_ERR_ALLOC 3       /* device memory could not be obtained */
+#define SROM_ERR_TIMEOUT 4     /* a bounded device-side wait ran out */
+#define SROM_ERR_UNSUPPORTED 5 /* shape or option this build does not handle */
+
+/* ---- per-frequency info values (int per frequency) ------------------------------- */
+/*  0   solved;
+ *  k>0 U(k,k) is exactly zero (1-based column), as LAPACK zgetrf reports it
+ *      (the reference ignores this value, KrylovROMSubstructure.cpp:1428);
+ * -1   mixed-precision refinement did not reach the tolerance within max_refine steps
+ *      and SROM_FLAG_FALLBACK_FP64 was not set (the last iterate is returned).        */
+#define SROM_INFO_NOT_CONVERGED (-1)
+
+/* ---- precision of the factorisation ---------------------------------------------- */
+#define SROM_FP64 0        /* all-FP64 complex LU, bit-identical to the restated zgetrf */
+#define SROM_MIXED_FP32 1  /* complex FP32 LU + FP64 residual refinement               */
+#define SROM_MIXED_TF32 2  /* complex LU with 3xTF32 tensor-core trailing updates + FP64 refinement */
+
+/* ---- sweep flags ---------------------------------------------------------------------- */
+#define SROM_FLAG_FALLBACK_FP64 1 /* re-solve non-converged frequencies with the FP64 kernel */
+#define SROM_FLAG_KEEP_FACTORS 2  /* write LU factors + pivots into desc.LU / desc.ipiv (FP64) */
+
+/*
+ * One reduced-order model and its frequency request.  Mirrors the members the reference's
+ * sweep reads (myKComplexReduced, myMComplexReduced, myDComplexReduced, KrylovROMSubstructure.h:210-221)
+ * and the arguments of backTransformKMOR (frequency list, load matrix, number of load cases;
+ * KrylovROMSubstructure.h:156).
+ *   A(w) = (1 + i*eta) * K + (-w^2) * M + (i*w) * D          (D may be NULL)
+ * assembled per entry in the reference's zaxpy order (KrylovROMSubstructure.cpp:1411-1420).
+ */
+typedef struct {
+    int n;                  /* ROM order (rows of K)                                 */
+    int r;                  /* number of right-hand sides (load cases)               */
+    int F;                  /* number of frequencies                                 */
+    int ldk;                /* leading dimension of K, M, D (>= n)                   */
+    const srom_complex *K;  /* n x n                                                 */
+    const srom_complex *M;  /* n x n                                                 */
+    const srom_complex *D;  /* n x n or NULL                                         */
+    double eta;             /* hysteretic loss factor applied to K; 0 keeps K as is  */
+    const srom_complex *rhs;/* n x r, leading dimension ldb (= B_r * F)              */
+    int ldb;
+    const double *omega;    /* F angular frequencies (rad/s)                         */
+    srom_complex *X;        /* F blocks of n x r (ld n): x(w_f) = A(w_f)^-1 rhs      */
+    int *info;              /* F ints or NULL                                        */
+    int *steps;             /* F ints or NULL: refinement steps taken (-1: FP64 fallback) */
+    double *berr;           /* F doubles or NULL: final normwise backward error      */
+    srom_complex *LU;       /* F blocks of n x n or NULL (SROM_FLAG_KEEP_FACTORS)    */
+    int *ipiv;              /* F blocks of n ints (1-based) or NULL                  */
+} srom_rom_desc;
+
+typedef struct {
+    int precision;   /* SROM_FP64 / SROM_MIXED_FP32 / SROM_MIXED_TF32                */
+    int max_refine;  /* refinement steps for the mixed forms (default 5 when <= 0)   */
+    double tol;      /* stop when ||r||_inf <= tol * ||A||_inf * ||x||_inf; 0 = sqrt(n)*eps (LAPACK zcgesv) */
+    int flags;       /* SROM_FLAG_*                                                  */
+} srom_sweep_opts;
+
+/* ---- handle -------------------------------------------------------------------------- */
+SROM_API int srom_create(srom_handle **h, int device);
+SROM_API int srom_destroy(srom_handle *h);
+SROM_API int srom_set_stream(srom_handle *h, void *cuda_stream);
+SROM_API const char *srom_status_string(int status);
+SROM_API const char *srom_last_error(const srom_handle *h);
+SROM_API int srom_version(void);
+
+/*
+ * Frequency sweep over one or many ROMs in one call: for every (ROM, frequency) pair
+ * assemble A(w), factor it with partial pivoting and solve for all r right-hand sides.
+ * Replaces the hot loop of backTransformKMOR (KrylovROMSubstructure.cpp:1403-1453), the
+ * dense CPU sweep of srcPerformanceTest/main.cpp:359-404 and the cuBLAS/cuSOLVER sweeps of
+ * test/krylovTestGPU/matrixInSingleLoop/gpu/src/main.cu:236-387 and
+ * test/krylovMidsizeTest/gpu/concurrent/batchedLU/src/main.cu:209-268 (which do not pivot).
+ * All descriptor pointers are device pointers.  Asynchronous on the handle's stream.
+ */
+SROM_API int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts);
+
+/*
+ * Same sweep with HOST buffers in every pointer of the descriptors (K, M, D, rhs, omega
+ * in; X, info, steps, berr out).  Copies in, sweeps and copies out on the handle's stream,
+ * then synchronises.  This is the drop-in form of backTransformKMOR, whose data live in
+ * host std::vectors (KrylovROMSubstructure.h:210-221).
+ */
+SROM_API int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STACCATO_ROM_H */

@@ -1,0 +1,125 @@
+"""ctypes binding of ``libstaccato_rom.so`` (the C ABI in include/staccato_rom.h).
+
+The library is built in-tree by ``staccato_b200/build.py``.  There is no fallback: if the
+shared object is missing or cannot be loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libstaccato_rom.so")
+
+SROM_OK = 0
+SROM_ERR_INVALID = 1
+SROM_ERR_CUDA = 2
+SROM_ERR_ALLOC = 3
+SROM_ERR_TIMEOUT = 4
+SROM_ERR_UNSUPPORTED = 5
+
+SROM_FP64 = 0
+SROM_MIXED_FP32 = 1
+SROM_MIXED_TF32 = 2
+
+SROM_FLAG_FALLBACK_FP64 = 1
+SROM_FLAG_KEEP_FACTORS = 2
+
+SROM_INFO_NOT_CONVERGED = -1
+
+#: every symbol include/staccato_rom.h declares (checked by the CPU test-suite)
+EXPORTS = [
+    "srom_create", "srom_destroy", "srom_set_stream", "srom_status_string", "srom_last_error",
+    "srom_version", "srom_sweep", "srom_sweep_host",
+]
+
+
+class RomDesc(C.Structure):
+    _fields_ = [
+        ("n", C.c_int), ("r", C.c_int), ("F", C.c_int), ("ldk", C.c_int),
+        ("K", C.c_void_p), ("M", C.c_void_p), ("D", C.c_void_p),
+        ("eta", C.c_double),
+        ("rhs", C.c_void_p), ("ldb", C.c_int),
+        ("omega", C.c_void_p),
+        ("X", C.c_void_p), ("info", C.c_void_p), ("steps", C.c_void_p), ("berr", C.c_void_p),
+        ("LU", C.c_void_p), ("ipiv", C.c_void_p),
+    ]
+
+
+class SweepOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("max_refine", C.c_int), ("tol", C.c_double),
+                ("flags", C.c_int)]
+
+
+class SromError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"srom status {status}: {msg}")
+        self.status = status
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: run staccato_b200/build.py (or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        vp, i, pp = C.c_void_p, C.c_int, C.POINTER(C.c_void_p)
+        L.srom_create.argtypes = [pp, i]
+        L.srom_create.restype = i
+        L.srom_destroy.argtypes = [vp]
+        L.srom_destroy.restype = i
+        L.srom_set_stream.argtypes = [vp, vp]
+        L.srom_set_stream.restype = i
+        L.srom_status_string.argtypes = [i]
+        L.srom_status_string.restype = C.c_char_p
+        L.srom_last_error.argtypes = [vp]
+        L.srom_last_error.restype = C.c_char_p
+        L.srom_version.restype = i
+        for name in ("srom_sweep", "srom_sweep_host"):
+            fn = getattr(L, name)
+            fn.argtypes = [vp, C.POINTER(RomDesc), i, C.POINTER(SweepOpts)]
+            fn.restype = i
+        _lib = L
+    return _lib
+
+
+def check(handle, status: int) -> None:
+    if status != SROM_OK:
+        L = lib()
+        msg = L.srom_last_error(handle) if handle else None
+        txt = (msg.decode() if msg else "") or L.srom_status_string(status).decode()
+        raise SromError(status, txt)
+
+
+class Handle:
+    """Owns one ``srom_handle`` bound to a device (and optionally a CUDA stream)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        st = lib().srom_create(C.byref(self._h), device)
+        if st != SROM_OK:
+            raise SromError(st, f"srom_create(device={device}) failed")
+        self.device = device
+
+    @property
+    def ptr(self):
+        return self._h
+
+    def set_stream(self, stream_ptr: int) -> None:
+        check(self._h, lib().srom_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def close(self) -> None:
+        if self._h:
+            lib().srom_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass

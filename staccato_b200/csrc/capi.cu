@@ -1,0 +1,392 @@
+// C ABI of the B200 frequency sweep (declarations in include/staccato_rom.h).
+//
+// Host responsibilities: argument validation, turning the ROM descriptors into one flat,
+// cost-sorted list of (ROM, frequency) systems, staging that list to the device, sizing
+// scratch memory and launching the persistent kernels on the handle's stream.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/staccato_rom.h"
+#include "srom_device.cuh"
+#include "sweep_kernels.h"
+
+using srom::Item;
+using srom::RomDev;
+
+struct srom_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    int max_smem_optin = 0;
+    // per-CTA scratch for the global-storage kernels
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    // descriptor + work-list staging
+    void *d_meta = nullptr;
+    size_t d_meta_bytes = 0;
+    void *h_meta = nullptr;
+    size_t h_meta_bytes = 0;
+    cudaEvent_t meta_done = nullptr;
+    bool meta_pending = false;
+    // device buffers used by srom_sweep_host
+    void *d_host_arena = nullptr;
+    size_t d_host_arena_bytes = 0;
+    std::string err;
+};
+
+namespace {
+
+int set_err(srom_handle *h, int code, const char *fmt, ...) {
+    if (h) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        h->err = buf;
+    }
+    return code;
+}
+
+#define SROM_CUDA(h, call)                                                                  \
+    do {                                                                                    \
+        cudaError_t _e = (call);                                                            \
+        if (_e != cudaSuccess)                                                              \
+            return set_err((h), SROM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(_e)); \
+    } while (0)
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int ensure_device_buffer(srom_handle *h, void **ptr, size_t *have, size_t need) {
+    if (*have >= need) return SROM_OK;
+    if (*ptr) {
+        // The previous buffer may still be read by queued work on the handle's stream.
+        SROM_CUDA(h, cudaStreamSynchronize(h->stream));
+        SROM_CUDA(h, cudaFree(*ptr));
+        *ptr = nullptr;
+        *have = 0;
+    }
+    size_t sz = std::max(need, (size_t)(*have * 5 / 4));
+    cudaError_t e = cudaMalloc(ptr, sz);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        cudaGetLastError();
+        return set_err(h, SROM_ERR_ALLOC, "cudaMalloc(%zu) failed: %s", sz, cudaGetErrorString(e));
+    }
+    *have = sz;
+    return SROM_OK;
+}
+
+int ensure_host_pinned(srom_handle *h, size_t need) {
+    if (h->h_meta_bytes >= need) return SROM_OK;
+    if (h->meta_pending) {
+        SROM_CUDA(h, cudaEventSynchronize(h->meta_done));
+        h->meta_pending = false;
+    }
+    if (h->h_meta) SROM_CUDA(h, cudaFreeHost(h->h_meta));
+    h->h_meta = nullptr;
+    size_t sz = std::max(need, h->h_meta_bytes * 2);
+    SROM_CUDA(h, cudaMallocHost(&h->h_meta, sz));
+    h->h_meta_bytes = sz;
+    return SROM_OK;
+}
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int validate_desc(srom_handle *h, const srom_rom_desc &d, int idx) {
+    if (d.n < 0 || d.r < 0 || d.F < 0) return set_err(h, SROM_ERR_INVALID, "rom %d: negative size", idx);
+    if (d.n == 0 || d.F == 0 || d.r == 0) return SROM_OK;
+    if (!d.K || !d.M || !d.rhs || !d.omega || !d.X)
+        return set_err(h, SROM_ERR_INVALID, "rom %d: K, M, rhs, omega and X must be non-null", idx);
+    if (d.ldk < d.n) return set_err(h, SROM_ERR_INVALID, "rom %d: ldk (%d) < n (%d)", idx, d.ldk, d.n);
+    if (d.ldb < d.n) return set_err(h, SROM_ERR_INVALID, "rom %d: ldb (%d) < n (%d)", idx, d.ldb, d.n);
+    if ((d.LU == nullptr) != (d.ipiv == nullptr))
+        return set_err(h, SROM_ERR_INVALID, "rom %d: LU and ipiv must be given together", idx);
+    return SROM_OK;
+}
+
+RomDev to_dev(const srom_rom_desc &d) {
+    RomDev r;
+    r.n = d.n;
+    r.r = d.r;
+    r.F = d.F;
+    r.ldk = d.ldk;
+    r.K = reinterpret_cast<const double2 *>(d.K);
+    r.M = reinterpret_cast<const double2 *>(d.M);
+    r.D = reinterpret_cast<const double2 *>(d.D);
+    r.eta = d.eta;
+    r.rhs = reinterpret_cast<const double2 *>(d.rhs);
+    r.ldb = d.ldb;
+    r.omega = d.omega;
+    r.X = reinterpret_cast<double2 *>(d.X);
+    r.info = d.info;
+    r.steps = d.steps;
+    r.berr = d.berr;
+    r.LU = reinterpret_cast<double2 *>(d.LU);
+    r.ipiv = d.ipiv;
+    return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+int srom_version(void) { return 100; }
+
+const char *srom_status_string(int s) {
+    switch (s) {
+        case SROM_OK: return "ok";
+        case SROM_ERR_INVALID: return "invalid argument";
+        case SROM_ERR_CUDA: return "CUDA error";
+        case SROM_ERR_ALLOC: return "device allocation failed";
+        case SROM_ERR_TIMEOUT: return "device wait timed out";
+        case SROM_ERR_UNSUPPORTED: return "unsupported shape or option";
+        default: return "unknown status";
+    }
+}
+
+const char *srom_last_error(const srom_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int srom_create(srom_handle **out, int device) {
+    if (!out) return SROM_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return SROM_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) return SROM_ERR_INVALID;
+    srom_handle *h = new srom_handle();
+    h->device = device;
+    DeviceGuard g(device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete h;
+        return SROM_ERR_CUDA;
+    }
+    h->sm_count = prop.multiProcessorCount;
+    h->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
+    if (cudaEventCreateWithFlags(&h->meta_done, cudaEventDisableTiming) != cudaSuccess) {
+        delete h;
+        return SROM_ERR_CUDA;
+    }
+    *out = h;
+    return SROM_OK;
+}
+
+int srom_destroy(srom_handle *h) {
+    if (!h) return SROM_OK;
+    DeviceGuard g(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    else cudaDeviceSynchronize();
+    if (h->scratch) cudaFree(h->scratch);
+    if (h->d_meta) cudaFree(h->d_meta);
+    if (h->d_host_arena) cudaFree(h->d_host_arena);
+    if (h->h_meta) cudaFreeHost(h->h_meta);
+    if (h->meta_done) cudaEventDestroy(h->meta_done);
+    delete h;
+    return SROM_OK;
+}
+
+int srom_set_stream(srom_handle *h, void *stream) {
+    if (!h) return SROM_ERR_INVALID;
+    h->stream = reinterpret_cast<cudaStream_t>(stream);
+    return SROM_OK;
+}
+
+int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    if (n_roms < 0 || (n_roms > 0 && !roms)) return set_err(h, SROM_ERR_INVALID, "roms is null");
+    srom_sweep_opts o = opts ? *opts : srom_sweep_opts{SROM_FP64, 5, 0.0, 0};
+    if (o.precision != SROM_FP64)
+        return set_err(h, SROM_ERR_UNSUPPORTED, "precision %d not available in this build", o.precision);
+    for (int i = 0; i < n_roms; ++i) {
+        int s = validate_desc(h, roms[i], i);
+        if (s) return s;
+    }
+    DeviceGuard g(h->device);
+
+    // ---- classify and order the work ---------------------------------------------------
+    const size_t smem_cap = (size_t)h->max_smem_optin;
+    std::vector<RomDev> dev(n_roms);
+    std::vector<int> cls(n_roms, -1);  // 0 smem, 1 global
+    size_t smem_max = 0;
+    int g_nmax = 0, g_rmax = 0;
+    long long n_items[2] = {0, 0};
+    for (int i = 0; i < n_roms; ++i) {
+        dev[i] = to_dev(roms[i]);
+        const srom_rom_desc &d = roms[i];
+        if (d.n == 0 || d.F == 0 || d.r == 0) continue;
+        size_t s = srom::fp64_smem_bytes(d.n, d.r);
+        if (s <= smem_cap) {
+            cls[i] = 0;
+            smem_max = std::max(smem_max, s);
+        } else {
+            cls[i] = 1;
+            g_nmax = std::max(g_nmax, d.n);
+            g_rmax = std::max(g_rmax, d.r);
+        }
+        n_items[cls[i]] += d.F;
+    }
+    if (g_nmax > 0 && srom::fp64_global_smem_bytes(g_nmax, g_rmax) > smem_cap)
+        return set_err(h, SROM_ERR_UNSUPPORTED, "n=%d with r=%d exceeds the shared-memory panel budget",
+                       g_nmax, g_rmax);
+    if (n_items[0] + n_items[1] > INT32_MAX) return set_err(h, SROM_ERR_UNSUPPORTED, "too many systems");
+
+    std::vector<int> order(n_roms);
+    for (int i = 0; i < n_roms; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return roms[a].n > roms[b].n; });
+
+    // ---- stage descriptors + work lists ---------------------------------------------------
+    const size_t off_items0 = align_up(sizeof(RomDev) * std::max(n_roms, 1), 256);
+    const size_t off_items1 = off_items0 + align_up(sizeof(Item) * (size_t)n_items[0] + 1, 256);
+    const size_t off_ctr = off_items1 + align_up(sizeof(Item) * (size_t)n_items[1] + 1, 256);
+    const size_t meta_bytes = off_ctr + 256;
+    int s = ensure_host_pinned(h, meta_bytes);
+    if (s) return s;
+    if (h->meta_pending) {
+        SROM_CUDA(h, cudaEventSynchronize(h->meta_done));
+        h->meta_pending = false;
+    }
+    s = ensure_device_buffer(h, &h->d_meta, &h->d_meta_bytes, meta_bytes);
+    if (s) return s;
+    char *hm = static_cast<char *>(h->h_meta);
+    if (n_roms) memcpy(hm, dev.data(), sizeof(RomDev) * n_roms);
+    Item *it0 = reinterpret_cast<Item *>(hm + off_items0);
+    Item *it1 = reinterpret_cast<Item *>(hm + off_items1);
+    long long k0 = 0, k1 = 0;
+    for (int oi = 0; oi < n_roms; ++oi) {
+        const int i = order[oi];
+        if (cls[i] < 0) continue;
+        Item *dst = cls[i] == 0 ? it0 : it1;
+        long long &k = cls[i] == 0 ? k0 : k1;
+        for (int f = 0; f < roms[i].F; ++f) dst[k++] = Item{i, f};
+    }
+    int *ctr = reinterpret_cast<int *>(hm + off_ctr);
+    ctr[0] = 0;
+    ctr[1] = 0;
+    SROM_CUDA(h, cudaMemcpyAsync(h->d_meta, h->h_meta, meta_bytes, cudaMemcpyHostToDevice, h->stream));
+    SROM_CUDA(h, cudaEventRecord(h->meta_done, h->stream));
+    h->meta_pending = true;
+    char *dm = static_cast<char *>(h->d_meta);
+    const RomDev *d_roms = reinterpret_cast<const RomDev *>(dm);
+    const Item *d_it0 = reinterpret_cast<const Item *>(dm + off_items0);
+    const Item *d_it1 = reinterpret_cast<const Item *>(dm + off_items1);
+    int *d_ctr = reinterpret_cast<int *>(dm + off_ctr);
+
+    // ---- launches ------------------------------------------------------------------------
+    if (n_items[0] > 0) {
+        int bps = srom::fp64_smem_blocks_per_sm(smem_max);
+        if (bps <= 0) return set_err(h, SROM_ERR_UNSUPPORTED, "smem kernel cannot be resident (%zu B)", smem_max);
+        long long grid = std::min<long long>(n_items[0], (long long)bps * h->sm_count);
+        SROM_CUDA(h, srom::launch_fp64_smem(d_roms, d_it0, (int)n_items[0], d_ctr, smem_max, (int)grid, h->stream));
+    }
+    if (n_items[1] > 0) {
+        long long grid = std::min<long long>(n_items[1], h->sm_count);
+        bool all_keep = true;
+        for (int i = 0; i < n_roms; ++i)
+            if (cls[i] == 1 && !roms[i].LU) all_keep = false;
+        const int64_t slot = (int64_t)g_nmax * g_nmax;
+        double2 *scr = nullptr;
+        if (!all_keep) {
+            s = ensure_device_buffer(h, &h->scratch, &h->scratch_bytes, sizeof(double2) * (size_t)slot * grid);
+            if (s) return s;
+            scr = static_cast<double2 *>(h->scratch);
+        }
+        SROM_CUDA(h, srom::launch_fp64_global(d_roms, d_it1, (int)n_items[1], d_ctr + 1, scr, slot, g_nmax,
+                                              g_rmax, (int)grid, h->stream));
+    }
+    return SROM_OK;
+}
+
+int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    if (n_roms < 0 || (n_roms > 0 && !roms)) return set_err(h, SROM_ERR_INVALID, "roms is null");
+    for (int i = 0; i < n_roms; ++i) {
+        int s = validate_desc(h, roms[i], i);
+        if (s) return s;
+    }
+    DeviceGuard g(h->device);
+    // Lay out every input and output of every ROM in one device arena.
+    std::vector<size_t> offs(n_roms * 10, 0);
+    size_t total = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = total;
+        total = align_up(total + bytes, 256);
+        return o;
+    };
+    for (int i = 0; i < n_roms; ++i) {
+        const srom_rom_desc &d = roms[i];
+        if (d.n == 0 || d.F == 0 || d.r == 0) continue;
+        const size_t nn = (size_t)d.ldk * d.n, cz = sizeof(srom_complex);
+        size_t *o = &offs[i * 10];
+        o[0] = take(cz * nn);
+        o[1] = take(cz * nn);
+        o[2] = d.D ? take(cz * nn) : 0;
+        o[3] = take(cz * (size_t)d.ldb * d.r);
+        o[4] = take(sizeof(double) * d.F);
+        o[5] = take(cz * (size_t)d.F * d.n * d.r);
+        o[6] = d.info ? take(sizeof(int) * d.F) : 0;
+        o[7] = d.steps ? take(sizeof(int) * d.F) : 0;
+        o[8] = d.berr ? take(sizeof(double) * d.F) : 0;
+    }
+    int s = ensure_device_buffer(h, &h->d_host_arena, &h->d_host_arena_bytes, std::max<size_t>(total, 256));
+    if (s) return s;
+    char *base = static_cast<char *>(h->d_host_arena);
+    std::vector<srom_rom_desc> dd(roms, roms + n_roms);
+    const cudaMemcpyKind H2D = cudaMemcpyHostToDevice, D2H = cudaMemcpyDeviceToHost;
+    for (int i = 0; i < n_roms; ++i) {
+        const srom_rom_desc &d = roms[i];
+        if (d.n == 0 || d.F == 0 || d.r == 0) continue;
+        const size_t nn = (size_t)d.ldk * d.n, cz = sizeof(srom_complex);
+        size_t *o = &offs[i * 10];
+        srom_rom_desc &e = dd[i];
+        e.K = reinterpret_cast<const srom_complex *>(base + o[0]);
+        e.M = reinterpret_cast<const srom_complex *>(base + o[1]);
+        e.D = d.D ? reinterpret_cast<const srom_complex *>(base + o[2]) : nullptr;
+        e.rhs = reinterpret_cast<const srom_complex *>(base + o[3]);
+        e.omega = reinterpret_cast<const double *>(base + o[4]);
+        e.X = reinterpret_cast<srom_complex *>(base + o[5]);
+        e.info = d.info ? reinterpret_cast<int *>(base + o[6]) : nullptr;
+        e.steps = d.steps ? reinterpret_cast<int *>(base + o[7]) : nullptr;
+        e.berr = d.berr ? reinterpret_cast<double *>(base + o[8]) : nullptr;
+        e.LU = nullptr;
+        e.ipiv = nullptr;
+        SROM_CUDA(h, cudaMemcpyAsync((void *)e.K, d.K, cz * nn, H2D, h->stream));
+        SROM_CUDA(h, cudaMemcpyAsync((void *)e.M, d.M, cz * nn, H2D, h->stream));
+        if (d.D) SROM_CUDA(h, cudaMemcpyAsync((void *)e.D, d.D, cz * nn, H2D, h->stream));
+        SROM_CUDA(h, cudaMemcpyAsync((void *)e.rhs, d.rhs, cz * (size_t)d.ldb * d.r, H2D, h->stream));
+        SROM_CUDA(h, cudaMemcpyAsync((void *)e.omega, d.omega, sizeof(double) * d.F, H2D, h->stream));
+    }
+    s = srom_sweep(h, dd.data(), n_roms, opts);
+    if (s) return s;
+    for (int i = 0; i < n_roms; ++i) {
+        const srom_rom_desc &d = roms[i];
+        const srom_rom_desc &e = dd[i];
+        if (d.n == 0 || d.F == 0 || d.r == 0) continue;
+        SROM_CUDA(h, cudaMemcpyAsync(d.X, e.X, sizeof(srom_complex) * (size_t)d.F * d.n * d.r, D2H, h->stream));
+        if (d.info) SROM_CUDA(h, cudaMemcpyAsync(d.info, e.info, sizeof(int) * d.F, D2H, h->stream));
+        if (d.steps) SROM_CUDA(h, cudaMemcpyAsync(d.steps, e.steps, sizeof(int) * d.F, D2H, h->stream));
+        if (d.berr) SROM_CUDA(h, cudaMemcpyAsync(d.berr, e.berr, sizeof(double) * d.F, D2H, h->stream));
+    }
+    SROM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return SROM_OK;
+}
+
+}  // extern "C"

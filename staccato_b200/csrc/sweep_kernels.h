@@ -1,0 +1,23 @@
+// Host-side entry points of the sweep kernels (used by the C ABI in capi.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace srom {
+
+struct RomDev;
+struct Item;
+
+// ---- FP64 (bit-identical to the restated zgetrf/zgetrs) ----
+size_t fp64_smem_bytes(int n, int r);
+size_t fp64_global_smem_bytes(int n_max, int r_max);
+int fp64_smem_blocks_per_sm(size_t smem);
+cudaError_t launch_fp64_smem(const RomDev *roms, const Item *items, int n_items, int *counter,
+                             size_t smem, int grid, cudaStream_t st);
+cudaError_t launch_fp64_global(const RomDev *roms, const Item *items, int n_items, int *counter,
+                               double2 *scratch, int64_t slot_elems, int n_max, int r_max,
+                               int grid, cudaStream_t st);
+
+}  // namespace srom

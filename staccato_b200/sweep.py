@@ -1,0 +1,156 @@
+"""Python front end of the batched frequency sweep (device-resident torch buffers).
+
+``sweep()`` packs one or many ROMs into ``srom_rom_desc`` records and calls ``srom_sweep``
+on the handle's stream; ``sweep_host()`` does the same through ``srom_sweep_host`` with
+host (numpy) buffers, which is the end-to-end form of the reference's backTransformKMOR.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _capi
+from ._capi import RomDesc, SweepOpts, check
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def colmajor(a) -> np.ndarray:
+    """Column-major complex128 data of a matrix as a flat array."""
+    return np.asarray(a, dtype=np.complex128).ravel(order="F")
+
+
+@dataclasses.dataclass
+class DeviceRom:
+    """One ROM with its inputs and outputs in device memory (flat column-major tensors)."""
+
+    n: int
+    r: int
+    F: int
+    K: "object"
+    M: "object"
+    D: Optional["object"]
+    rhs: "object"
+    omega: "object"
+    eta: float = 0.0
+    X: Optional["object"] = None
+    info: Optional["object"] = None
+    steps: Optional["object"] = None
+    berr: Optional["object"] = None
+    LU: Optional["object"] = None
+    ipiv: Optional["object"] = None
+
+    @classmethod
+    def from_host(cls, K, M, D, rhs, omega, eta: float = 0.0, device="cuda",
+                  keep_factors: bool = False) -> "DeviceRom":
+        torch = _torch()
+        K = np.asarray(K)
+        n = int(K.shape[0])
+        rhs = np.asarray(rhs, dtype=np.complex128)
+        if rhs.ndim == 1:
+            rhs = rhs[:, None]
+        r = int(rhs.shape[1])
+        omega = np.ascontiguousarray(omega, dtype=np.float64)
+        F = int(omega.shape[0])
+        t = lambda a: torch.from_numpy(colmajor(a)).to(device)
+        rom = cls(n=n, r=r, F=F, K=t(K), M=t(M), D=None if D is None else t(D), rhs=t(rhs),
+                  omega=torch.from_numpy(omega).to(device), eta=float(eta))
+        rom.allocate_outputs(device, keep_factors)
+        return rom
+
+    def allocate_outputs(self, device="cuda", keep_factors: bool = False) -> None:
+        torch = _torch()
+        self.X = torch.empty(self.F * self.n * self.r, dtype=torch.complex128, device=device)
+        self.info = torch.empty(self.F, dtype=torch.int32, device=device)
+        self.steps = torch.empty(self.F, dtype=torch.int32, device=device)
+        self.berr = torch.empty(self.F, dtype=torch.float64, device=device)
+        if keep_factors:
+            self.LU = torch.empty(self.F * self.n * self.n, dtype=torch.complex128, device=device)
+            self.ipiv = torch.empty(self.F * self.n, dtype=torch.int32, device=device)
+
+    def desc(self) -> RomDesc:
+        p = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+        return RomDesc(n=self.n, r=self.r, F=self.F, ldk=self.n, K=p(self.K), M=p(self.M),
+                       D=p(self.D), eta=self.eta, rhs=p(self.rhs), ldb=self.n,
+                       omega=p(self.omega), X=p(self.X), info=p(self.info), steps=p(self.steps),
+                       berr=p(self.berr), LU=p(self.LU), ipiv=p(self.ipiv))
+
+    def solutions(self) -> np.ndarray:
+        """X as a numpy array of shape (F, n, r)."""
+        x = self.X.cpu().numpy().reshape(self.F, self.r, self.n)
+        return np.ascontiguousarray(x.transpose(0, 2, 1))
+
+
+def opts(precision: int = _capi.SROM_FP64, max_refine: int = 5, tol: float = 0.0,
+         flags: int = 0) -> SweepOpts:
+    return SweepOpts(precision=precision, max_refine=max_refine, tol=tol, flags=flags)
+
+
+def sweep(handle: _capi.Handle, roms: Sequence[DeviceRom], precision: int = _capi.SROM_FP64,
+          max_refine: int = 5, tol: float = 0.0, flags: int = 0) -> None:
+    """Asynchronous batched sweep of every ROM on the handle's stream."""
+    arr = (RomDesc * max(len(roms), 1))(*[r.desc() for r in roms])
+    o = opts(precision, max_refine, tol, flags)
+    check(handle.ptr, _capi.lib().srom_sweep(handle.ptr, arr, len(roms), C.byref(o)))
+
+
+@dataclasses.dataclass
+class HostRom:
+    """Host (numpy) buffers for ``sweep_host``; outputs are filled in place."""
+
+    K: np.ndarray
+    M: np.ndarray
+    D: Optional[np.ndarray]
+    rhs: np.ndarray
+    omega: np.ndarray
+    eta: float = 0.0
+    X: Optional[np.ndarray] = None
+    info: Optional[np.ndarray] = None
+    steps: Optional[np.ndarray] = None
+    berr: Optional[np.ndarray] = None
+
+    def __post_init__(self):
+        self.K = colmajor(self.K)
+        self.M = colmajor(self.M)
+        self.D = None if self.D is None else colmajor(self.D)
+        rhs = np.asarray(self.rhs, dtype=np.complex128)
+        if rhs.ndim == 1:
+            rhs = rhs[:, None]
+        self.n = int(rhs.shape[0])
+        self.r = int(rhs.shape[1])
+        self.rhs = colmajor(rhs)
+        self.omega = np.ascontiguousarray(self.omega, dtype=np.float64)
+        self.F = int(self.omega.shape[0])
+        if self.X is None:
+            self.X = np.empty(self.F * self.n * self.r, dtype=np.complex128)
+        if self.info is None:
+            self.info = np.empty(self.F, dtype=np.int32)
+        if self.steps is None:
+            self.steps = np.empty(self.F, dtype=np.int32)
+        if self.berr is None:
+            self.berr = np.empty(self.F, dtype=np.float64)
+
+    def desc(self) -> RomDesc:
+        p = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+        return RomDesc(n=self.n, r=self.r, F=self.F, ldk=self.n, K=p(self.K), M=p(self.M),
+                       D=p(self.D), eta=self.eta, rhs=p(self.rhs), ldb=self.n,
+                       omega=p(self.omega), X=p(self.X), info=p(self.info), steps=p(self.steps),
+                       berr=p(self.berr), LU=None, ipiv=None)
+
+    def solutions(self) -> np.ndarray:
+        return np.ascontiguousarray(self.X.reshape(self.F, self.r, self.n).transpose(0, 2, 1))
+
+
+def sweep_host(handle: _capi.Handle, roms: Sequence[HostRom], precision: int = _capi.SROM_FP64,
+               max_refine: int = 5, tol: float = 0.0, flags: int = 0) -> None:
+    """Synchronous sweep with host buffers (copies in, sweeps, copies out)."""
+    arr = (RomDesc * max(len(roms), 1))(*[r.desc() for r in roms])
+    o = opts(precision, max_refine, tol, flags)
+    check(handle.ptr, _capi.lib().srom_sweep_host(handle.ptr, arr, len(roms), C.byref(o)))

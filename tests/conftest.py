@@ -1,0 +1,30 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
+
+
+@pytest.fixture(scope="session")
+def cuda_device():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu-marked tests")
+    return torch.device("cuda:0")
+
+
+@pytest.fixture(scope="session")
+def handle(cuda_device):
+    from staccato_b200 import _capi
+
+    h = _capi.Handle(0)
+    yield h
+    h.close()

@@ -1,0 +1,71 @@
+"""The C-ABI library loads and exports every declared symbol; struct layouts agree."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from staccato_b200 import _capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HDR_DIR = os.path.join(ROOT, "include")
+
+
+def _declared():
+    names = []
+    for f in sorted(os.listdir(HDR_DIR)):
+        if f.endswith(".h"):
+            txt = open(os.path.join(HDR_DIR, f)).read()
+            names += re.findall(r"SROM_API\s+[\w\s\*]+?\b(srom_\w+)\s*\(", txt)
+    return names
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = _capi.lib()
+    names = _declared()
+    assert names, "no SROM_API declarations found"
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) == set(_capi.EXPORTS)
+    assert lib.srom_version() >= 100
+
+
+def test_status_strings():
+    lib = _capi.lib()
+    assert lib.srom_status_string(0) == b"ok"
+    assert b"unsupported" in lib.srom_status_string(5)
+
+
+def test_struct_layout_matches_header():
+    src = r'''
+#include <stddef.h>
+#include <stdio.h>
+#include "staccato_rom.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(srom_rom_desc), offsetof(srom_rom_desc, eta),
+         offsetof(srom_rom_desc, ldb), offsetof(srom_rom_desc, ipiv), sizeof(srom_sweep_opts),
+         offsetof(srom_sweep_opts, flags));
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(c, "w").write(src)
+        subprocess.run(["gcc", "-I", HDR_DIR, c, "-o", exe], check=True)
+        got = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
+    R, S = _capi.RomDesc, _capi.SweepOpts
+    want = [C.sizeof(R), R.eta.offset, R.ldb.offset, R.ipiv.offset, C.sizeof(S), S.flags.offset]
+    assert got == want
+
+
+def test_create_without_gpu_fails_cleanly():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    st = _capi.lib().srom_create(C.byref(h), 0)
+    assert st != _capi.SROM_OK and not h
