@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark of the batched reduced-order frequency sweep on one (or N) B200.
+
+Metric: frequency-solves per second at <= 1e-10 relative error, mixed precision + FP64
+refinement versus plain FP64.  One "step" is one full sweep of the batching workload:
+64 seeded ROMs, n ~ U[24, 512], F ~ U[1000, 4000] frequencies over 1..2000 Hz, 1 or 4
+right-hand sides (164,933 systems, 12.8 TFLOP of complex LU + solve per step).  Inputs
+(167 MB of ROM matrices) and outputs (1.6 GB of solutions) are larger than the 126 MB L2,
+so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank sweeps its own copy of the workload (weak scaling, no
+collective on the data path); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "freq-solves/s at <=1e-10 rel err: mixed+refine vs plain FP64, 1 B200"
+WORKLOAD = ("batching: 64 ROMs, n~U[24,512], F~U[1000,4000] over 1-2000 Hz, r in {1,4}, "
+            "hysteretic eta=0.02, seed 3")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--precision", choices=["fp64"], default="fp64")
+    p.add_argument("--cpu-sample-stride", type=int, default=16,
+                   help="CPU baseline sweeps every k-th frequency of every ROM")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def workload_stats(roms):
+    n = np.array([r.n for r in roms], dtype=np.float64)
+    F = np.array([r.F for r in roms], dtype=np.float64)
+    r = np.array([r.r for r in roms], dtype=np.float64)
+    flops = float(((8.0 / 3.0) * n ** 3 + 8.0 * n ** 2 * r) @ F)
+    return int(F.sum()), flops
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = []
+        for line in (getattr(self, "out", "") or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = np.array([r[0] for r in rows])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k, v in enumerate(r[2]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(r[1] for r in rows)),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- peaks
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(path))
+    except (OSError, ValueError):
+        return {}
+
+
+def fp64_gemm_peak_tflops(torch, dev) -> float:
+    """cuBLAS DGEMM 8192^3, best of 5 (CUDA events): the FP64 denominator, measured in-run
+    because the FP64 rate is not part of the measured-peaks file."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+# ----------------------------------------------------------------------------- CPU legs
+
+def cpu_sample(roms, stride):
+    """Every stride-th frequency of every ROM (same n / r mix as the full workload)."""
+    return [(i, np.arange(0, rom.F, stride)) for i, rom in enumerate(roms)]
+
+
+def run_cpu_sweep(roms, sample, threads=0):
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    total = 0
+    outs = []
+    for i, idx in sample:
+        rom = roms[i]
+        om = np.ascontiguousarray(rom.omega[idx])
+        X = O.cpu_sweep(rom.K, rom.M, rom.D, 0.0, rom.rhs, om, 0, len(om), threads)
+        outs.append(X)
+        total += len(om)
+    dt = time.perf_counter() - t0
+    return total, dt, outs
+
+
+def cpu_baseline_leg(roms, stride, gpu_solutions):
+    """Time the CPU restatement on a bounded sample; check GPU accuracy on the same systems."""
+    from oracle import oracle as O
+
+    L = O.cpu_lib()
+    cores = int(L.cpu_baseline_default_threads())
+    sample = cpu_sample(roms, stride)
+    total, dt, outs = run_cpu_sweep(roms, sample, threads=cores)
+    kind = "port"
+    lapack = "OpenBLAS LAPACKE zgetrf/zgetrs" if L.cpu_baseline_using_lapacke() else "restated unblocked zgetrf/zgetrs"
+    base = {"value": total / dt, "unit": "freq-solves/s", "cores": cores, "kind": kind,
+            "sample": f"every {stride}th frequency of all 64 ROMs ({total} systems, {dt:.1f} s), {lapack}, "
+                      f"threaded over frequencies"}
+    acc = None
+    if gpu_solutions is not None:
+        errs_cpu, errs_ref = [], []
+        rng = np.random.default_rng(0)
+        for (i, idx), Xc in zip(sample, outs):
+            Xg = gpu_solutions(i, idx)
+            errs_cpu.append(O.rel_err(Xg, Xc))
+            pick = rng.choice(len(idx), size=1, replace=False)
+            rom = roms[i]
+            xr = O.x_ref(rom.K, rom.M, rom.D, 0.0, rom.rhs, rom.omega[idx[pick]])
+            errs_ref.append(O.rel_err(Xg[pick], xr))
+        e_cpu = np.concatenate(errs_cpu)
+        e_ref = np.concatenate(errs_ref)
+        acc = {"vs_cpu_fp64_max": float(e_cpu.max()), "vs_xref_max": float(e_ref.max()),
+               "vs_xref_median": float(np.median(e_ref)), "checked_systems": int(e_ref.size),
+               "gate_1e-10": bool(e_ref.max() <= 1e-10)}
+    return base, acc
+
+
+# ----------------------------------------------------------------------------- arms
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from staccato_b200 import workloads as W
+
+    roms = W.batching_roms()
+    stride = args.cpu_sample_stride
+    sample = cpu_sample(roms, stride)
+    from oracle import oracle as O
+
+    cores = int(O.cpu_lib().cpu_baseline_default_threads())
+    for _ in range(args.warmup):
+        run_cpu_sweep(roms, sample[:2], cores)
+    times, total = [], 0
+    for _ in range(args.steps):
+        total, dt, _ = run_cpu_sweep(roms, sample, cores)
+        times.append(dt)
+    dt = float(np.mean(times))
+    value = total / dt
+    lapack = ("OpenBLAS LAPACKE zgetrf/zgetrs" if O.cpu_lib().cpu_baseline_using_lapacke()
+              else "restated unblocked zgetrf/zgetrs")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "freq-solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "step": f"every {stride}th frequency of all 64 ROMs ({total} systems)"},
+        "cpu_baseline": {"value": value, "unit": "freq-solves/s", "cores": cores, "kind": "port",
+                         "sample": f"{total} systems per step; {lapack}; the reference's MKL build is not "
+                                   f"available (no MKL), this is the C restatement of its host sweep"},
+        "e2e": {"value": value, "unit": "freq-solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+
+    from staccato_b200 import _capi, workloads as W
+    from staccato_b200.sweep import DeviceRom, HostRom, sweep, sweep_host
+
+    roms = W.batching_roms()
+    systems, flops = workload_stats(roms)
+    h = _capi.Handle(local)
+    stream = torch.cuda.current_stream(dev)
+    h.set_stream(stream.cuda_stream)
+    drom = [DeviceRom.from_host(r.K, r.M, r.D, r.rhs, r.omega, device=dev) for r in roms]
+    precision = _capi.SROM_FP64
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    for _ in range(args.warmup):
+        sweep(h, drom, precision=precision)
+    torch.cuda.synchronize(dev)
+
+    h.profile(True)
+    h.read_profile()
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize(dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            sweep(h, drom, precision=precision)
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+    h.profile(False)
+    ms = t0.elapsed_time(t1) / args.steps
+    recs, nrec = h.read_profile()
+    if pg is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = systems * world / (ms * 1e-3)
+
+    # dominant kernel roofline (FP64 complex LU: flop-bound)
+    per = {}
+    for name, kms, items, kfl, kby in recs:
+        a = per.setdefault(name, [0.0, 0, 0.0, 0])
+        a[0] += kms
+        a[1] += items
+        a[2] += kfl
+        a[3] += 1
+    dom = max(per, key=lambda k: per[k][0]) if per else None
+    info = {}
+    if rank == 0:
+        peak64 = fp64_gemm_peak_tflops(torch, dev)
+        kms, kitems, kfl, kl = per[dom]
+        achieved = kfl / (kms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                "frac": achieved / peak64, "traffic": None, "kernel": dom,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)",
+                "algorithmic": "8/3 n^3 + 8 n^2 r real flops per system",
+                "kernels": {k: {"ms_per_launch": v[0] / v[3], "launches": v[3],
+                                "tflops": v[2] / (v[0] * 1e-3) / 1e12,
+                                "share": v[0] / sum(x[0] for x in per.values())} for k, v in per.items()}}
+        info["roofline"] = roof
+
+    # end to end through the host-buffer C ABI call (pinned host memory)
+    e2e = None
+    if not args.no_e2e:
+        def pinned(a):
+            a = np.ascontiguousarray(a)
+            t = torch.from_numpy(a.view(np.uint8).ravel()).pin_memory()
+            return t.numpy().view(a.dtype).reshape(a.shape)
+
+        hroms = []
+        h2d = d2h = 0
+        for r in roms:
+            hr = HostRom(r.K, r.M, r.D, r.rhs, r.omega)
+            for name in ("K", "M", "rhs", "omega", "X", "info", "steps", "berr"):
+                setattr(hr, name, pinned(getattr(hr, name)))
+            hroms.append(hr)
+            h2d += hr.K.nbytes + hr.M.nbytes + hr.rhs.nbytes + hr.omega.nbytes
+            d2h += hr.X.nbytes + hr.info.nbytes + hr.steps.nbytes + hr.berr.nbytes
+        sweep_host(h, hroms, precision=precision)
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            sweep_host(h, hroms, precision=precision)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        ems = e0.elapsed_time(e1) / args.steps
+        if pg is not None:
+            t = torch.tensor([ems], dtype=torch.float64, device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": systems * world / (ems * 1e-3), "unit": "freq-solves/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "api": "srom_sweep_host (host buffers in, host results out)"}
+
+    cpu = acc = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        def gpu_solutions(i, idx):
+            return drom[i].solutions()[idx]
+
+        cpu, acc = cpu_baseline_leg(roms, args.cpu_sample_stride, gpu_solutions)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "freq-solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "systems_per_gpu": systems,
+                       "tflop_per_step_per_gpu": flops / 1e12, "precision": args.precision,
+                       "l2": "inputs 167 MB + outputs 1.6 GB per step exceed L2; no flush",
+                       "parallelism": f"replica sweep per GPU x{world}"},
+            "roofline": info.get("roofline"),
+            "cpu_baseline": cpu,
+            "accuracy": acc,
+            "e2e": e2e,
+            "clocks": clk.summary(),
+            "gpu_launches": int(nrec),
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    h.close()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -122,6 +122,23 @@ SROM_API int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, c
  */
 SROM_API int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts);
 
+/* ---- per-launch timing -------------------------------------------------------------- */
+/* One record per kernel launch issued while profiling is enabled: CUDA events recorded on
+ * the handle's stream around the launch, plus the algorithmic work the launch performs
+ * (complex LU + solve: 8/3 n^3 + 8 n^2 r real flops per system; projection: bytes). */
+typedef struct {
+    char name[32];
+    float ms;         /* device time between the launch's start and end events */
+    long long items;  /* systems (or rows) the launch processed                */
+    double flops;     /* algorithmic real floating-point operations            */
+    double bytes;     /* algorithmic DRAM bytes                                */
+} srom_kernel_time;
+
+SROM_API int srom_profile_enable(srom_handle *h, int enable);
+/* Waits for the recorded launches, copies up to max records into out (may be NULL),
+ * stores the number of records in *count and clears the list. */
+SROM_API int srom_profile_read(srom_handle *h, srom_kernel_time *out, int max, int *count);
+
 #ifdef __cplusplus
 }
 #endif

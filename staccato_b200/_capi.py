@@ -31,8 +31,13 @@ SROM_INFO_NOT_CONVERGED = -1
 #: every symbol include/staccato_rom.h declares (checked by the CPU test-suite)
 EXPORTS = [
     "srom_create", "srom_destroy", "srom_set_stream", "srom_status_string", "srom_last_error",
-    "srom_version", "srom_sweep", "srom_sweep_host",
+    "srom_version", "srom_sweep", "srom_sweep_host", "srom_profile_enable", "srom_profile_read",
 ]
+
+
+class KernelTime(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("ms", C.c_float), ("items", C.c_longlong),
+                ("flops", C.c_double), ("bytes", C.c_double)]
 
 
 class RomDesc(C.Structure):
@@ -80,6 +85,10 @@ def lib() -> C.CDLL:
         L.srom_last_error.argtypes = [vp]
         L.srom_last_error.restype = C.c_char_p
         L.srom_version.restype = i
+        L.srom_profile_enable.argtypes = [vp, i]
+        L.srom_profile_enable.restype = i
+        L.srom_profile_read.argtypes = [vp, C.POINTER(KernelTime), i, C.POINTER(C.c_int)]
+        L.srom_profile_read.restype = i
         for name in ("srom_sweep", "srom_sweep_host"):
             fn = getattr(L, name)
             fn.argtypes = [vp, C.POINTER(RomDesc), i, C.POINTER(SweepOpts)]
@@ -112,6 +121,17 @@ class Handle:
 
     def set_stream(self, stream_ptr: int) -> None:
         check(self._h, lib().srom_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def profile(self, enable: bool = True) -> None:
+        check(self._h, lib().srom_profile_enable(self._h, int(enable)))
+
+    def read_profile(self, max_records: int = 4096):
+        """List of (name, ms, items, flops, bytes) for the launches since the last read."""
+        buf = (KernelTime * max_records)()
+        cnt = C.c_int()
+        check(self._h, lib().srom_profile_read(self._h, buf, max_records, C.byref(cnt)))
+        return [(buf[k].name.decode(), buf[k].ms, buf[k].items, buf[k].flops, buf[k].bytes)
+                for k in range(min(cnt.value, max_records))], cnt.value
 
     def close(self) -> None:
         if self._h:

@@ -35,6 +35,16 @@ struct srom_handle {
     // device buffers used by srom_sweep_host
     void *d_host_arena = nullptr;
     size_t d_host_arena_bytes = 0;
+    // per-launch profiling
+    struct ProfRec {
+        std::string name;
+        cudaEvent_t a, b;
+        long long items;
+        double flops, bytes;
+    };
+    bool prof = false;
+    std::vector<ProfRec> recs;
+    std::vector<cudaEvent_t> event_pool;
     std::string err;
 };
 
@@ -106,6 +116,35 @@ int ensure_host_pinned(srom_handle *h, size_t need) {
 }
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+cudaEvent_t pooled_event(srom_handle *h) {
+    if (!h->event_pool.empty()) {
+        cudaEvent_t e = h->event_pool.back();
+        h->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one launch with events when profiling is on.
+struct ProfScope {
+    srom_handle *h;
+    int idx = -1;
+    ProfScope(srom_handle *h_, const char *name, long long items, double flops, double bytes) : h(h_) {
+        if (!h->prof) return;
+        srom_handle::ProfRec r{name, pooled_event(h), pooled_event(h), items, flops, bytes};
+        cudaEventRecord(r.a, h->stream);
+        h->recs.push_back(r);
+        idx = (int)h->recs.size() - 1;
+    }
+    ~ProfScope() {
+        if (idx >= 0) cudaEventRecord(h->recs[idx].b, h->stream);
+    }
+};
+
+double lu_flops(int n, int r) { return 8.0 / 3.0 * (double)n * n * n + 8.0 * (double)n * n * r; }
 
 int validate_desc(srom_handle *h, const srom_rom_desc &d, int idx) {
     if (d.n < 0 || d.r < 0 || d.F < 0) return set_err(h, SROM_ERR_INVALID, "rom %d: negative size", idx);
@@ -198,6 +237,11 @@ int srom_destroy(srom_handle *h) {
     if (h->d_host_arena) cudaFree(h->d_host_arena);
     if (h->h_meta) cudaFreeHost(h->h_meta);
     if (h->meta_done) cudaEventDestroy(h->meta_done);
+    for (auto &r : h->recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : h->event_pool) cudaEventDestroy(e);
     delete h;
     return SROM_OK;
 }
@@ -205,6 +249,36 @@ int srom_destroy(srom_handle *h) {
 int srom_set_stream(srom_handle *h, void *stream) {
     if (!h) return SROM_ERR_INVALID;
     h->stream = reinterpret_cast<cudaStream_t>(stream);
+    return SROM_OK;
+}
+
+int srom_profile_enable(srom_handle *h, int enable) {
+    if (!h) return SROM_ERR_INVALID;
+    h->prof = enable != 0;
+    return SROM_OK;
+}
+
+int srom_profile_read(srom_handle *h, srom_kernel_time *out, int max, int *count) {
+    if (!h) return SROM_ERR_INVALID;
+    DeviceGuard g(h->device);
+    int k = 0;
+    for (auto &r : h->recs) {
+        SROM_CUDA(h, cudaEventSynchronize(r.b));
+        if (out && k < max) {
+            srom_kernel_time &t = out[k];
+            memset(&t, 0, sizeof t);
+            strncpy(t.name, r.name.c_str(), sizeof(t.name) - 1);
+            SROM_CUDA(h, cudaEventElapsedTime(&t.ms, r.a, r.b));
+            t.items = r.items;
+            t.flops = r.flops;
+            t.bytes = r.bytes;
+        }
+        ++k;
+        h->event_pool.push_back(r.a);
+        h->event_pool.push_back(r.b);
+    }
+    h->recs.clear();
+    if (count) *count = k;
     return SROM_OK;
 }
 
@@ -290,10 +364,14 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
     int *d_ctr = reinterpret_cast<int *>(dm + off_ctr);
 
     // ---- launches ------------------------------------------------------------------------
+    double flops[2] = {0.0, 0.0};
+    for (int i = 0; i < n_roms; ++i)
+        if (cls[i] >= 0) flops[cls[i]] += lu_flops(roms[i].n, roms[i].r) * roms[i].F;
     if (n_items[0] > 0) {
         int bps = srom::fp64_smem_blocks_per_sm(smem_max);
         if (bps <= 0) return set_err(h, SROM_ERR_UNSUPPORTED, "smem kernel cannot be resident (%zu B)", smem_max);
         long long grid = std::min<long long>(n_items[0], (long long)bps * h->sm_count);
+        ProfScope ps(h, "fp64_smem", n_items[0], flops[0], 0.0);
         SROM_CUDA(h, srom::launch_fp64_smem(d_roms, d_it0, (int)n_items[0], d_ctr, smem_max, (int)grid, h->stream));
     }
     if (n_items[1] > 0) {
@@ -308,6 +386,7 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
             if (s) return s;
             scr = static_cast<double2 *>(h->scratch);
         }
+        ProfScope ps(h, "fp64_global", n_items[1], flops[1], 0.0);
         SROM_CUDA(h, srom::launch_fp64_global(d_roms, d_it1, (int)n_items[1], d_ctr + 1, scr, slot, g_nmax,
                                               g_rmax, (int)grid, h->stream));
     }
