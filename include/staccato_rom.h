@@ -122,6 +122,23 @@ SROM_API int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, c
  */
 SROM_API int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts);
 
+/*
+ * FP64 sweep of one ROM that allocates no device memory.  No counterpart in the reference.
+ * For callers that cannot let a library allocate: programs that own all device memory
+ * through their own pool, or real-time loops in which cudaMalloc's implicit synchronisation
+ * and possible failure are not acceptable.  It needs no handle; it runs on the current
+ * device and the given stream (NULL = legacy default stream) and returns after enqueueing.
+ * Scratch is a 33 MB array inside the library (descriptor, work list and 32 MiB of matrix
+ * slots), held on every device that loads the library until the process exits.
+ * Limits: n <= 512, F <= 65536, and the panel must fit in shared memory (r <= 11 at n = 512);
+ * larger requests return SROM_ERR_UNSUPPORTED with the reason in err (err_len bytes).
+ * The first call on each device looks up the array's device address; make that first call
+ * before any stream capture.  Every call reuses the array (the work counter is cleared on
+ * each call): calls whose work overlaps on the GPU race and must be serialised by the caller.
+ * Results are bit-identical to srom_sweep with SROM_FP64.
+ */
+SROM_API int srom_sweep_fp64_noalloc(const srom_rom_desc *rom, void *cuda_stream, char *err, int err_len);
+
 /* ---- per-launch timing -------------------------------------------------------------- */
 /* One record per kernel launch issued while profiling is enabled: CUDA events recorded on
  * the handle's stream around the launch, plus the algorithmic work the launch performs

@@ -32,6 +32,7 @@ SROM_INFO_NOT_CONVERGED = -1
 EXPORTS = [
     "srom_create", "srom_destroy", "srom_set_stream", "srom_status_string", "srom_last_error",
     "srom_version", "srom_sweep", "srom_sweep_host", "srom_profile_enable", "srom_profile_read",
+    "srom_sweep_fp64_noalloc",
 ]
 
 
@@ -89,6 +90,8 @@ def lib() -> C.CDLL:
         L.srom_profile_enable.restype = i
         L.srom_profile_read.argtypes = [vp, C.POINTER(KernelTime), i, C.POINTER(C.c_int)]
         L.srom_profile_read.restype = i
+        L.srom_sweep_fp64_noalloc.argtypes = [C.POINTER(RomDesc), vp, C.c_char_p, i]
+        L.srom_sweep_fp64_noalloc.restype = i
         for name in ("srom_sweep", "srom_sweep_host"):
             fn = getattr(L, name)
             fn.argtypes = [vp, C.POINTER(RomDesc), i, C.POINTER(SweepOpts)]

@@ -1,0 +1,77 @@
+"""srom_sweep_fp64_noalloc: the sweep entry point that allocates no device memory.
+
+It exists for callers that cannot let a library allocate -- host programs that own all
+device memory through their own pool, or real-time loops in which cudaMalloc's implicit
+synchronisation and possible failure are not acceptable.  Its results must equal those of
+srom_sweep (FP64 results are bit-identical, the tolerance every FP64 test here uses), on
+two calls in a row, because every call reuses the library's scratch array.  This file is
+named so that pytest collects it last.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from staccato_b200 import _capi
+from staccato_b200.sweep import DeviceRom, sweep
+
+pytestmark = pytest.mark.gpu
+
+
+def _rom(seed, n, r, F, with_d):
+    rng = np.random.default_rng(seed)
+    c = lambda s: rng.standard_normal(s) + 1j * rng.standard_normal(s)
+    K = c((n, n)) * 10.0 + 3.0 * np.eye(n)
+    return DeviceRom.from_host(K, c((n, n)), c((n, n)) if with_d else None, c((n, r)),
+                               rng.uniform(0.1, 3.0, size=F), eta=0.01)
+
+
+def _noalloc(rom, stream):
+    d = rom.desc()
+    err = C.create_string_buffer(256)
+    st = _capi.lib().srom_sweep_fp64_noalloc(C.byref(d), C.c_void_p(stream), err, 256)
+    return st, err.value.decode()
+
+
+def _same(a, b):
+    return np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_noalloc_matches_srom_sweep_on_consecutive_calls(handle):
+    import torch
+
+    stream = torch.cuda.current_stream().cuda_stream
+    handle.set_stream(stream)
+    cases = [_rom(11, 100, 3, 37, True), _rom(12, 300, 2, 19, False), _rom(13, 512, 1, 9, True)]
+    refs = []
+    for rom in cases:
+        sweep(handle, [rom])
+        torch.cuda.synchronize()
+        refs.append((rom.solutions().copy(), rom.info.cpu().numpy().copy()))
+    for rnd in range(2):  # two calls in a row per case, and the cases back to back
+        for rom, (X, info) in zip(cases, refs):
+            rom.X.fill_(float("nan"))
+            rom.info.fill_(-7)
+            st, msg = _noalloc(rom, stream)
+            assert st == _capi.SROM_OK, msg
+            torch.cuda.synchronize()
+            assert _same(rom.solutions(), X), f"round {rnd} n={rom.n}"
+            assert np.array_equal(rom.info.cpu().numpy(), info)
+
+
+def test_noalloc_rejects_sizes_beyond_its_limit(handle):
+    import torch
+
+    rom = _rom(14, 4, 1, 2, False)
+    d = rom.desc()
+    d.n = 600
+    d.ldk = d.ldb = 600
+    err = C.create_string_buffer(256)
+    st = _capi.lib().srom_sweep_fp64_noalloc(C.byref(d), None, err, 256)
+    assert st == _capi.SROM_ERR_UNSUPPORTED
+    assert b"exceeds the limit of 512" in err.value
+    d = rom.desc()
+    d.F = 70000
+    st = _capi.lib().srom_sweep_fp64_noalloc(C.byref(d), None, err, 256)
+    assert st == _capi.SROM_ERR_UNSUPPORTED and b"65536" in err.value
+    torch.cuda.synchronize()
