@@ -287,15 +287,24 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
     h->err.clear();
     if (n_roms < 0 || (n_roms > 0 && !roms)) return set_err(h, SROM_ERR_INVALID, "roms is null");
     srom_sweep_opts o = opts ? *opts : srom_sweep_opts{SROM_FP64, 5, 0.0, 0};
-    if (o.precision != SROM_FP64)
+    if (o.precision != SROM_FP64 && o.precision != SROM_MIXED_FP32)
         return set_err(h, SROM_ERR_UNSUPPORTED, "precision %d not available in this build", o.precision);
+    const bool mixed = o.precision != SROM_FP64;
+    if (o.max_refine <= 0) o.max_refine = 5;
+    if (o.tol < 0.0) return set_err(h, SROM_ERR_INVALID, "tol must be >= 0");
     for (int i = 0; i < n_roms; ++i) {
         int s = validate_desc(h, roms[i], i);
         if (s) return s;
+        if (mixed && roms[i].LU)
+            return set_err(h, SROM_ERR_UNSUPPORTED, "rom %d: factors are kept only by the FP64 form", i);
+        if (mixed && roms[i].r > srom::MIXED_MAX_R)
+            return set_err(h, SROM_ERR_UNSUPPORTED, "rom %d: mixed form supports r <= %d", i, srom::MIXED_MAX_R);
     }
     DeviceGuard g(h->device);
 
     // ---- classify and order the work ---------------------------------------------------
+    // FP64: systems that fit shared memory use the smem kernel, the rest the global kernel.
+    // Mixed: every system uses the global kernel (FP32 factors + FP64 refinement).
     const size_t smem_cap = (size_t)h->max_smem_optin;
     std::vector<RomDev> dev(n_roms);
     std::vector<int> cls(n_roms, -1);  // 0 smem, 1 global
@@ -307,7 +316,7 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
         const srom_rom_desc &d = roms[i];
         if (d.n == 0 || d.F == 0 || d.r == 0) continue;
         size_t s = srom::fp64_smem_bytes(d.n, d.r);
-        if (s <= smem_cap) {
+        if (!mixed && s <= smem_cap) {
             cls[i] = 0;
             smem_max = std::max(smem_max, s);
         } else {
@@ -317,7 +326,8 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
         }
         n_items[cls[i]] += d.F;
     }
-    if (g_nmax > 0 && srom::fp64_global_smem_bytes(g_nmax, g_rmax) > smem_cap)
+    if (g_nmax > 0 && (srom::global_rpt(g_nmax) > srom::GLOBAL_MAX_RPT ||
+                       srom::global_smem_bytes(g_nmax, g_rmax) + srom::GLOBAL_STATIC_SMEM > smem_cap))
         return set_err(h, SROM_ERR_UNSUPPORTED, "n=%d with r=%d exceeds the shared-memory panel budget",
                        g_nmax, g_rmax);
     if (n_items[0] + n_items[1] > INT32_MAX) return set_err(h, SROM_ERR_UNSUPPORTED, "too many systems");
@@ -376,19 +386,20 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
     }
     if (n_items[1] > 0) {
         long long grid = std::min<long long>(n_items[1], h->sm_count);
-        bool all_keep = true;
+        bool all_keep = !mixed;
         for (int i = 0; i < n_roms; ++i)
             if (cls[i] == 1 && !roms[i].LU) all_keep = false;
-        const int64_t slot = (int64_t)g_nmax * g_nmax;
-        double2 *scr = nullptr;
+        const int64_t slot_bytes = (int64_t)g_nmax * g_nmax * (int64_t)sizeof(double2);
+        void *scr = nullptr;
         if (!all_keep) {
-            s = ensure_device_buffer(h, &h->scratch, &h->scratch_bytes, sizeof(double2) * (size_t)slot * grid);
+            s = ensure_device_buffer(h, &h->scratch, &h->scratch_bytes, (size_t)slot_bytes * grid);
             if (s) return s;
-            scr = static_cast<double2 *>(h->scratch);
+            scr = h->scratch;
         }
-        ProfScope ps(h, "fp64_global", n_items[1], flops[1], 0.0);
-        SROM_CUDA(h, srom::launch_fp64_global(d_roms, d_it1, (int)n_items[1], d_ctr + 1, scr, slot, g_nmax,
-                                              g_rmax, (int)grid, h->stream));
+        ProfScope ps(h, mixed ? "mixed_global" : "fp64_global", n_items[1], flops[1], 0.0);
+        SROM_CUDA(h, srom::launch_global(mixed, d_roms, d_it1, (int)n_items[1], d_ctr + 1, scr, slot_bytes, g_nmax,
+                                         g_rmax, (int)grid, o.max_refine, o.tol,
+                                         (o.flags & SROM_FLAG_FALLBACK_FP64) ? 1 : 0, h->stream));
     }
     return SROM_OK;
 }

@@ -106,3 +106,59 @@ __device__ __forceinline__ void swap2(double2 &a, double2 &b) {
 }
 
 }  // namespace srom
+
+namespace srom {
+
+// Complex arithmetic per storage type.  double2: the bit-exact FP64 contract above.
+// float2: the mixed-precision factorisation (fused multiply-adds, Smith division).
+template <typename T>
+struct CT;
+
+template <>
+struct CT<double2> {
+    using R = double;
+    static __device__ __forceinline__ double2 subm(double2 c, double2 a, double2 b) { return csubmul(c, a, b); }
+    static __device__ __forceinline__ double2 mul(double2 a, double2 b) { return cmul(a, b); }
+    static __device__ __forceinline__ double2 recip(double2 z) { return crecip(z); }
+    static __device__ __forceinline__ double2 div(double2 a, double2 b) { return cdiv(a, b); }
+    static __device__ __forceinline__ double abs1(double2 z) { return cabs1(z); }
+    static __device__ __forceinline__ double2 zero() { return make_double2(0.0, 0.0); }
+    static __device__ __forceinline__ double2 shfl(double2 v, int src, int width) {
+        return make_double2(__shfl_sync(FULL_MASK, v.x, src, width), __shfl_sync(FULL_MASK, v.y, src, width));
+    }
+};
+
+template <>
+struct CT<float2> {
+    using R = float;
+    static __device__ __forceinline__ float2 subm(float2 c, float2 a, float2 b) {
+        return make_float2(__fmaf_rn(-a.x, b.x, __fmaf_rn(a.y, b.y, c.x)),
+                           __fmaf_rn(-a.x, b.y, __fmaf_rn(-a.y, b.x, c.y)));
+    }
+    static __device__ __forceinline__ float2 mul(float2 a, float2 b) {
+        return make_float2(__fmaf_rn(a.x, b.x, -a.y * b.y), __fmaf_rn(a.x, b.y, a.y * b.x));
+    }
+    static __device__ __forceinline__ float2 recip(float2 z) {
+        if (fabsf(z.x) >= fabsf(z.y)) {
+            float t = z.y / z.x, d = z.x + z.y * t;
+            return make_float2(1.0f / d, -t / d);
+        }
+        float t = z.x / z.y, d = z.x * t + z.y;
+        return make_float2(t / d, -1.0f / d);
+    }
+    static __device__ __forceinline__ float2 div(float2 a, float2 b) {
+        if (fabsf(b.x) >= fabsf(b.y)) {
+            float t = b.y / b.x, d = b.x + b.y * t;
+            return make_float2((a.x + a.y * t) / d, (a.y - a.x * t) / d);
+        }
+        float t = b.x / b.y, d = b.x * t + b.y;
+        return make_float2((a.x * t + a.y) / d, (a.y * t - a.x) / d);
+    }
+    static __device__ __forceinline__ float abs1(float2 z) { return fabsf(z.x) + fabsf(z.y); }
+    static __device__ __forceinline__ float2 zero() { return make_float2(0.f, 0.f); }
+    static __device__ __forceinline__ float2 shfl(float2 v, int src, int width) {
+        return make_float2(__shfl_sync(FULL_MASK, v.x, src, width), __shfl_sync(FULL_MASK, v.y, src, width));
+    }
+};
+
+}  // namespace srom

@@ -1,0 +1,822 @@
+// Frequency-sweep kernels: fused assembly + partial-pivot complex LU + solve (+ refinement).
+//
+// One CTA owns one (ROM, frequency) system at a time and pulls the next one from a work
+// counter (persistent launch; the host orders the work list largest systems first).
+//
+// Storage classes
+//   smem   : whole n x n FP64 matrix and right-hand sides in shared memory (n up to ~112);
+//            unblocked right-looking LU, one warp searches each pivot.
+//   global : matrix in a per-CTA scratch slot (L2-resident while in flight); blocked
+//            right-looking LU.  The NB-column panel is staged in shared memory and factored
+//            by all warps with one CTA barrier per column: row interchanges are tracked as a
+//            logical permutation, so no row is physically moved while the column is being
+//            searched.  After the panel, every warp independently processes its own groups
+//            of CW trailing columns: apply the panel's interchanges, solve the unit-lower
+//            triangle for the U rows (warp shuffles), and update the remaining rows with
+//            register-tiled complex FMAs.  No CTA barrier separates the column groups.
+//
+// Precision forms
+//   FP64  (double2): reproduces LAPACK zgetrf/zgetrs as restated in the oracle bit for bit:
+//          IZAMAX pivots (largest |re|+|im|, smallest row index on ties) and every entry
+//          updated in increasing pivot-column order with the same fused multiply-adds.
+//   MIXED (float2 factors, NB = 32): the FP64-assembled matrix is rounded to complex FP32
+//          and factored; the solution is refined with residuals r = b - A(w) x computed in
+//          FP64 from K, M, D on the fly (the same assembly arithmetic) and corrections solved
+//          with the FP32 factors, until every right-hand side's last correction satisfies
+//          ||d||_inf <= tol ||x||_inf (default tol = 2^-33; the error left is about rho*tol,
+//          rho the contraction of the iteration), at most max_refine corrections after the
+//          first solve.  Frequencies that do not converge are re-solved in FP64 by the same
+//          CTA when asked (steps = -1).
+//
+// Reference sequence: src/analysis/KrylovROMSubstructure.cpp:1403-1453 (host, MKL), the
+// cuBLAS batched sweep of test/krylovMidsizeTest/gpu/concurrent/batchedLU/src/main.cu:223-267
+// (no pivoting), the classical stopping rule of iterative refinement on the correction size (Wilkinson; Moler 1967).
+#include <climits>
+
+#include "srom_device.cuh"
+#include "sweep_kernels.h"
+
+namespace srom {
+
+constexpr int NT = 256;
+constexpr int NW = NT / 32;
+constexpr int CW = 4;      // trailing columns per warp group
+constexpr int RQ = 4;      // Schur rows per lane per pass
+constexpr int NB64 = 16;   // FP64 panel width
+constexpr int NB32 = 32;   // FP32 panel width
+
+// ====================================================================================
+// smem class (FP64)
+// ====================================================================================
+__device__ void panel_factor_smem(double2 *P, int ldp, int m, int ncols, int *ipiv, int *s_info,
+                                  double2 *Bs, int ldbs, int nrhs, int *s_bc) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int jj = 0; jj < ncols; ++jj) {
+        if (warp == 0) {
+            double best = -1.0;
+            int bi = INT_MAX;
+            for (int i = jj + lane; i < m; i += 32) {
+                double v = cabs1(P[i + (int64_t)jj * ldp]);
+                if (v > best) {
+                    best = v;
+                    bi = i;
+                }
+            }
+#pragma unroll
+            for (int off = 16; off; off >>= 1) {
+                double ob = __shfl_xor_sync(FULL_MASK, best, off);
+                int oi = __shfl_xor_sync(FULL_MASK, bi, off);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            // IZAMAX starts from the first entry: a NaN there is returned as the pivot.
+            double first = cabs1(P[jj + (int64_t)jj * ldp]);
+            if (bi == INT_MAX || first != first) bi = jj;
+            double2 piv = P[bi + (int64_t)jj * ldp];
+            bool nz = (piv.x != 0.0 || piv.y != 0.0);
+            if (nz) {
+                if (bi != jj) {
+                    if (lane == 0) {
+                        P[bi + (int64_t)jj * ldp] = P[jj + (int64_t)jj * ldp];
+                        P[jj + (int64_t)jj * ldp] = piv;
+                    }
+                    if (Bs)
+                        for (int c = lane; c < nrhs; c += 32)
+                            swap2(Bs[jj + (int64_t)c * ldbs], Bs[bi + (int64_t)c * ldbs]);
+                }
+                __syncwarp();
+                double2 inv = crecip(piv);
+                for (int i = jj + 1 + lane; i < m; i += 32)
+                    P[i + (int64_t)jj * ldp] = cmul(P[i + (int64_t)jj * ldp], inv);
+            } else if (lane == 0 && *s_info == 0) {
+                *s_info = jj + 1;
+            }
+            if (lane == 0) {
+                s_bc[0] = bi;
+                s_bc[1] = nz ? 1 : 0;
+                ipiv[jj] = bi + 1;
+            }
+        }
+        __syncthreads();
+        const int p = s_bc[0];
+        const bool doswap = s_bc[1] && p != jj;
+        if (doswap)
+            for (int c = tid; c < jj; c += NT) swap2(P[jj + (int64_t)c * ldp], P[p + (int64_t)c * ldp]);
+        for (int c = jj + 1 + warp; c < ncols; c += NW) {
+            double2 *col = P + (int64_t)c * ldp;
+            if (doswap) {
+                if (lane == 0) swap2(col[jj], col[p]);
+                __syncwarp();
+            }
+            const double2 u = col[jj];
+            const double2 *lcol = P + (int64_t)jj * ldp;
+            for (int i = jj + 1 + lane; i < m; i += 32) col[i] = csubmul(col[i], lcol[i], u);
+        }
+        __syncthreads();
+    }
+}
+
+// zgetrs 'N' on an in-place LU (A, lda) with B (n x nrhs, ldb) in shared memory; the row
+// interchanges have already been applied to B.  32-row blocks: one warp per right-hand side
+// solves the diagonal triangle, then all threads apply the block to the remaining rows; each
+// entry of B receives its updates in the oracle's order.
+template <typename T>
+__device__ void lu_solve(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs) {
+    using C = CT<T>;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int jb = 0; jb < n; jb += 32) {
+        const int je = min(jb + 32, n);
+        for (int c = warp; c < nrhs; c += NW) {
+            T *b = B + (int64_t)c * ldb;
+            for (int j = jb; j < je; ++j) {
+                const T bj = b[j];
+                const int i = j + 1 + lane;
+                if (i < je) b[i] = C::subm(b[i], A[i + j * lda], bj);
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        const int rows = n - je;
+        for (int e = tid; e < rows * nrhs; e += NT) {
+            const int i = je + e % rows, c = e / rows;
+            T *b = B + (int64_t)c * ldb;
+            T acc = b[i];
+            for (int j = jb; j < je; ++j) acc = C::subm(acc, A[i + j * lda], b[j]);
+            b[i] = acc;
+        }
+        __syncthreads();
+    }
+    for (int jend = n; jend > 0; jend -= 32) {
+        const int jb = max(jend - 32, 0);
+        for (int c = warp; c < nrhs; c += NW) {
+            T *b = B + (int64_t)c * ldb;
+            for (int j = jend - 1; j >= jb; --j) {
+                if (lane == 0) b[j] = C::div(b[j], A[j + j * lda]);
+                __syncwarp();
+                const T bj = b[j];
+                const int i = jb + lane;
+                if (i < j) b[i] = C::subm(b[i], A[i + j * lda], bj);
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < jb * nrhs; e += NT) {
+            const int i = e % jb, c = e / jb;
+            T *b = B + (int64_t)c * ldb;
+            T acc = b[i];
+            for (int j = jend - 1; j >= jb; --j) acc = C::subm(acc, A[i + j * lda], b[j]);
+            b[i] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ int next_item(int *counter, int *s_item) {
+    if (threadIdx.x == 0) *s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    int it = *s_item;
+    __syncthreads();
+    return it;
+}
+
+template <typename T>
+__device__ __forceinline__ T to_store(double2 v);
+template <>
+__device__ __forceinline__ double2 to_store<double2>(double2 v) { return v; }
+template <>
+__device__ __forceinline__ float2 to_store<float2>(double2 v) {
+    return make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
+}
+
+template <typename T>
+__device__ void assemble_into(T *A, int64_t lda, const RomDev &R, double w) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double s = -__dmul_rn(w, w);
+    for (int j = warp; j < R.n; j += NW)
+        for (int i = lane; i < R.n; i += 32) {
+            const int64_t e = i + (int64_t)j * R.ldk;
+            A[i + j * lda] = to_store<T>(assemble_entry(R.K[e], R.M[e], R.D, e, R.eta, s, w));
+        }
+}
+
+__device__ void load_rhs(double2 *B, int ldbs, const RomDev &R) {
+    for (int e = threadIdx.x; e < R.n * R.r; e += NT) {
+        const int i = e % R.n, c = e / R.n;
+        B[i + (int64_t)c * ldbs] = R.rhs[i + (int64_t)c * R.ldb];
+    }
+}
+
+__device__ void store_solution(const double2 *B, int ldbs, const RomDev &R, int f) {
+    double2 *X = R.X + (int64_t)f * R.n * R.r;
+    for (int e = threadIdx.x; e < R.n * R.r; e += NT) {
+        const int i = e % R.n, c = e / R.n;
+        X[i + (int64_t)c * R.n] = B[i + (int64_t)c * ldbs];
+    }
+}
+
+__global__ void __launch_bounds__(NT) sweep_fp64_smem_kernel(const RomDev *__restrict__ roms,
+                                                              const Item *__restrict__ items,
+                                                              int n_items, int *counter) {
+    extern __shared__ double2 smem[];
+    __shared__ int s_item, s_info, s_bc[2];
+    for (;;) {
+        const int it = next_item(counter, &s_item);
+        if (it >= n_items) break;
+        const Item w = items[it];
+        const RomDev R = roms[w.rom];
+        const int n = R.n;
+        const int lda = n | 1;
+        double2 *A = smem;
+        double2 *B = A + (int64_t)n * lda;
+        int *ipiv = reinterpret_cast<int *>(B + (int64_t)n * R.r);
+        assemble_into<double2>(A, lda, R, R.omega[w.f]);
+        load_rhs(B, n, R);
+        if (threadIdx.x == 0) s_info = 0;
+        __syncthreads();
+        panel_factor_smem(A, lda, n, n, ipiv, &s_info, B, n, R.r, s_bc);
+        lu_solve<double2>(A, lda, n, B, n, R.r);
+        store_solution(B, n, R, w.f);
+        if (R.LU) {
+            double2 *LU = R.LU + (int64_t)w.f * n * n;
+            for (int j = threadIdx.x >> 5; j < n; j += NW)
+                for (int i = threadIdx.x & 31; i < n; i += 32) LU[i + (int64_t)j * n] = A[i + j * lda];
+            for (int j = threadIdx.x; j < n; j += NT) R.ipiv[(int64_t)w.f * n + j] = ipiv[j];
+        }
+        if (threadIdx.x == 0) {
+            if (R.info) R.info[w.f] = s_info;
+            if (R.steps) R.steps[w.f] = 0;
+            if (R.berr) R.berr[w.f] = 0.0;
+        }
+        __syncthreads();
+    }
+}
+
+// ====================================================================================
+// global class
+// ====================================================================================
+template <typename Rl>
+struct PivotXchg {
+    Rl val[2][NW];
+    int lg[2][NW];
+    int ph[2][NW];
+    int physjj[2];
+    int firstnan[2];
+};
+
+struct PanelLists {
+    int nmoved;
+    int info;
+};
+
+// Factor the m x ncols panel P (physical row order, leading dimension ldp) with partial
+// pivoting.  Thread t owns physical rows t + k*NT.  On return s_perm[l] is the physical row
+// at logical position l, s_pivlg[jj] the logical row chosen at step jj (LAPACK ipiv - 1,
+// relative to the panel), and (s_mdst, s_msrc) list every row whose position changed.
+template <typename T, int RPT>
+__device__ void panel_factor_par(T *P, int ldp, int m, int ncols, int *s_perm, int *s_pivlg,
+                                 int *s_mdst, int *s_msrc, PanelLists &PL, int info_off,
+                                 PivotXchg<typename CT<T>::R> &X) {
+    using C = CT<T>;
+    using Rl = typename C::R;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int lg[RPT];
+    bool done[RPT];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+        const int ph = tid + k * NT;
+        lg[k] = ph;
+        done[k] = ph >= m;
+    }
+    for (int jj = 0; jj < ncols; ++jj) {
+        const int buf = jj & 1;
+        Rl best = Rl(-1);
+        int bl = INT_MAX, bp = -1;
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+            if (done[k]) continue;
+            const int ph = tid + k * NT;
+            const Rl v = C::abs1(P[ph + (int64_t)jj * ldp]);
+            if (v > best || (v == best && lg[k] < bl)) {
+                best = v;
+                bl = lg[k];
+                bp = ph;
+            }
+            if (lg[k] == jj) {
+                X.physjj[buf] = ph;
+                X.firstnan[buf] = (v != v);
+            }
+        }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            const Rl ob = __shfl_xor_sync(FULL_MASK, best, off);
+            const int ol = __shfl_xor_sync(FULL_MASK, bl, off);
+            const int op = __shfl_xor_sync(FULL_MASK, bp, off);
+            if (ob > best || (ob == best && ol < bl)) {
+                best = ob;
+                bl = ol;
+                bp = op;
+            }
+        }
+        if (lane == 0) {
+            X.val[buf][warp] = best;
+            X.lg[buf][warp] = bl;
+            X.ph[buf][warp] = bp;
+        }
+        __syncthreads();
+        best = X.val[buf][0];
+        bl = X.lg[buf][0];
+        bp = X.ph[buf][0];
+#pragma unroll
+        for (int w = 1; w < NW; ++w) {
+            const Rl ob = X.val[buf][w];
+            const int ol = X.lg[buf][w];
+            if (ob > best || (ob == best && ol < bl)) {
+                best = ob;
+                bl = ol;
+                bp = X.ph[buf][w];
+            }
+        }
+        const int physjj = X.physjj[buf];
+        // IZAMAX starts from the first entry: a NaN there is the pivot; all-NaN likewise.
+        if (X.firstnan[buf] || bp < 0) {
+            bp = physjj;
+            bl = jj;
+        }
+        const T piv = P[bp + (int64_t)jj * ldp];
+        const bool nz = (piv.x != 0 || piv.y != 0);
+        if (!nz) {  // LAPACK interchanges nothing for a zero pivot
+            bp = physjj;
+            bl = jj;
+        }
+        if (tid == 0) {
+            s_pivlg[jj] = bl;
+            if (!nz && PL.info == 0) PL.info = info_off + jj + 1;
+        }
+        const T inv = nz ? C::recip(piv) : C::zero();
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+            if (done[k]) continue;
+            const int ph = tid + k * NT;
+            if (ph == bp) {
+                done[k] = true;
+                lg[k] = jj;
+                continue;
+            }
+            if (ph == physjj) lg[k] = bl;
+            T l = P[ph + (int64_t)jj * ldp];
+            if (nz) {
+                l = C::mul(l, inv);
+                P[ph + (int64_t)jj * ldp] = l;
+            }
+            for (int c = jj + 1; c < ncols; ++c)
+                P[ph + (int64_t)c * ldp] = C::subm(P[ph + (int64_t)c * ldp], l, P[bp + (int64_t)c * ldp]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+        const int ph = tid + k * NT;
+        if (ph < m) {
+            s_perm[lg[k]] = ph;
+            if (lg[k] != ph) {
+                const int e = atomicAdd(&PL.nmoved, 1);
+                s_mdst[e] = lg[k];
+                s_msrc[e] = ph;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Per-warp processing of the columns outside the panel after panel j0 has been factored.
+//   * columns [0, j0) and the nrhs right-hand-side columns of B: apply the interchanges;
+//   * columns [j0+nbc, n) in groups of CW: interchanges, U rows by forward substitution with
+//     the unit-lower panel triangle, then A22 -= L21 U12 for logical rows [nbc, m).
+template <typename T, int NB>
+__device__ void trailing_update(T *A, int64_t lda, int n, int j0, int nbc, const T *P, int ldp,
+                                const int *s_perm, const int *s_mdst, const int *s_msrc, int nmoved,
+                                T *s_u, T *B, int ldbs, int nrhs) {
+    using C = CT<T>;
+    constexpr int MV = (2 * NB + 31) / 32;
+    constexpr int TR = 32 / NB;  // row segments per warp in the triangle solve
+    constexpr int TC = CW / TR;  // columns per lane in the triangle solve
+    static_assert(TR * TC == CW, "triangle solve covers the column group");
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int m = n - j0;
+
+    for (int c = warp; c < j0 + nrhs; c += NW) {
+        T *col = c < j0 ? A + (int64_t)c * lda + j0 : B + (int64_t)(c - j0) * ldbs + j0;
+        T mv[MV];
+#pragma unroll
+        for (int q = 0; q < MV; ++q) {
+            const int e = lane + 32 * q;
+            if (e < nmoved) mv[q] = col[s_msrc[e]];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < MV; ++q) {
+            const int e = lane + 32 * q;
+            if (e < nmoved) col[s_mdst[e]] = mv[q];
+        }
+        __syncwarp();
+    }
+
+    T *u = s_u + warp * NB * CW;
+    const int trow = lane % NB, tgrp = lane / NB;
+    for (int c0 = j0 + nbc + warp * CW; c0 < n; c0 += NW * CW) {
+        T mv[MV][CW];
+        T uv[TC];
+#pragma unroll
+        for (int q = 0; q < MV; ++q) {
+            const int e = lane + 32 * q;
+            if (e < nmoved) {
+                const int s = s_msrc[e];
+#pragma unroll
+                for (int cc = 0; cc < CW; ++cc)
+                    if (c0 + cc < n) mv[q][cc] = A[(j0 + s) + (int64_t)(c0 + cc) * lda];
+            }
+        }
+        const int prow = trow < nbc ? s_perm[trow] : 0;
+#pragma unroll
+        for (int t = 0; t < TC; ++t) {
+            const int cc = tgrp * TC + t;
+            uv[t] = (trow < nbc && c0 + cc < n) ? A[(j0 + prow) + (int64_t)(c0 + cc) * lda] : C::zero();
+        }
+        __syncwarp();
+        for (int k = 0; k < nbc; ++k) {
+            const bool act = trow > k && trow < nbc;
+            const T lk = act ? P[prow + (int64_t)k * ldp] : C::zero();
+#pragma unroll
+            for (int t = 0; t < TC; ++t) {
+                const T ukt = C::shfl(uv[t], k, NB);
+                if (act) uv[t] = C::subm(uv[t], lk, ukt);
+            }
+        }
+        if (trow < nbc) {
+#pragma unroll
+            for (int t = 0; t < TC; ++t) {
+                const int cc = tgrp * TC + t;
+                u[trow * CW + cc] = uv[t];
+                if (c0 + cc < n) A[(j0 + trow) + (int64_t)(c0 + cc) * lda] = uv[t];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < MV; ++q) {
+            const int e = lane + 32 * q;
+            if (e < nmoved) {
+                const int d = s_mdst[e];
+                if (d >= nbc) {
+#pragma unroll
+                    for (int cc = 0; cc < CW; ++cc)
+                        if (c0 + cc < n) A[(j0 + d) + (int64_t)(c0 + cc) * lda] = mv[q][cc];
+                }
+            }
+        }
+        __syncwarp();
+        for (int rb = nbc; rb < m; rb += 32 * RQ) {
+            T acc[RQ][CW];
+            int pr[RQ];
+#pragma unroll
+            for (int q = 0; q < RQ; ++q) {
+                const int l = rb + lane + 32 * q;
+                pr[q] = l < m ? s_perm[l] : 0;
+#pragma unroll
+                for (int cc = 0; cc < CW; ++cc)
+                    acc[q][cc] = (l < m && c0 + cc < n) ? A[(j0 + l) + (int64_t)(c0 + cc) * lda] : C::zero();
+            }
+            for (int k = 0; k < nbc; ++k) {
+                T lv[RQ], uw[CW];
+#pragma unroll
+                for (int q = 0; q < RQ; ++q) lv[q] = P[pr[q] + (int64_t)k * ldp];
+#pragma unroll
+                for (int cc = 0; cc < CW; ++cc) uw[cc] = u[k * CW + cc];
+#pragma unroll
+                for (int q = 0; q < RQ; ++q)
+#pragma unroll
+                    for (int cc = 0; cc < CW; ++cc) acc[q][cc] = C::subm(acc[q][cc], lv[q], uw[cc]);
+            }
+#pragma unroll
+            for (int q = 0; q < RQ; ++q) {
+                const int l = rb + lane + 32 * q;
+#pragma unroll
+                for (int cc = 0; cc < CW; ++cc)
+                    if (l < m && c0 + cc < n) A[(j0 + l) + (int64_t)(c0 + cc) * lda] = acc[q][cc];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Shared-memory carve-up of the global-class kernels (bytes from the dynamic base).
+struct GlobalSmem {
+    size_t panel, u, work64, work32, perm, ptot, pos, ipiv, moved, total;
+    static __host__ __device__ size_t up(size_t b) { return (b + 255) / 256 * 256; }
+    __host__ __device__ GlobalSmem(int ldp, int n_max, int r_max) {
+        panel = 0;                                         // ldp x 16 double2 == ldp x 32 float2
+        u = panel + up((size_t)ldp * 256);                 // per warp NB x CW complex
+        work64 = u + up((size_t)NW * 1024);
+        work32 = work64 + up((size_t)n_max * r_max * 16);
+        perm = work32 + up((size_t)n_max * r_max * 8);
+        ptot = perm + up((size_t)ldp * 4);
+        pos = ptot + up((size_t)ldp * 4);
+        ipiv = pos + up((size_t)ldp * 4);
+        moved = ipiv + up((size_t)ldp * 4);
+        total = moved + up((size_t)2 * 2 * NB32 * 4);
+    }
+};
+
+// Blocked LU of the system already assembled in A (n x n, lda).  B (smem, ld n, nrhs
+// columns, may be null) receives the interchanges; s_ptot (smem) the composite row
+// permutation (final row l holds original row s_ptot[l]); s_ipiv the LAPACK pivots.
+template <typename T, int NB, int RPT>
+__device__ void factor_global(T *A, int64_t lda, int n, int ldp, unsigned char *sm, const GlobalSmem &L,
+                              T *B, int nrhs, PanelLists &PL, PivotXchg<typename CT<T>::R> &X,
+                              int *s_pivlg) {
+    T *P = reinterpret_cast<T *>(sm + L.panel);
+    T *s_u = reinterpret_cast<T *>(sm + L.u);
+    int *s_perm = reinterpret_cast<int *>(sm + L.perm);
+    int *s_ptot = reinterpret_cast<int *>(sm + L.ptot);
+    int *s_ipiv = reinterpret_cast<int *>(sm + L.ipiv);
+    int *s_mdst = reinterpret_cast<int *>(sm + L.moved);
+    int *s_msrc = s_mdst + 2 * NB32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < n; i += NT) s_ptot[i] = i;
+    if (tid == 0) PL.info = 0;
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int nbc = min(NB, n - j0);
+        const int m = n - j0;
+        for (int c = warp; c < nbc; c += NW)
+            for (int i = lane; i < m; i += 32) P[i + (int64_t)c * ldp] = A[(j0 + i) + (j0 + c) * lda];
+        if (tid == 0) PL.nmoved = 0;
+        __syncthreads();
+        panel_factor_par<T, RPT>(P, ldp, m, nbc, s_perm, s_pivlg, s_mdst, s_msrc, PL, j0, X);
+        const int nmoved = PL.nmoved;
+        for (int c = warp; c < nbc; c += NW)
+            for (int i = lane; i < m; i += 32) A[(j0 + i) + (j0 + c) * lda] = P[s_perm[i] + (int64_t)c * ldp];
+        if (tid < nbc) s_ipiv[j0 + tid] = j0 + s_pivlg[tid] + 1;
+        if (warp == NW - 1) {
+            int v[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int e = lane + 32 * q;
+                if (e < nmoved) v[q] = s_ptot[j0 + s_msrc[e]];
+            }
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int e = lane + 32 * q;
+                if (e < nmoved) s_ptot[j0 + s_mdst[e]] = v[q];
+            }
+            __syncwarp();
+        }
+        trailing_update<T, NB>(A, lda, n, j0, nbc, P, ldp, s_perm, s_mdst, s_msrc, nmoved, s_u, B, n, nrhs);
+        __syncthreads();
+    }
+}
+
+// r = b - A(w) x in FP64 with A(w) re-assembled from K, M, D (the FP64 assembly arithmetic),
+// written permuted and rounded to FP32 into B32 (B32[pos[i]] = r[i]) for the next correction.
+// Thread t owns rows t + k*NT; right-hand sides are processed four at a time.
+template <int RPT>
+__device__ void residual64(const RomDev &R, double w, const double2 *X64, float2 *B32, const int *s_pos) {
+    const int tid = threadIdx.x;
+    const int n = R.n;
+    const double s = -__dmul_rn(w, w);
+    for (int c0 = 0; c0 < R.r; c0 += 4) {
+        const int nc = min(4, R.r - c0);
+        double2 acc[RPT][4];
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+            const int i = tid + k * NT;
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc)
+                acc[k][cc] = (i < n && cc < nc) ? R.rhs[i + (int64_t)(c0 + cc) * R.ldb] : make_double2(0.0, 0.0);
+        }
+#pragma unroll 2
+        for (int j = 0; j < n; ++j) {
+            double2 xj[4];
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) xj[cc] = cc < nc ? X64[j + (int64_t)(c0 + cc) * n] : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) {
+                const int i = tid + k * NT;
+                if (i < n) {
+                    const int64_t e = i + (int64_t)j * R.ldk;
+                    const double2 a = assemble_entry(R.K[e], R.M[e], R.D, e, R.eta, s, w);
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) acc[k][cc] = csubmul(acc[k][cc], a, xj[cc]);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+            const int i = tid + k * NT;
+            if (i < n) {
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc)
+                    if (cc < nc)
+                        B32[s_pos[i] + (int64_t)(c0 + cc) * n] =
+                            make_float2(__double2float_rn(acc[k][cc].x), __double2float_rn(acc[k][cc].y));
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// x += d (FP32 correction) and, per right-hand side, the relative correction size
+// ||d||_inf / ||x||_inf (|re|+|im| norms) into s_dx; one warp per right-hand side.
+__device__ void apply_correction(double2 *X, const float2 *B32, int n, int nrhs, double *s_dx) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = warp; c < nrhs; c += NW) {
+        double dm = 0.0, xm = 0.0;
+        for (int i = lane; i < n; i += 32) {
+            const float2 d = B32[i + (int64_t)c * n];
+            double2 &x = X[i + (int64_t)c * n];
+            x.x += (double)d.x;
+            x.y += (double)d.y;
+            dm = fmax(dm, fabs((double)d.x) + fabs((double)d.y));
+            xm = fmax(xm, fabs(x.x) + fabs(x.y));
+        }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            dm = fmax(dm, __shfl_xor_sync(FULL_MASK, dm, off));
+            xm = fmax(xm, __shfl_xor_sync(FULL_MASK, xm, off));
+        }
+        if (lane == 0) s_dx[c] = xm > 0.0 ? dm / xm : (dm > 0.0 ? INFINITY : 0.0);
+    }
+    __syncthreads();
+}
+
+constexpr int RMAX_MIXED = 16;
+constexpr int SROM_INFO_NOT_CONVERGED_DEV = -1;
+
+template <bool MIXED, int RPT>
+__global__ void __launch_bounds__(NT) sweep_global_kernel(const RomDev *__restrict__ roms,
+                                                           const Item *__restrict__ items, int n_items,
+                                                           int *counter, unsigned char *scratch,
+                                                           int64_t slot_bytes, int ldp, int n_max,
+                                                           int r_max, int max_refine, double tol,
+                                                           int fallback) {
+    extern __shared__ __align__(256) unsigned char sm[];
+    __shared__ int s_item;
+    __shared__ int s_pivlg[NB32];
+    __shared__ PanelLists PL;
+    __shared__ PivotXchg<double> X64x;
+    __shared__ PivotXchg<float> X32x;
+    __shared__ double s_dx[RMAX_MIXED];
+    const GlobalSmem L(ldp, n_max, r_max);
+    const int tid = threadIdx.x;
+    for (;;) {
+        const int it = next_item(counter, &s_item);
+        if (it >= n_items) break;
+        const Item wi = items[it];
+        const RomDev R = roms[wi.rom];
+        const int n = R.n;
+        const double w = R.omega[wi.f];
+        int *s_ipiv = reinterpret_cast<int *>(sm + L.ipiv);
+        bool need64 = !MIXED;
+        int steps = 0, info = 0;
+        double berr = 0.0;
+        if (MIXED) {
+            float2 *A32 = reinterpret_cast<float2 *>(scratch + (int64_t)blockIdx.x * slot_bytes);
+            double2 *X = reinterpret_cast<double2 *>(sm + L.work64);
+            float2 *B32 = reinterpret_cast<float2 *>(sm + L.work32);
+            int *s_pos = reinterpret_cast<int *>(sm + L.pos);
+            int *s_ptot = reinterpret_cast<int *>(sm + L.ptot);
+            assemble_into<float2>(A32, n, R, w);
+            __syncthreads();
+            factor_global<float2, NB32, RPT>(A32, n, n, ldp, sm, L, nullptr, 0, PL, X32x, s_pivlg);
+            info = PL.info;
+            for (int l = tid; l < n; l += NT) s_pos[s_ptot[l]] = l;
+            __syncthreads();
+            for (int e = tid; e < n * R.r; e += NT) {
+                const int i = e % n, c = e / n;
+                X[i + (int64_t)c * n] = make_double2(0.0, 0.0);
+                const double2 b = R.rhs[i + (int64_t)c * R.ldb];
+                B32[s_pos[i] + (int64_t)c * n] = make_float2(__double2float_rn(b.x), __double2float_rn(b.y));
+            }
+            __syncthreads();
+            const double tol_x = tol > 0.0 ? tol : 1.1641532182693481e-10;  // 2^-33
+            bool conv = false;
+            for (int s = 0;; ++s) {
+                if (s > 0) residual64<RPT>(R, w, X, B32, s_pos);
+                lu_solve<float2>(A32, n, n, B32, n, R.r);
+                apply_correction(X, B32, n, R.r, s_dx);
+                if (s > 0) {
+                    double worst = 0.0;
+                    for (int c = 0; c < R.r; ++c) worst = fmax(worst, s_dx[c]);
+                    berr = worst;
+                    conv = worst <= tol_x;
+                }
+                steps = s;
+                if (conv || s >= max_refine) break;
+            }
+            if (conv) {
+                store_solution(X, n, R, wi.f);
+            } else if (fallback) {
+                need64 = true;
+                steps = -1;
+            } else {
+                store_solution(X, n, R, wi.f);
+                info = info == 0 ? SROM_INFO_NOT_CONVERGED_DEV : info;
+            }
+            __syncthreads();
+        }
+        if (need64) {
+            double2 *A64 = R.LU ? R.LU + (int64_t)wi.f * n * n
+                                : reinterpret_cast<double2 *>(scratch + (int64_t)blockIdx.x * slot_bytes);
+            double2 *B = reinterpret_cast<double2 *>(sm + L.work64);
+            assemble_into<double2>(A64, n, R, w);
+            load_rhs(B, n, R);
+            __syncthreads();
+            factor_global<double2, NB64, RPT>(A64, n, n, ldp, sm, L, B, R.r, PL, X64x, s_pivlg);
+            info = PL.info;
+            lu_solve<double2>(A64, n, n, B, n, R.r);
+            store_solution(B, n, R, wi.f);
+            if (!MIXED) berr = 0.0;
+        }
+        if (tid == 0) {
+            if (R.info) R.info[wi.f] = info;
+            if (R.steps) R.steps[wi.f] = steps;
+            if (R.berr) R.berr[wi.f] = berr;
+        }
+        if (R.ipiv && need64)
+            for (int j = tid; j < n; j += NT) R.ipiv[(int64_t)wi.f * n + j] = s_ipiv[j];
+        __syncthreads();
+    }
+}
+
+// ====================================================================================
+// host-side launch helpers
+// ====================================================================================
+size_t fp64_smem_bytes(int n, int r) {
+    const size_t lda = (size_t)(n | 1);
+    return sizeof(double2) * (lda * n + (size_t)n * r) + sizeof(int) * (size_t)n;
+}
+
+size_t global_smem_bytes(int n_max, int r_max) { return GlobalSmem(n_max | 1, n_max, r_max).total; }
+
+size_t fp64_global_smem_bytes(int n_max, int r_max) { return global_smem_bytes(n_max, r_max); }
+
+int global_rpt(int n_max) { return (n_max + NT - 1) / NT; }
+
+cudaError_t launch_fp64_smem(const RomDev *roms, const Item *items, int n_items, int *counter,
+                             size_t smem, int grid, cudaStream_t st) {
+    auto k = sweep_fp64_smem_kernel;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, NT, smem, st>>>(roms, items, n_items, counter);
+    return cudaGetLastError();
+}
+
+int fp64_smem_blocks_per_sm(size_t smem) {
+    int b = 0;
+    auto k = sweep_fp64_smem_kernel;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, NT, smem) != cudaSuccess) return 0;
+    return b;
+}
+
+template <bool MIXED, int RPT>
+static cudaError_t launch_global_t(const RomDev *roms, const Item *items, int n_items, int *counter,
+                                   void *scratch, int64_t slot_bytes, int n_max, int r_max, int grid,
+                                   int max_refine, double tol, int fallback, cudaStream_t st) {
+    auto k = sweep_global_kernel<MIXED, RPT>;
+    const size_t smem = global_smem_bytes(n_max, r_max);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, NT, smem, st>>>(roms, items, n_items, counter, static_cast<unsigned char *>(scratch), slot_bytes,
+                              n_max | 1, n_max, r_max, max_refine, tol, fallback);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_global(bool mixed, const RomDev *roms, const Item *items, int n_items, int *counter,
+                          void *scratch, int64_t slot_bytes, int n_max, int r_max, int grid,
+                          int max_refine, double tol, int fallback, cudaStream_t st) {
+    const int rpt = global_rpt(n_max);
+    if (r_max > RMAX_MIXED && mixed) return cudaErrorInvalidValue;
+#define SROM_LG(M, RP)                                                                               \
+    return launch_global_t<M, RP>(roms, items, n_items, counter, scratch, slot_bytes, n_max, r_max, grid, \
+                                  max_refine, tol, fallback, st)
+    if (mixed) {
+        if (rpt <= 1) SROM_LG(true, 1);
+        if (rpt == 2) SROM_LG(true, 2);
+        if (rpt == 3) SROM_LG(true, 3);
+    } else {
+        if (rpt <= 1) SROM_LG(false, 1);
+        if (rpt == 2) SROM_LG(false, 2);
+        if (rpt == 3) SROM_LG(false, 3);
+    }
+#undef SROM_LG
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_fp64_global(const RomDev *roms, const Item *items, int n_items, int *counter,
+                               double2 *scratch, int64_t slot_elems, int n_max, int r_max, int grid,
+                               cudaStream_t st) {
+    return launch_global(false, roms, items, n_items, counter, scratch, slot_elems * (int64_t)sizeof(double2),
+                         n_max, r_max, grid, 0, 0.0, 0, st);
+}
+
+}  // namespace srom

@@ -16,6 +16,15 @@ size_t fp64_global_smem_bytes(int n_max, int r_max);
 int fp64_smem_blocks_per_sm(size_t smem);
 cudaError_t launch_fp64_smem(const RomDev *roms, const Item *items, int n_items, int *counter,
                              size_t smem, int grid, cudaStream_t st);
+size_t global_smem_bytes(int n_max, int r_max);
+int global_rpt(int n_max);
+constexpr int GLOBAL_MAX_RPT = 3;
+constexpr int MIXED_MAX_R = 16;
+constexpr size_t GLOBAL_STATIC_SMEM = 4096;
+// Global-storage kernel, FP64 (mixed = false) or complex-FP32 factors + FP64 refinement.
+cudaError_t launch_global(bool mixed, const RomDev *roms, const Item *items, int n_items, int *counter,
+                          void *scratch, int64_t slot_bytes, int n_max, int r_max, int grid,
+                          int max_refine, double tol, int fallback, cudaStream_t st);
 cudaError_t launch_fp64_global(const RomDev *roms, const Item *items, int n_items, int *counter,
                                double2 *scratch, int64_t slot_elems, int n_max, int r_max,
                                int grid, cudaStream_t st);
