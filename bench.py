@@ -39,7 +39,8 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--precision", choices=["fp64"], default="fp64")
+    p.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
+                   help="both: headline = mixed+refine, plain FP64 measured beside it")
     p.add_argument("--cpu-sample-stride", type=int, default=16,
                    help="CPU baseline sweeps every k-th frequency of every ROM")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -121,12 +122,15 @@ def measured_peaks():
         return {}
 
 
-def fp64_gemm_peak_tflops(torch, dev) -> float:
-    """cuBLAS DGEMM 8192^3, best of 5 (CUDA events): the FP64 denominator, measured in-run
-    because the FP64 rate is not part of the measured-peaks file."""
+def gemm_peak_tflops(torch, dev, dtype) -> float:
+    """cuBLAS GEMM 8192^3 (DGEMM for float64; SGEMM with TF32 off for float32), best of 5
+    (CUDA events): the FP64 / FP32-FMA denominators, measured in-run because only the HBM
+    and bf16 rates are in the measured-peaks file."""
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device=dev)
-    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(n, n, dtype=dtype, device=dev)
+    b = torch.randn(n, n, dtype=dtype, device=dev)
     torch.matmul(a, b)
     best = 1e30
     for _ in range(5):
@@ -138,6 +142,7 @@ def fp64_gemm_peak_tflops(torch, dev) -> float:
         best = min(best, s.elapsed_time(e))
     del a, b
     torch.cuda.empty_cache()
+    torch.backends.cuda.matmul.allow_tf32 = prev
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
@@ -259,60 +264,88 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     h.set_stream(stream.cuda_stream)
     drom = [DeviceRom.from_host(r.K, r.M, r.D, r.rhs, r.omega, device=dev) for r in roms]
-    precision = _capi.SROM_FP64
+    FORMS = {"fp64": (_capi.SROM_FP64, 0),
+             "mixed": (_capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)}
+    forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    headline = forms[-1]
 
     def barrier():
         if pg is not None:
             pg.barrier()
 
-    for _ in range(args.warmup):
-        sweep(h, drom, precision=precision)
-    torch.cuda.synchronize(dev)
-
-    h.profile(True)
-    h.read_profile()
-    with ClockSampler(local) as clk:
-        barrier()
+    results = {}
+    clk = None
+    nrec_total = 0
+    for form in forms:
+        precision, flags = FORMS[form]
+        for _ in range(args.warmup):
+            sweep(h, drom, precision=precision, flags=flags)
         torch.cuda.synchronize(dev)
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
-        t0.record(stream)
-        for _ in range(args.steps):
-            sweep(h, drom, precision=precision)
-        t1.record(stream)
-        torch.cuda.synchronize(dev)
-        barrier()
-    h.profile(False)
-    ms = t0.elapsed_time(t1) / args.steps
-    recs, nrec = h.read_profile()
-    if pg is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-    value = systems * world / (ms * 1e-3)
+        h.profile(True)
+        h.read_profile()
+        with ClockSampler(local) as c:
+            barrier()
+            torch.cuda.synchronize(dev)
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(args.steps):
+                sweep(h, drom, precision=precision, flags=flags)
+            t1.record(stream)
+            torch.cuda.synchronize(dev)
+            barrier()
+        h.profile(False)
+        ms = t0.elapsed_time(t1) / args.steps
+        recs, nrec = h.read_profile()
+        nrec_total += nrec
+        if pg is not None:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        per = {}
+        for name, kms, items, kfl, kby in recs:
+            a = per.setdefault(name, [0.0, 0, 0.0, 0])
+            a[0] += kms
+            a[1] += items
+            a[2] += kfl
+            a[3] += 1
+        steps_hist = None
+        if form == "mixed":
+            st = np.concatenate([d.steps.cpu().numpy() for d in drom])
+            steps_hist = {str(k): int(v) for k, v in zip(*np.unique(st, return_counts=True))}
+        results[form] = {"ms": ms, "value": systems * world / (ms * 1e-3), "per": per, "steps": steps_hist}
+        if form == headline:
+            clk = c
 
-    # dominant kernel roofline (FP64 complex LU: flop-bound)
-    per = {}
-    for name, kms, items, kfl, kby in recs:
-        a = per.setdefault(name, [0.0, 0, 0.0, 0])
-        a[0] += kms
-        a[1] += items
-        a[2] += kfl
-        a[3] += 1
-    dom = max(per, key=lambda k: per[k][0]) if per else None
-    info = {}
-    if rank == 0:
-        peak64 = fp64_gemm_peak_tflops(torch, dev)
+    ms = results[headline]["ms"]
+    value = results[headline]["value"]
+    nrec = nrec_total
+
+    def roofline(form, peak, peak_source):
+        per = results[form]["per"]
+        dom = max(per, key=lambda k: per[k][0])
         kms, kitems, kfl, kl = per[dom]
         achieved = kfl / (kms * 1e-3) / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
-                "frac": achieved / peak64, "traffic": None, "kernel": dom,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)",
-                "algorithmic": "8/3 n^3 + 8 n^2 r real flops per system",
+        tot = sum(x[0] for x in per.values())
+        return {"bound": "tensor" if form == "fp64" else "fma", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "kernel": dom,
+                "peak_source": peak_source,
+                "algorithmic": "8/3 n^3 + 8 n^2 r real flops per system (LU + solve, both forms)",
                 "kernels": {k: {"ms_per_launch": v[0] / v[3], "launches": v[3],
-                                "tflops": v[2] / (v[0] * 1e-3) / 1e12,
-                                "share": v[0] / sum(x[0] for x in per.values())} for k, v in per.items()}}
-        info["roofline"] = roof
+                                "tflops": (v[2] / (v[0] * 1e-3) / 1e12) if v[0] > 0 else 0.0,
+                                "share": v[0] / tot if tot > 0 else 0.0} for k, v in per.items()}}
+
+    info = {}
+    if rank == 0:
+        if "fp64" in results:
+            p64 = gemm_peak_tflops(torch, dev, torch.float64)
+            info["roofline_fp64"] = roofline("fp64", p64, "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)")
+        if "mixed" in results:
+            p32 = gemm_peak_tflops(torch, dev, torch.float32)
+            info["roofline_mixed"] = roofline("mixed", p32, "cuBLAS SGEMM 8192^3, TF32 off, measured in this run (FP32 FMA rate is not in MEASURED_PEAKS.json)")
+        info["roofline"] = info.get("roofline_mixed") or info.get("roofline_fp64")
+    precision = FORMS[headline][0]
+    pflags = FORMS[headline][1]
 
     # end to end through the host-buffer C ABI call (pinned host memory)
     e2e = None
@@ -331,13 +364,13 @@ def run_ours(args):
             hroms.append(hr)
             h2d += hr.K.nbytes + hr.M.nbytes + hr.rhs.nbytes + hr.omega.nbytes
             d2h += hr.X.nbytes + hr.info.nbytes + hr.steps.nbytes + hr.berr.nbytes
-        sweep_host(h, hroms, precision=precision)
+        sweep_host(h, hroms, precision=precision, flags=pflags)
         barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
-            sweep_host(h, hroms, precision=precision)
+            sweep_host(h, hroms, precision=precision, flags=pflags)
         e1.record(stream)
         torch.cuda.synchronize(dev)
         barrier()
@@ -361,13 +394,20 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": "freq-solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 LU + c128 refinement" if headline == "mixed" else "c128",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "systems_per_gpu": systems,
-                       "tflop_per_step_per_gpu": flops / 1e12, "precision": args.precision,
+                       "tflop_per_step_per_gpu": flops / 1e12, "precision": headline,
+                       "refine": "complex-FP32 LU, FP64 residuals, <=5 corrections, stop at ||d||<=2^-33||x||, FP64 fallback",
                        "l2": "inputs 167 MB + outputs 1.6 GB per step exceed L2; no flush",
                        "parallelism": f"replica sweep per GPU x{world}"},
             "roofline": info.get("roofline"),
+            "roofline_fp64": info.get("roofline_fp64"),
+            "plain_fp64": ({"value": results["fp64"]["value"], "unit": "freq-solves/s",
+                            "ms_per_step": results["fp64"]["ms"]} if "fp64" in results else None),
+            "mixed_vs_plain": (results["mixed"]["value"] / results["fp64"]["value"]
+                               if "mixed" in results and "fp64" in results else None),
+            "refine_steps_hist": results.get("mixed", {}).get("steps"),
             "cpu_baseline": cpu,
             "accuracy": acc,
             "e2e": e2e,

@@ -339,7 +339,8 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
     // ---- stage descriptors + work lists ---------------------------------------------------
     const size_t off_items0 = align_up(sizeof(RomDev) * std::max(n_roms, 1), 256);
     const size_t off_items1 = off_items0 + align_up(sizeof(Item) * (size_t)n_items[0] + 1, 256);
-    const size_t off_ctr = off_items1 + align_up(sizeof(Item) * (size_t)n_items[1] + 1, 256);
+    const size_t off_fb = off_items1 + align_up(sizeof(Item) * (size_t)n_items[1] + 1, 256);
+    const size_t off_ctr = off_fb + (mixed ? align_up(sizeof(Item) * (size_t)n_items[1] + 1, 256) : 0);
     const size_t meta_bytes = off_ctr + 256;
     int s = ensure_host_pinned(h, meta_bytes);
     if (s) return s;
@@ -362,8 +363,7 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
         for (int f = 0; f < roms[i].F; ++f) dst[k++] = Item{i, f};
     }
     int *ctr = reinterpret_cast<int *>(hm + off_ctr);
-    ctr[0] = 0;
-    ctr[1] = 0;
+    for (int k = 0; k < 8; ++k) ctr[k] = 0;  // smem, global, fallback count, fallback work
     SROM_CUDA(h, cudaMemcpyAsync(h->d_meta, h->h_meta, meta_bytes, cudaMemcpyHostToDevice, h->stream));
     SROM_CUDA(h, cudaEventRecord(h->meta_done, h->stream));
     h->meta_pending = true;
@@ -396,10 +396,38 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
             if (s) return s;
             scr = h->scratch;
         }
-        ProfScope ps(h, mixed ? "mixed_global" : "fp64_global", n_items[1], flops[1], 0.0);
-        SROM_CUDA(h, srom::launch_global(mixed, d_roms, d_it1, (int)n_items[1], d_ctr + 1, scr, slot_bytes, g_nmax,
-                                         g_rmax, (int)grid, o.max_refine, o.tol,
-                                         (o.flags & SROM_FLAG_FALLBACK_FP64) ? 1 : 0, h->stream));
+        srom::GlobalArgs a{};
+        a.roms = d_roms;
+        a.items = d_it1;
+        a.n_items = (int)n_items[1];
+        a.counter = d_ctr + 1;
+        a.scratch = static_cast<unsigned char *>(scr);
+        a.slot_bytes = slot_bytes;
+        a.n_max = g_nmax;
+        a.r_max = g_rmax;
+        a.max_refine = o.max_refine;
+        a.tol = o.tol;
+        if (mixed && (o.flags & SROM_FLAG_FALLBACK_FP64)) {
+            a.fb_items = reinterpret_cast<Item *>(dm + off_fb);
+            a.fb_count = d_ctr + 2;
+        }
+        {
+            ProfScope ps(h, mixed ? "mixed_global" : "fp64_global", n_items[1], flops[1], 0.0);
+            SROM_CUDA(h, srom::launch_global(mixed, a, (int)grid, h->stream));
+        }
+        if (a.fb_items) {
+            // FP64 re-solve of the systems the mixed kernel could not refine; the item count
+            // stays on the device, so the launch needs no host synchronisation.
+            srom::GlobalArgs b = a;
+            b.items = a.fb_items;
+            b.n_items_dev = a.fb_count;
+            b.counter = d_ctr + 3;
+            b.fb_items = nullptr;
+            b.fb_count = nullptr;
+            b.steps_value = -1;
+            ProfScope ps(h, "fp64_fallback", 0, 0.0, 0.0);
+            SROM_CUDA(h, srom::launch_global(false, b, (int)grid, h->stream));
+        }
     }
     return SROM_OK;
 }

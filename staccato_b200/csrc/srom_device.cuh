@@ -118,6 +118,15 @@ template <>
 struct CT<double2> {
     using R = double;
     static __device__ __forceinline__ double2 subm(double2 c, double2 a, double2 b) { return csubmul(c, a, b); }
+    // csubmul split into its two FMA layers (c.x += a.y b.y, c.y -= a.y b.x; then the a.x terms)
+    static __device__ __forceinline__ void subm_first(double2 &c, double2 a, double2 b) {
+        c.x = __fma_rn(a.y, b.y, c.x);
+        c.y = __fma_rn(-a.y, b.x, c.y);
+    }
+    static __device__ __forceinline__ void subm_second(double2 &c, double2 a, double2 b) {
+        c.x = __fma_rn(-a.x, b.x, c.x);
+        c.y = __fma_rn(-a.x, b.y, c.y);
+    }
     static __device__ __forceinline__ double2 mul(double2 a, double2 b) { return cmul(a, b); }
     static __device__ __forceinline__ double2 recip(double2 z) { return crecip(z); }
     static __device__ __forceinline__ double2 div(double2 a, double2 b) { return cdiv(a, b); }
@@ -137,6 +146,14 @@ struct CT<float2> {
     }
     static __device__ __forceinline__ float2 mul(float2 a, float2 b) {
         return make_float2(__fmaf_rn(a.x, b.x, -a.y * b.y), __fmaf_rn(a.x, b.y, a.y * b.x));
+    }
+    static __device__ __forceinline__ void subm_first(float2 &c, float2 a, float2 b) {
+        c.x = __fmaf_rn(a.y, b.y, c.x);
+        c.y = __fmaf_rn(-a.y, b.x, c.y);
+    }
+    static __device__ __forceinline__ void subm_second(float2 &c, float2 a, float2 b) {
+        c.x = __fmaf_rn(-a.x, b.x, c.x);
+        c.y = __fmaf_rn(-a.x, b.y, c.y);
     }
     static __device__ __forceinline__ float2 recip(float2 z) {
         if (fabsf(z.x) >= fabsf(z.y)) {

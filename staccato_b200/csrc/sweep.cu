@@ -32,6 +32,7 @@
 // cuBLAS batched sweep of test/krylovMidsizeTest/gpu/concurrent/batchedLU/src/main.cu:223-267
 // (no pivoting), the classical stopping rule of iterative refinement on the correction size (Wilkinson; Moler 1967).
 #include <climits>
+#include <type_traits>
 
 #include "srom_device.cuh"
 #include "sweep_kernels.h"
@@ -119,55 +120,96 @@ __device__ void panel_factor_smem(double2 *P, int ldp, int m, int ncols, int *ip
 }
 
 // zgetrs 'N' on an in-place LU (A, lda) with B (n x nrhs, ldb) in shared memory; the row
-// interchanges have already been applied to B.  32-row blocks: one warp per right-hand side
-// solves the diagonal triangle, then all threads apply the block to the remaining rows; each
-// entry of B receives its updates in the oracle's order.
+// interchanges have already been applied to B.  32-row blocks: the block's diagonal triangle
+// is staged in shared memory (tile, 32 x 33) when A lives in global memory, one warp per
+// right-hand side solves it with the values in registers (warp shuffles), then every thread
+// takes rows below (above) the block and applies the block to all right-hand sides of the
+// row.  Every entry of B receives its updates in the oracle's order.
 template <typename T>
-__device__ void lu_solve(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs) {
+__device__ void lu_solve(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs, T *tile) {
     using C = CT<T>;
+    constexpr int LDT = 33;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int jb = 0; jb < n; jb += 32) {
-        const int je = min(jb + 32, n);
+        const int je = min(jb + 32, n), bs = je - jb;
+        const T *D = A + jb + jb * lda;
+        int ldd = (int)lda;
+        if (tile) {
+            for (int j = warp; j < bs; j += NW)
+                if (lane < bs) tile[lane + j * LDT] = D[lane + j * lda];
+            D = tile;
+            ldd = LDT;
+            __syncthreads();
+        }
         for (int c = warp; c < nrhs; c += NW) {
-            T *b = B + (int64_t)c * ldb;
-            for (int j = jb; j < je; ++j) {
-                const T bj = b[j];
-                const int i = j + 1 + lane;
-                if (i < je) b[i] = C::subm(b[i], A[i + j * lda], bj);
-                __syncwarp();
+            T *b = B + (int64_t)c * ldb + jb;
+            T v = lane < bs ? b[lane] : C::zero();
+            for (int j = 0; j < bs; ++j) {
+                const T bj = C::shfl(v, j, 32);
+                if (lane > j && lane < bs) v = C::subm(v, D[lane + j * ldd], bj);
             }
+            if (lane < bs) b[lane] = v;
         }
         __syncthreads();
-        const int rows = n - je;
-        for (int e = tid; e < rows * nrhs; e += NT) {
-            const int i = je + e % rows, c = e / rows;
-            T *b = B + (int64_t)c * ldb;
-            T acc = b[i];
-            for (int j = jb; j < je; ++j) acc = C::subm(acc, A[i + j * lda], b[j]);
-            b[i] = acc;
+        for (int i = je + tid; i < n; i += NT) {
+            for (int c0 = 0; c0 < nrhs; c0 += 4) {
+                const int nc = min(4, nrhs - c0);
+                T acc[4];
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) acc[cc] = cc < nc ? B[i + (int64_t)(c0 + cc) * ldb] : C::zero();
+#pragma unroll 8
+                for (int j = jb; j < je; ++j) {
+                    const T a = A[i + j * lda];
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc)
+                        if (cc < nc) acc[cc] = C::subm(acc[cc], a, B[j + (int64_t)(c0 + cc) * ldb]);
+                }
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc)
+                    if (cc < nc) B[i + (int64_t)(c0 + cc) * ldb] = acc[cc];
+            }
         }
         __syncthreads();
     }
     for (int jend = n; jend > 0; jend -= 32) {
-        const int jb = max(jend - 32, 0);
+        const int jb = max(jend - 32, 0), bs = jend - jb;
+        const T *D = A + jb + jb * lda;
+        int ldd = (int)lda;
+        if (tile) {
+            for (int j = warp; j < bs; j += NW)
+                if (lane < bs) tile[lane + j * LDT] = D[lane + j * lda];
+            D = tile;
+            ldd = LDT;
+            __syncthreads();
+        }
         for (int c = warp; c < nrhs; c += NW) {
-            T *b = B + (int64_t)c * ldb;
-            for (int j = jend - 1; j >= jb; --j) {
-                if (lane == 0) b[j] = C::div(b[j], A[j + j * lda]);
-                __syncwarp();
-                const T bj = b[j];
-                const int i = jb + lane;
-                if (i < j) b[i] = C::subm(b[i], A[i + j * lda], bj);
-                __syncwarp();
+            T *b = B + (int64_t)c * ldb + jb;
+            T v = lane < bs ? b[lane] : C::zero();
+            for (int j = bs - 1; j >= 0; --j) {
+                if (lane == j) v = C::div(v, D[j + j * ldd]);
+                const T bj = C::shfl(v, j, 32);
+                if (lane < j) v = C::subm(v, D[lane + j * ldd], bj);
             }
+            if (lane < bs) b[lane] = v;
         }
         __syncthreads();
-        for (int e = tid; e < jb * nrhs; e += NT) {
-            const int i = e % jb, c = e / jb;
-            T *b = B + (int64_t)c * ldb;
-            T acc = b[i];
-            for (int j = jend - 1; j >= jb; --j) acc = C::subm(acc, A[i + j * lda], b[j]);
-            b[i] = acc;
+        for (int i = tid; i < jb; i += NT) {
+            for (int c0 = 0; c0 < nrhs; c0 += 4) {
+                const int nc = min(4, nrhs - c0);
+                T acc[4];
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) acc[cc] = cc < nc ? B[i + (int64_t)(c0 + cc) * ldb] : C::zero();
+#pragma unroll 8
+                for (int j = jend - 1; j >= jb; --j) {
+                    const T a = A[i + j * lda];
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc)
+                        if (cc < nc) acc[cc] = C::subm(acc[cc], a, B[j + (int64_t)(c0 + cc) * ldb]);
+                }
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc)
+                    if (cc < nc) B[i + (int64_t)(c0 + cc) * ldb] = acc[cc];
+            }
         }
         __syncthreads();
     }
@@ -236,7 +278,7 @@ __global__ void __launch_bounds__(NT) sweep_fp64_smem_kernel(const RomDev *__res
         if (threadIdx.x == 0) s_info = 0;
         __syncthreads();
         panel_factor_smem(A, lda, n, n, ipiv, &s_info, B, n, R.r, s_bc);
-        lu_solve<double2>(A, lda, n, B, n, R.r);
+        lu_solve<double2>(A, lda, n, B, n, R.r, nullptr);
         store_solution(B, n, R, w.f);
         if (R.LU) {
             double2 *LU = R.LU + (int64_t)w.f * n * n;
@@ -405,19 +447,33 @@ __device__ void trailing_update(T *A, int64_t lda, int n, int j0, int nbc, const
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int m = n - j0;
 
-    for (int c = warp; c < j0 + nrhs; c += NW) {
-        T *col = c < j0 ? A + (int64_t)c * lda + j0 : B + (int64_t)(c - j0) * ldbs + j0;
-        T mv[MV];
+    constexpr int CB = 8;  // swap-only columns per warp pass (loads in flight)
+    for (int cb = warp * CB; cb < j0 + nrhs; cb += NW * CB) {
+        T mv[MV][CB];
 #pragma unroll
-        for (int q = 0; q < MV; ++q) {
-            const int e = lane + 32 * q;
-            if (e < nmoved) mv[q] = col[s_msrc[e]];
+        for (int t = 0; t < CB; ++t) {
+            const int c = cb + t;
+            if (c < j0 + nrhs) {
+                const T *col = c < j0 ? A + (int64_t)c * lda + j0 : B + (int64_t)(c - j0) * ldbs + j0;
+#pragma unroll
+                for (int q = 0; q < MV; ++q) {
+                    const int e = lane + 32 * q;
+                    if (e < nmoved) mv[q][t] = col[s_msrc[e]];
+                }
+            }
         }
         __syncwarp();
 #pragma unroll
-        for (int q = 0; q < MV; ++q) {
-            const int e = lane + 32 * q;
-            if (e < nmoved) col[s_mdst[e]] = mv[q];
+        for (int t = 0; t < CB; ++t) {
+            const int c = cb + t;
+            if (c < j0 + nrhs) {
+                T *col = c < j0 ? A + (int64_t)c * lda + j0 : B + (int64_t)(c - j0) * ldbs + j0;
+#pragma unroll
+                for (int q = 0; q < MV; ++q) {
+                    const int e = lane + 32 * q;
+                    if (e < nmoved) col[s_mdst[e]] = mv[q][t];
+                }
+            }
         }
         __syncwarp();
     }
@@ -474,27 +530,45 @@ __device__ void trailing_update(T *A, int64_t lda, int n, int j0, int nbc, const
             }
         }
         __syncwarp();
-        for (int rb = nbc; rb < m; rb += 32 * RQ) {
-            T acc[RQ][CW];
-            int pr[RQ];
+        T nxt[RQ][CW];
+        int npr[RQ];
+        auto load_chunk = [&](int rb, T (&dst)[RQ][CW], int (&pr)[RQ]) {
 #pragma unroll
             for (int q = 0; q < RQ; ++q) {
                 const int l = rb + lane + 32 * q;
                 pr[q] = l < m ? s_perm[l] : 0;
 #pragma unroll
                 for (int cc = 0; cc < CW; ++cc)
-                    acc[q][cc] = (l < m && c0 + cc < n) ? A[(j0 + l) + (int64_t)(c0 + cc) * lda] : C::zero();
+                    dst[q][cc] = (l < m && c0 + cc < n) ? A[(j0 + l) + (int64_t)(c0 + cc) * lda] : C::zero();
             }
+        };
+        if (nbc < m) load_chunk(nbc, nxt, npr);
+        for (int rb = nbc; rb < m; rb += 32 * RQ) {
+            T acc[RQ][CW];
+            int pr[RQ];
+#pragma unroll
+            for (int q = 0; q < RQ; ++q) {
+                pr[q] = npr[q];
+#pragma unroll
+                for (int cc = 0; cc < CW; ++cc) acc[q][cc] = nxt[q][cc];
+            }
+            if (rb + 32 * RQ < m) load_chunk(rb + 32 * RQ, nxt, npr);
             for (int k = 0; k < nbc; ++k) {
                 T lv[RQ], uw[CW];
 #pragma unroll
                 for (int q = 0; q < RQ; ++q) lv[q] = P[pr[q] + (int64_t)k * ldp];
 #pragma unroll
                 for (int cc = 0; cc < CW; ++cc) uw[cc] = u[k * CW + cc];
+                // c - a*b as two FMA layers over the whole tile: the same two roundings per
+                // component as C::subm, but every first FMA is issued before any second one.
 #pragma unroll
                 for (int q = 0; q < RQ; ++q)
 #pragma unroll
-                    for (int cc = 0; cc < CW; ++cc) acc[q][cc] = C::subm(acc[q][cc], lv[q], uw[cc]);
+                    for (int cc = 0; cc < CW; ++cc) C::subm_first(acc[q][cc], lv[q], uw[cc]);
+#pragma unroll
+                for (int q = 0; q < RQ; ++q)
+#pragma unroll
+                    for (int cc = 0; cc < CW; ++cc) C::subm_second(acc[q][cc], lv[q], uw[cc]);
             }
 #pragma unroll
             for (int q = 0; q < RQ; ++q) {
@@ -510,7 +584,7 @@ __device__ void trailing_update(T *A, int64_t lda, int n, int j0, int nbc, const
 
 // Shared-memory carve-up of the global-class kernels (bytes from the dynamic base).
 struct GlobalSmem {
-    size_t panel, u, work64, work32, perm, ptot, pos, ipiv, moved, total;
+    size_t panel, u, work64, work32, perm, ptot, pos, ipiv, moved, tile, total;
     static __host__ __device__ size_t up(size_t b) { return (b + 255) / 256 * 256; }
     __host__ __device__ GlobalSmem(int ldp, int n_max, int r_max) {
         panel = 0;                                         // ldp x 16 double2 == ldp x 32 float2
@@ -522,7 +596,8 @@ struct GlobalSmem {
         pos = ptot + up((size_t)ldp * 4);
         ipiv = pos + up((size_t)ldp * 4);
         moved = ipiv + up((size_t)ldp * 4);
-        total = moved + up((size_t)2 * 2 * NB32 * 4);
+        tile = moved + up((size_t)2 * 2 * NB32 * 4);
+        total = tile + up((size_t)32 * 33 * 16);          // diagonal block of the solves
     }
 };
 
@@ -580,6 +655,7 @@ __device__ void factor_global(T *A, int64_t lda, int n, int ldp, unsigned char *
 // Thread t owns rows t + k*NT; right-hand sides are processed four at a time.
 template <int RPT>
 __device__ void residual64(const RomDev &R, double w, const double2 *X64, float2 *B32, const int *s_pos) {
+    constexpr int JB = RPT >= 3 ? 1 : 4 / RPT;  // columns of K, M, D loaded per batch
     const int tid = threadIdx.x;
     const int n = R.n;
     const double s = -__dmul_rn(w, w);
@@ -593,19 +669,49 @@ __device__ void residual64(const RomDev &R, double w, const double2 *X64, float2
             for (int cc = 0; cc < 4; ++cc)
                 acc[k][cc] = (i < n && cc < nc) ? R.rhs[i + (int64_t)(c0 + cc) * R.ldb] : make_double2(0.0, 0.0);
         }
-#pragma unroll 2
-        for (int j = 0; j < n; ++j) {
-            double2 xj[4];
-#pragma unroll
-            for (int cc = 0; cc < 4; ++cc) xj[cc] = cc < nc ? X64[j + (int64_t)(c0 + cc) * n] : make_double2(0.0, 0.0);
+        for (int j0 = 0; j0 < n; j0 += JB) {
+            double2 kv[RPT][JB], mv[RPT][JB], dv[RPT][JB];
 #pragma unroll
             for (int k = 0; k < RPT; ++k) {
                 const int i = tid + k * NT;
-                if (i < n) {
-                    const int64_t e = i + (int64_t)j * R.ldk;
-                    const double2 a = assemble_entry(R.K[e], R.M[e], R.D, e, R.eta, s, w);
 #pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) acc[k][cc] = csubmul(acc[k][cc], a, xj[cc]);
+                for (int jj = 0; jj < JB; ++jj) {
+                    if (i < n && j0 + jj < n) {
+                        const int64_t e = i + (int64_t)(j0 + jj) * R.ldk;
+                        kv[k][jj] = R.K[e];
+                        mv[k][jj] = R.M[e];
+                        dv[k][jj] = R.D ? R.D[e] : make_double2(0.0, 0.0);
+                    }
+                }
+            }
+#pragma unroll
+            for (int jj = 0; jj < JB; ++jj) {
+                const int j = j0 + jj;
+                if (j >= n) break;
+                double2 xj[4];
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc)
+                    xj[cc] = cc < nc ? X64[j + (int64_t)(c0 + cc) * n] : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int k = 0; k < RPT; ++k) {
+                    const int i = tid + k * NT;
+                    if (i < n) {
+                        double2 kk = kv[k][jj];
+                        if (R.eta != 0.0) {
+                            const double t1 = __dmul_rn(R.eta, kk.y), t2 = __dmul_rn(R.eta, kk.x);
+                            kk.x = __dsub_rn(kk.x, t1);
+                            kk.y = __dadd_rn(kk.y, t2);
+                        }
+                        double2 a;
+                        a.x = __dadd_rn(kk.x, __dmul_rn(s, mv[k][jj].x));
+                        a.y = __dadd_rn(kk.y, __dmul_rn(s, mv[k][jj].y));
+                        if (R.D) {
+                            a.x = __dsub_rn(a.x, __dmul_rn(w, dv[k][jj].y));
+                            a.y = __dadd_rn(a.y, __dmul_rn(w, dv[k][jj].x));
+                        }
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc) acc[k][cc] = csubmul(acc[k][cc], a, xj[cc]);
+                    }
                 }
             }
         }
@@ -651,42 +757,41 @@ __device__ void apply_correction(double2 *X, const float2 *B32, int n, int nrhs,
 constexpr int RMAX_MIXED = 16;
 constexpr int SROM_INFO_NOT_CONVERGED_DEV = -1;
 
+// Global-class kernel.  MIXED: complex-FP32 factors + FP64 refinement; systems that do not
+// converge are appended to a.fb_items (when given) for the FP64 kernel launched after it.
+// FP64: the bit-exact path; a.n_items_dev (when given) holds the item count (fallback list).
 template <bool MIXED, int RPT>
-__global__ void __launch_bounds__(NT) sweep_global_kernel(const RomDev *__restrict__ roms,
-                                                           const Item *__restrict__ items, int n_items,
-                                                           int *counter, unsigned char *scratch,
-                                                           int64_t slot_bytes, int ldp, int n_max,
-                                                           int r_max, int max_refine, double tol,
-                                                           int fallback) {
+__global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
     extern __shared__ __align__(256) unsigned char sm[];
     __shared__ int s_item;
     __shared__ int s_pivlg[NB32];
     __shared__ PanelLists PL;
-    __shared__ PivotXchg<double> X64x;
-    __shared__ PivotXchg<float> X32x;
+    __shared__ PivotXchg<typename CT<typename std::conditional<MIXED, float2, double2>::type>::R> Xx;
     __shared__ double s_dx[RMAX_MIXED];
-    const GlobalSmem L(ldp, n_max, r_max);
+    using T = typename std::conditional<MIXED, float2, double2>::type;
+    const GlobalSmem L(a.ldp, a.n_max, a.r_max);
     const int tid = threadIdx.x;
+    const int n_items = a.n_items_dev ? *a.n_items_dev : a.n_items;
+    int *s_ipiv = reinterpret_cast<int *>(sm + L.ipiv);
     for (;;) {
-        const int it = next_item(counter, &s_item);
+        const int it = next_item(a.counter, &s_item);
         if (it >= n_items) break;
-        const Item wi = items[it];
-        const RomDev R = roms[wi.rom];
+        const Item wi = a.items[it];
+        const RomDev R = a.roms[wi.rom];
         const int n = R.n;
         const double w = R.omega[wi.f];
-        int *s_ipiv = reinterpret_cast<int *>(sm + L.ipiv);
-        bool need64 = !MIXED;
         int steps = 0, info = 0;
         double berr = 0.0;
-        if (MIXED) {
-            float2 *A32 = reinterpret_cast<float2 *>(scratch + (int64_t)blockIdx.x * slot_bytes);
+        bool write_status = true;
+        if constexpr (MIXED) {
+            float2 *A32 = reinterpret_cast<float2 *>(a.scratch + (int64_t)blockIdx.x * a.slot_bytes);
             double2 *X = reinterpret_cast<double2 *>(sm + L.work64);
             float2 *B32 = reinterpret_cast<float2 *>(sm + L.work32);
             int *s_pos = reinterpret_cast<int *>(sm + L.pos);
             int *s_ptot = reinterpret_cast<int *>(sm + L.ptot);
             assemble_into<float2>(A32, n, R, w);
             __syncthreads();
-            factor_global<float2, NB32, RPT>(A32, n, n, ldp, sm, L, nullptr, 0, PL, X32x, s_pivlg);
+            factor_global<float2, NB32, RPT>(A32, n, n, a.ldp, sm, L, nullptr, 0, PL, Xx, s_pivlg);
             info = PL.info;
             for (int l = tid; l < n; l += NT) s_pos[s_ptot[l]] = l;
             __syncthreads();
@@ -697,11 +802,12 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(const RomDev *__restri
                 B32[s_pos[i] + (int64_t)c * n] = make_float2(__double2float_rn(b.x), __double2float_rn(b.y));
             }
             __syncthreads();
-            const double tol_x = tol > 0.0 ? tol : 1.1641532182693481e-10;  // 2^-33
+            const double tol_x = a.tol > 0.0 ? a.tol : 1.1641532182693481e-10;  // 2^-33
             bool conv = false;
+            float2 *tile = reinterpret_cast<float2 *>(sm + L.tile);
             for (int s = 0;; ++s) {
                 if (s > 0) residual64<RPT>(R, w, X, B32, s_pos);
-                lu_solve<float2>(A32, n, n, B32, n, R.r);
+                lu_solve<float2>(A32, n, n, B32, n, R.r, tile);
                 apply_correction(X, B32, n, R.r, s_dx);
                 if (s > 0) {
                     double worst = 0.0;
@@ -710,39 +816,36 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(const RomDev *__restri
                     conv = worst <= tol_x;
                 }
                 steps = s;
-                if (conv || s >= max_refine) break;
+                if (conv || s >= a.max_refine) break;
             }
-            if (conv) {
-                store_solution(X, n, R, wi.f);
-            } else if (fallback) {
-                need64 = true;
-                steps = -1;
+            if (!conv && a.fb_items) {
+                // re-solved by the FP64 kernel that runs after this one; it writes X and status
+                if (tid == 0) a.fb_items[atomicAdd(a.fb_count, 1)] = wi;
+                write_status = false;
             } else {
                 store_solution(X, n, R, wi.f);
-                info = info == 0 ? SROM_INFO_NOT_CONVERGED_DEV : info;
+                if (!conv) info = info == 0 ? SROM_INFO_NOT_CONVERGED_DEV : info;
             }
-            __syncthreads();
-        }
-        if (need64) {
+        } else {
             double2 *A64 = R.LU ? R.LU + (int64_t)wi.f * n * n
-                                : reinterpret_cast<double2 *>(scratch + (int64_t)blockIdx.x * slot_bytes);
+                                : reinterpret_cast<double2 *>(a.scratch + (int64_t)blockIdx.x * a.slot_bytes);
             double2 *B = reinterpret_cast<double2 *>(sm + L.work64);
             assemble_into<double2>(A64, n, R, w);
             load_rhs(B, n, R);
             __syncthreads();
-            factor_global<double2, NB64, RPT>(A64, n, n, ldp, sm, L, B, R.r, PL, X64x, s_pivlg);
+            factor_global<double2, NB64, RPT>(A64, n, n, a.ldp, sm, L, B, R.r, PL, Xx, s_pivlg);
             info = PL.info;
-            lu_solve<double2>(A64, n, n, B, n, R.r);
+            lu_solve<double2>(A64, n, n, B, n, R.r, reinterpret_cast<double2 *>(sm + L.tile));
             store_solution(B, n, R, wi.f);
-            if (!MIXED) berr = 0.0;
+            steps = a.steps_value;
+            if (R.ipiv)
+                for (int j = tid; j < n; j += NT) R.ipiv[(int64_t)wi.f * n + j] = s_ipiv[j];
         }
-        if (tid == 0) {
+        if (tid == 0 && write_status) {
             if (R.info) R.info[wi.f] = info;
             if (R.steps) R.steps[wi.f] = steps;
             if (R.berr) R.berr[wi.f] = berr;
         }
-        if (R.ipiv && need64)
-            for (int j = tid; j < n; j += NT) R.ipiv[(int64_t)wi.f * n + j] = s_ipiv[j];
         __syncthreads();
     }
 }
@@ -779,44 +882,45 @@ int fp64_smem_blocks_per_sm(size_t smem) {
 }
 
 template <bool MIXED, int RPT>
-static cudaError_t launch_global_t(const RomDev *roms, const Item *items, int n_items, int *counter,
-                                   void *scratch, int64_t slot_bytes, int n_max, int r_max, int grid,
-                                   int max_refine, double tol, int fallback, cudaStream_t st) {
+static cudaError_t launch_global_t(const GlobalArgs &a, int grid, cudaStream_t st) {
     auto k = sweep_global_kernel<MIXED, RPT>;
-    const size_t smem = global_smem_bytes(n_max, r_max);
+    const size_t smem = global_smem_bytes(a.n_max, a.r_max);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k<<<grid, NT, smem, st>>>(roms, items, n_items, counter, static_cast<unsigned char *>(scratch), slot_bytes,
-                              n_max | 1, n_max, r_max, max_refine, tol, fallback);
+    k<<<grid, NT, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_global(bool mixed, const RomDev *roms, const Item *items, int n_items, int *counter,
-                          void *scratch, int64_t slot_bytes, int n_max, int r_max, int grid,
-                          int max_refine, double tol, int fallback, cudaStream_t st) {
-    const int rpt = global_rpt(n_max);
-    if (r_max > RMAX_MIXED && mixed) return cudaErrorInvalidValue;
-#define SROM_LG(M, RP)                                                                               \
-    return launch_global_t<M, RP>(roms, items, n_items, counter, scratch, slot_bytes, n_max, r_max, grid, \
-                                  max_refine, tol, fallback, st)
+cudaError_t launch_global(bool mixed, const GlobalArgs &a0, int grid, cudaStream_t st) {
+    GlobalArgs a = a0;
+    a.ldp = a.n_max | 1;
+    const int rpt = global_rpt(a.n_max);
+    if (mixed && a.r_max > RMAX_MIXED) return cudaErrorInvalidValue;
     if (mixed) {
-        if (rpt <= 1) SROM_LG(true, 1);
-        if (rpt == 2) SROM_LG(true, 2);
-        if (rpt == 3) SROM_LG(true, 3);
+        if (rpt <= 1) return launch_global_t<true, 1>(a, grid, st);
+        if (rpt == 2) return launch_global_t<true, 2>(a, grid, st);
+        if (rpt == 3) return launch_global_t<true, 3>(a, grid, st);
     } else {
-        if (rpt <= 1) SROM_LG(false, 1);
-        if (rpt == 2) SROM_LG(false, 2);
-        if (rpt == 3) SROM_LG(false, 3);
+        if (rpt <= 1) return launch_global_t<false, 1>(a, grid, st);
+        if (rpt == 2) return launch_global_t<false, 2>(a, grid, st);
+        if (rpt == 3) return launch_global_t<false, 3>(a, grid, st);
     }
-#undef SROM_LG
     return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_fp64_global(const RomDev *roms, const Item *items, int n_items, int *counter,
                                double2 *scratch, int64_t slot_elems, int n_max, int r_max, int grid,
                                cudaStream_t st) {
-    return launch_global(false, roms, items, n_items, counter, scratch, slot_elems * (int64_t)sizeof(double2),
-                         n_max, r_max, grid, 0, 0.0, 0, st);
+    GlobalArgs a{};
+    a.roms = roms;
+    a.items = items;
+    a.n_items = n_items;
+    a.counter = counter;
+    a.scratch = reinterpret_cast<unsigned char *>(scratch);
+    a.slot_bytes = slot_elems * (int64_t)sizeof(double2);
+    a.n_max = n_max;
+    a.r_max = r_max;
+    return launch_global(false, a, grid, st);
 }
 
 }  // namespace srom

@@ -21,10 +21,24 @@ int global_rpt(int n_max);
 constexpr int GLOBAL_MAX_RPT = 3;
 constexpr int MIXED_MAX_R = 16;
 constexpr size_t GLOBAL_STATIC_SMEM = 4096;
+// Arguments of the global-storage kernels.
+struct GlobalArgs {
+    const RomDev *roms;
+    const Item *items;
+    int n_items;
+    const int *n_items_dev;  // when non-null, the item count is read from device memory
+    int *counter;            // work counter (zero before the launch)
+    unsigned char *scratch;  // one slot of slot_bytes per CTA
+    int64_t slot_bytes;
+    int ldp, n_max, r_max;
+    int max_refine;
+    double tol;
+    Item *fb_items;  // mixed: non-converged systems are appended here (null: keep the last iterate)
+    int *fb_count;
+    int steps_value;  // FP64: value stored in steps (0; -1 when re-solving mixed fallbacks)
+};
 // Global-storage kernel, FP64 (mixed = false) or complex-FP32 factors + FP64 refinement.
-cudaError_t launch_global(bool mixed, const RomDev *roms, const Item *items, int n_items, int *counter,
-                          void *scratch, int64_t slot_bytes, int n_max, int r_max, int grid,
-                          int max_refine, double tol, int fallback, cudaStream_t st);
+cudaError_t launch_global(bool mixed, const GlobalArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_fp64_global(const RomDev *roms, const Item *items, int n_items, int *counter,
                                double2 *scratch, int64_t slot_elems, int n_max, int r_max,
                                int grid, cudaStream_t st);
