@@ -123,6 +123,30 @@ SROM_API int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, c
 SROM_API int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts);
 
 /*
+ * ROM projection R_m = V^T A_m V for up to three sparse FE matrices A_m (K, M, D) that share
+ * one CSR pattern -- the real-valued form of generateROM (KrylovROMSubstructure.cpp:709-765:
+ * mkl_sparse_z_mm for Y = A V, MathLibrary.cpp:491-532, then cblas_zgemm ConjTrans for
+ * V^H Y, MathLibrary.cpp:177-234).  CSR: n_rows rows, rowptr[n_rows+1] (int64), colind
+ * (int32), base 0 or 1 (the reference uses 1); upper != 0 means only the upper triangle of a
+ * symmetric matrix is stored (the reference's SPARSE_FILL_MODE_UPPER, MathLibrary.cpp:502-507).
+ * vals: host array of n_mats device pointers to the value arrays.  V: n_rows x k
+ * column-major (ldv), k <= 128.  R: host array of n_mats device pointers, each k x k
+ * column-major.  Summation order is fixed (deterministic results).
+ */
+SROM_API int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *rowptr, const int *colind, int base,
+                               int upper, const double *const *vals, int n_mats, const double *V, int k, int64_t ldv,
+                               double *const *R);
+
+/*
+ * FP64 Gram-Schmidt orthonormalisation of V (n_rows x k, column-major, ldv) in place:
+ * each column is projected out of the previous ones `passes` times (classical projections,
+ * two passes keep the basis orthonormal to rounding level) and normalised -- the column-wise
+ * form of the reference's block Gram-Schmidt with re-orthogonalisation
+ * (KrylovROMSubstructure.cpp:433-454, :513-534).
+ */
+SROM_API int srom_orthonormalize(srom_handle *h, double *V, int64_t n_rows, int k, int64_t ldv, int passes);
+
+/*
  * FP64 sweep of one ROM that allocates no device memory.  No counterpart in the reference.
  * For callers that cannot let a library allocate: programs that own all device memory
  * through their own pool, or real-time loops in which cudaMalloc's implicit synchronisation

@@ -32,7 +32,7 @@ SROM_INFO_NOT_CONVERGED = -1
 EXPORTS = [
     "srom_create", "srom_destroy", "srom_set_stream", "srom_status_string", "srom_last_error",
     "srom_version", "srom_sweep", "srom_sweep_host", "srom_profile_enable", "srom_profile_read",
-    "srom_sweep_fp64_noalloc",
+    "srom_sweep_fp64_noalloc", "srom_project_real", "srom_orthonormalize",
 ]
 
 
@@ -90,6 +90,11 @@ def lib() -> C.CDLL:
         L.srom_profile_enable.restype = i
         L.srom_profile_read.argtypes = [vp, C.POINTER(KernelTime), i, C.POINTER(C.c_int)]
         L.srom_profile_read.restype = i
+        L.srom_project_real.argtypes = [vp, C.c_int64, vp, vp, i, i, C.POINTER(C.c_void_p), i, vp, i,
+                                        C.c_int64, C.POINTER(C.c_void_p)]
+        L.srom_project_real.restype = i
+        L.srom_orthonormalize.argtypes = [vp, vp, C.c_int64, i, C.c_int64, i]
+        L.srom_orthonormalize.restype = i
         L.srom_sweep_fp64_noalloc.argtypes = [C.POINTER(RomDesc), vp, C.c_char_p, i]
         L.srom_sweep_fp64_noalloc.restype = i
         for name in ("srom_sweep", "srom_sweep_host"):

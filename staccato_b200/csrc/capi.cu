@@ -12,6 +12,7 @@
 
 #include "../../include/staccato_rom.h"
 #include "srom_device.cuh"
+#include "project_kernels.h"
 #include "sweep_kernels.h"
 
 using srom::Item;
@@ -35,6 +36,9 @@ struct srom_handle {
     // device buffers used by srom_sweep_host
     void *d_host_arena = nullptr;
     size_t d_host_arena_bytes = 0;
+    // projection / Gram-Schmidt scratch
+    void *d_proj = nullptr;
+    size_t d_proj_bytes = 0;
     // per-launch profiling
     struct ProfRec {
         std::string name;
@@ -235,6 +239,7 @@ int srom_destroy(srom_handle *h) {
     if (h->scratch) cudaFree(h->scratch);
     if (h->d_meta) cudaFree(h->d_meta);
     if (h->d_host_arena) cudaFree(h->d_host_arena);
+    if (h->d_proj) cudaFree(h->d_proj);
     if (h->h_meta) cudaFreeHost(h->h_meta);
     if (h->meta_done) cudaEventDestroy(h->meta_done);
     for (auto &r : h->recs) {
@@ -429,6 +434,71 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
             SROM_CUDA(h, srom::launch_global(false, b, (int)grid, h->stream));
         }
     }
+    return SROM_OK;
+}
+
+int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *rowptr, const int *colind, int base, int upper,
+                      const double *const *vals, int n_mats, const double *V, int k, int64_t ldv, double *const *R) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    if (n_rows < 0 || k < 0) return set_err(h, SROM_ERR_INVALID, "negative size");
+    if (n_mats < 1 || n_mats > 3) return set_err(h, SROM_ERR_INVALID, "n_mats must be 1..3");
+    if (k > 128) return set_err(h, SROM_ERR_UNSUPPORTED, "k = %d exceeds 128", k);
+    if (base != 0 && base != 1) return set_err(h, SROM_ERR_INVALID, "base must be 0 or 1");
+    if (!vals || !R) return set_err(h, SROM_ERR_INVALID, "vals and R must be non-null");
+    for (int m = 0; m < n_mats; ++m)
+        if (!vals[m] || !R[m]) return set_err(h, SROM_ERR_INVALID, "vals[%d] / R[%d] is null", m, m);
+    if (n_rows == 0 || k == 0) return SROM_OK;
+    if (!rowptr || !colind || !V) return set_err(h, SROM_ERR_INVALID, "rowptr, colind and V must be non-null");
+    if (ldv < n_rows) return set_err(h, SROM_ERR_INVALID, "ldv < n_rows");
+    DeviceGuard g(h->device);
+    const int kp = (k + 7) & ~7;
+    const int nblk = h->sm_count * 2;
+    const size_t vt_b = align_up(sizeof(double) * (size_t)n_rows * k, 256);
+    const size_t y_b = align_up(sizeof(double) * (size_t)n_rows * k * n_mats, 256);
+    const size_t p_b = align_up(sizeof(double) * (size_t)nblk * n_mats * kp * kp, 256);
+    int s = ensure_device_buffer(h, &h->d_proj, &h->d_proj_bytes, vt_b + y_b + p_b);
+    if (s) return s;
+    char *base_p = static_cast<char *>(h->d_proj);
+    double *Vt = reinterpret_cast<double *>(base_p);
+    double *Y = reinterpret_cast<double *>(base_p + vt_b);
+    double *part = reinterpret_cast<double *>(base_p + vt_b + y_b);
+    srom::ProjVals pv{};
+    srom::ProjOut po{};
+    for (int m = 0; m < n_mats; ++m) {
+        pv.v[m] = vals[m];
+        po.r[m] = R[m];
+    }
+    SROM_CUDA(h, srom::launch_transpose(V, n_rows, k, ldv, Vt, h->stream));
+    {
+        ProfScope ps(h, "spmm", n_rows, 0.0, 0.0);
+        SROM_CUDA(h, srom::launch_spmm(n_rows, rowptr, colind, base, upper, pv, n_mats, Vt, k, Y,
+                                       (int64_t)n_rows * k, h->sm_count, h->stream));
+    }
+    {
+        ProfScope ps(h, "vty_dmma", n_rows, 2.0 * (double)n_rows * k * k * n_mats, 0.0);
+        SROM_CUDA(h, srom::launch_vty(n_rows, k, Vt, Y, (int64_t)n_rows * k, n_mats, nblk, part, po, h->stream));
+    }
+    return SROM_OK;
+}
+
+int srom_orthonormalize(srom_handle *h, double *V, int64_t n_rows, int k, int64_t ldv, int passes) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    if (n_rows < 0 || k < 0 || passes < 0) return set_err(h, SROM_ERR_INVALID, "negative size");
+    if (n_rows == 0 || k == 0) return SROM_OK;
+    if (!V) return set_err(h, SROM_ERR_INVALID, "V is null");
+    if (ldv < n_rows) return set_err(h, SROM_ERR_INVALID, "ldv < n_rows");
+    if (k > n_rows) return set_err(h, SROM_ERR_INVALID, "k > n_rows: columns cannot be orthonormal");
+    DeviceGuard g(h->device);
+    const int nblk = h->sm_count;
+    const size_t need = sizeof(double) * ((size_t)nblk * (k + 1) + (k + 1));
+    int s = ensure_device_buffer(h, &h->d_proj, &h->d_proj_bytes, need);
+    if (s) return s;
+    double *part = static_cast<double *>(h->d_proj);
+    double *hv = part + (size_t)nblk * (k + 1);
+    ProfScope ps(h, "gram_schmidt", k, 4.0 * (double)n_rows * k * k * std::max(passes, 1), 0.0);
+    SROM_CUDA(h, srom::launch_gram_schmidt(V, n_rows, k, ldv, passes, part, hv, nblk, h->stream));
     return SROM_OK;
 }
 

@@ -1,0 +1,27 @@
+// Host-side entry points of the projection kernels (used by the C ABI in capi.cu).
+#pragma once
+
+#include <algorithm>
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace srom {
+
+struct ProjVals {
+    const double *v[3];
+};
+struct ProjOut {
+    double *r[3];
+};
+
+cudaError_t launch_transpose(const double *V, int64_t N, int k, int64_t ldv, double *Vt, cudaStream_t st);
+cudaError_t launch_spmm(int64_t N, const int64_t *rowptr, const int *colind, int base, int upper, ProjVals vals,
+                        int n_mats, const double *Vt, int k, double *Y, int64_t y_stride, int sms, cudaStream_t st);
+size_t vty_smem_bytes(int k, int n_mats);
+cudaError_t launch_vty(int64_t N, int k, const double *Vt, const double *Y, int64_t y_stride, int n_mats, int nblk,
+                       double *partial, ProjOut out, cudaStream_t st);
+cudaError_t launch_gram_schmidt(double *V, int64_t N, int k, int64_t ldv, int passes, double *part, double *h,
+                                int nblk, cudaStream_t st);
+
+}  // namespace srom

@@ -1,0 +1,84 @@
+"""``KrylovROMSubstructure``: the reference's ROM interface on the B200 kernels.
+
+Mirrors the two members of STACCATO's ``KrylovROMSubstructure`` that form the hot path
+(src/analysis/KrylovROMSubstructure.h:156, .cpp:709-765 and :1393-1460):
+
+* ``generate_rom(K, M, V, D=None, B=None, C=None)`` -- project the sparse FE operators onto
+  the basis: K_r = V^T K V, M_r = V^T M V (D_r = V^T D V), B_r = V^T B, C_r = C V;
+* ``back_transform_kmor(freq_hz, input_load)`` -- for every frequency assemble
+  A(w) = K_r - w^2 M_r + i w D_r (w = 2 pi f), solve A x = B_r F and return
+  y = C_r x stacked per frequency, like the reference's results vector.
+
+Matrices are torch tensors on the handle's device; results stay on the device.  The
+reduced operators are complex128 like the reference's ``myKComplexReduced`` etc.
+"""
+from __future__ import annotations
+
+import math
+from typing import Optional
+
+import numpy as np
+
+from . import _capi
+from .project import DeviceCsr, orthonormalize, project
+from .sweep import DeviceRom, sweep
+
+
+class KrylovROMSubstructure:
+    def __init__(self, device: int = 0, handle: Optional[_capi.Handle] = None):
+        self.handle = handle or _capi.Handle(device)
+        self.device = device
+        self.K_r = self.M_r = self.D_r = self.B_r = self.C_r = None
+        self.eta = 0.0
+
+    # --------------------------------------------------------------- reduced operators
+    def set_reduced(self, K_r, M_r, D_r=None, B_r=None, C_r=None, eta: float = 0.0):
+        """Install reduced operators (numpy or torch, n x n complex) directly."""
+        import torch
+
+        dev = torch.device("cuda", self.device)
+        c = lambda a: None if a is None else torch.as_tensor(a, dtype=torch.complex128, device=dev)
+        self.K_r, self.M_r, self.D_r, self.B_r, self.C_r = c(K_r), c(M_r), c(D_r), c(B_r), c(C_r)
+        self.eta = float(eta)
+
+    def generate_rom(self, csr: DeviceCsr, K_vals, M_vals, V, D_vals=None, B=None, C=None, eta: float = 0.0):
+        """Projection of the FE operators (real, sharing the CSR pattern) onto V.
+
+        V: (k, n) float64 tensor = n x k column-major basis.  B: n x n_in, C: n_out x n."""
+        import torch
+
+        mats = [K_vals, M_vals] + ([D_vals] if D_vals is not None else [])
+        R = project(self.handle, csr, mats, V)
+        to_c = lambda r: r.to(torch.complex128)
+        self.K_r, self.M_r = to_c(R[0]), to_c(R[1])
+        self.D_r = to_c(R[2]) if D_vals is not None else None
+        Vcm = V.t()  # n x k view
+        self.B_r = None if B is None else (Vcm.t().to(torch.complex128) @ torch.as_tensor(B, device=V.device).to(torch.complex128))
+        self.C_r = None if C is None else (torch.as_tensor(C, device=V.device).to(torch.complex128) @ Vcm.to(torch.complex128))
+        self.eta = float(eta)
+        return R
+
+    # --------------------------------------------------------------- frequency sweep
+    def back_transform_kmor(self, freq_hz, input_load, precision: int = _capi.SROM_FP64,
+                            flags: int = _capi.SROM_FLAG_FALLBACK_FP64, max_refine: int = 5):
+        """y(w) = C_r A(w)^-1 B_r F per frequency; returns (Y, info) with Y of shape
+        (F, n_out, r) (x itself when C_r is None)."""
+        import torch
+
+        freq = np.asarray(freq_hz, dtype=np.float64)
+        omega = 2.0 * math.pi * freq
+        F_load = torch.as_tensor(input_load, dtype=torch.complex128, device=self.K_r.device)
+        if F_load.ndim == 1:
+            F_load = F_load[:, None]
+        rhs = F_load if self.B_r is None else self.B_r @ F_load
+        n, r = int(rhs.shape[0]), int(rhs.shape[1])
+        rom = DeviceRom(n=n, r=r, F=len(omega),
+                        K=self.K_r.t().contiguous().reshape(-1), M=self.M_r.t().contiguous().reshape(-1),
+                        D=None if self.D_r is None else self.D_r.t().contiguous().reshape(-1),
+                        rhs=rhs.t().contiguous().reshape(-1),
+                        omega=torch.as_tensor(omega, device=self.K_r.device), eta=self.eta)
+        rom.allocate_outputs(self.K_r.device)
+        sweep(self.handle, [rom], precision=precision, flags=flags, max_refine=max_refine)
+        X = rom.X.reshape(rom.F, r, n).transpose(1, 2)  # (F, n, r)
+        Y = X if self.C_r is None else torch.matmul(self.C_r, X)
+        return Y, rom.info

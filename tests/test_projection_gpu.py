@@ -1,0 +1,113 @@
+"""Projection R = V^T A V (SpMM + FP64 tensor-core GEMM) and Gram-Schmidt on the GPU,
+against the CPU oracle (oracle/srom_oracle.c: CSR SpMM, V^T Y, modified Gram-Schmidt)."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from oracle import oracle as O
+from staccato_b200 import _capi, fe_tet10
+from staccato_b200.project import DeviceCsr, orthonormalize, project
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_sym_csr(n, density, seed):
+    rng = np.random.default_rng(seed)
+    A = sp.random(n, n, density=density, random_state=seed, format="csr")
+    A = (A + A.T + sp.eye(n) * 3.0).tocsr()
+    A.sort_indices()
+    B = sp.random(n, n, density=density, random_state=seed + 1, format="csr")
+    B = (B + B.T + sp.eye(n)).tocsr()
+    # same pattern for both values: use A's pattern with B's values resampled
+    Bv = rng.standard_normal(A.nnz)
+    Bm = sp.csr_matrix((Bv, A.indices, A.indptr), shape=A.shape)
+    Bm = ((Bm + Bm.T) * 0.5).tocsr()
+    Bm = sp.csr_matrix((np.asarray(Bm[A.nonzero()]).ravel(), A.indices, A.indptr), shape=A.shape)
+    return A, Bm
+
+
+def _dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("k", [1, 8, 33, 96, 128])
+@pytest.mark.parametrize("base,upper", [(0, False), (1, False), (1, True)])
+def test_projection_random(handle, k, base, upper):
+    n = 1500
+    A, B = _rand_sym_csr(n, 0.01, 7 + k)
+    rng = np.random.default_rng(k)
+    V = np.asfortranarray(rng.standard_normal((n, k)))
+    if upper:
+        Au, Bu = sp.triu(A).tocsr(), sp.triu(B).tocsr()
+        Au.sort_indices()
+        Bu = sp.csr_matrix((np.asarray(B[Au.nonzero()]).ravel(), Au.indices, Au.indptr), shape=A.shape)
+        indptr, indices, va, vb = Au.indptr, Au.indices, Au.data, Bu.data
+    else:
+        indptr, indices, va, vb = A.indptr, A.indices, A.data, B.data
+    csr = DeviceCsr.from_host(indptr.astype(np.int64) + base, indices.astype(np.int32) + base, base=base, upper=upper)
+    Vt = _dev(np.ascontiguousarray(V.T))
+    RA, RB = project(handle, csr, [_dev(va), _dev(vb)], Vt)
+    refA = O.project(indptr, indices, va, V, upper=upper)
+    refB = O.project(indptr, indices, vb, V, upper=upper)
+    for R, ref in ((RA, refA), (RB, refB)):
+        R = R.cpu().numpy()
+        assert np.abs(R - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_projection_identity_basis_extracts_block(handle):
+    n, k = 400, 24
+    A, B = _rand_sym_csr(n, 0.05, 3)
+    V = np.zeros((n, k), order="F")
+    V[np.arange(k), np.arange(k)] = 1.0
+    csr = DeviceCsr.from_host(A.indptr, A.indices)
+    (RA,) = project(handle, csr, [_dev(A.data)], _dev(np.ascontiguousarray(V.T)))
+    assert np.array_equal(RA.cpu().numpy(), A.toarray()[:k, :k])
+
+
+@pytest.fixture(scope="module")
+def block_model():
+    return fe_tet10.clamped_block()
+
+
+def test_projection_tet10_block(handle, block_model):
+    m = block_model
+    V = O.mgs(fe_tet10.basis(m.n_dof, 96, seed=1), passes=2)
+    csr = DeviceCsr.from_host(m.indptr, m.indices)
+    Kr, Mr = project(handle, csr, [_dev(m.K), _dev(m.M)], _dev(np.ascontiguousarray(V.T)))
+    refK = O.project(m.indptr, m.indices, m.K, V)
+    refM = O.project(m.indptr, m.indices, m.M, V)
+    Kr, Mr = Kr.cpu().numpy(), Mr.cpu().numpy()
+    assert np.abs(Kr - refK).max() <= 1e-12 * np.abs(refK).max()
+    assert np.abs(Mr - refM).max() <= 1e-12 * np.abs(refM).max()
+    # size-independent properties: symmetry and positive semi-definiteness of the projections
+    assert np.abs(Kr - Kr.T).max() <= 1e-12 * np.abs(Kr).max()
+    assert np.linalg.eigvalsh(0.5 * (Mr + Mr.T)).min() > 0
+
+
+@pytest.mark.parametrize("n,k", [(64, 1), (1000, 17), (20000, 96)])
+def test_gram_schmidt_matches_mgs(handle, n, k):
+    import torch
+
+    V0 = np.asfortranarray(np.random.default_rng(n + k).standard_normal((n, k)))
+    Vt = _dev(np.ascontiguousarray(V0.T))
+    orthonormalize(handle, Vt, passes=2)
+    torch.cuda.synchronize()
+    Vg = Vt.cpu().numpy().T
+    Vo = O.mgs(V0, passes=2)
+    assert np.abs(Vg - Vo).max() <= 1e-12
+    assert np.abs(Vg.T @ Vg - np.eye(k)).max() <= 1e-13
+
+
+def test_gram_schmidt_full_basis(handle, block_model):
+    import torch
+
+    V0 = fe_tet10.basis(block_model.n_dof, 96, seed=1)
+    Vt = _dev(np.ascontiguousarray(V0.T))
+    orthonormalize(handle, Vt, passes=2)
+    torch.cuda.synchronize()
+    Vg = Vt.cpu().numpy().T
+    assert np.abs(Vg.T @ Vg - np.eye(96)).max() <= 1e-13
+    Vo = O.mgs(V0, passes=2)
+    assert np.abs(Vg - Vo).max() <= 1e-12
