@@ -122,6 +122,38 @@ SROM_API int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, c
  */
 SROM_API int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts);
 
+/* ---- adjoint (backward) sweep ---------------------------------------------------------- */
+#define SROM_DPARAM_LOWRANK 0
+#define SROM_DPARAM_DENSE 1
+
+/* Derivative of A(w) with respect to one parameter:
+ *   dA/dp(w) = (c0 + c1 (i w) + c2 (-w^2)) * G,   G = U diag(s) W^T (LOWRANK) or G (DENSE).
+ * A stiffness-scaling parameter of a modal ROM is LOWRANK with U = W = its mode block and
+ * s = the block's eigenvalues, c0 = 1 + i eta; the hysteretic loss factor is DENSE with
+ * G = K and c0 = i; a damping scale is c1 = 1 with G = D; a mass scale is c2 = 1 with G = M. */
+typedef struct {
+    int kind;                /* SROM_DPARAM_LOWRANK or SROM_DPARAM_DENSE        */
+    int rank;                /* LOWRANK: number of columns of U (and W)          */
+    const srom_complex *U;   /* LOWRANK: n x rank (ld n)                         */
+    const srom_complex *W;   /* LOWRANK: n x rank (ld n) or NULL for W = U       */
+    const double *s;         /* LOWRANK: rank scales or NULL (ones)              */
+    const srom_complex *G;   /* DENSE: n x n (ld n)                              */
+    srom_complex c0, c1, c2; /* frequency polynomial of the derivative           */
+} srom_dparam;
+
+/*
+ * Backward call of the FP64 sweep (no counterpart in the reference, which has no adjoint).
+ * rom must come from srom_sweep with SROM_FLAG_KEEP_FACTORS (rom->LU, rom->ipiv, rom->X).
+ * gbar: F blocks of n x r cotangents (leading dimension ldg, block stride ldg * r),
+ * gbar_f = 2 dJ/d conj(x_f) for a real objective J.  For each frequency the kernel solves
+ * A^H lambda = gbar_f with the kept factors and accumulates
+ *     dJdp[j] = sum_f -Re( sum_c lambda_c^H dA_j(w_f) x_c ).
+ * params: host array of n_params descriptors whose U/W/s/G are device pointers.
+ * dJdp: n_params doubles (device).  lambda: F blocks of n x r (device) or NULL.
+ */
+SROM_API int srom_sweep_backward(srom_handle *h, const srom_rom_desc *rom, const srom_complex *gbar, int ldg,
+                                 const srom_dparam *params, int n_params, double *dJdp, srom_complex *lambda);
+
 /*
  * ROM projection R_m = V^T A_m V for up to three sparse FE matrices A_m (K, M, D) that share
  * one CSR pattern -- the real-valued form of generateROM (KrylovROMSubstructure.cpp:709-765:

@@ -32,8 +32,20 @@ SROM_INFO_NOT_CONVERGED = -1
 EXPORTS = [
     "srom_create", "srom_destroy", "srom_set_stream", "srom_status_string", "srom_last_error",
     "srom_version", "srom_sweep", "srom_sweep_host", "srom_profile_enable", "srom_profile_read",
-    "srom_sweep_fp64_noalloc", "srom_project_real", "srom_orthonormalize",
+    "srom_sweep_fp64_noalloc", "srom_project_real", "srom_orthonormalize", "srom_sweep_backward",
 ]
+
+SROM_DPARAM_LOWRANK = 0
+SROM_DPARAM_DENSE = 1
+
+
+class Complex(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+class DParam(C.Structure):
+    _fields_ = [("kind", C.c_int), ("rank", C.c_int), ("U", C.c_void_p), ("W", C.c_void_p),
+                ("s", C.c_void_p), ("G", C.c_void_p), ("c0", Complex), ("c1", Complex), ("c2", Complex)]
 
 
 class KernelTime(C.Structure):
@@ -95,6 +107,8 @@ def lib() -> C.CDLL:
         L.srom_project_real.restype = i
         L.srom_orthonormalize.argtypes = [vp, vp, C.c_int64, i, C.c_int64, i]
         L.srom_orthonormalize.restype = i
+        L.srom_sweep_backward.argtypes = [vp, C.POINTER(RomDesc), vp, i, C.POINTER(DParam), i, vp, vp]
+        L.srom_sweep_backward.restype = i
         L.srom_sweep_fp64_noalloc.argtypes = [C.POINTER(RomDesc), vp, C.c_char_p, i]
         L.srom_sweep_fp64_noalloc.restype = i
         for name in ("srom_sweep", "srom_sweep_host"):

@@ -12,6 +12,7 @@
 
 #include "../../include/staccato_rom.h"
 #include "srom_device.cuh"
+#include "adjoint_kernels.h"
 #include "project_kernels.h"
 #include "sweep_kernels.h"
 
@@ -39,6 +40,9 @@ struct srom_handle {
     // projection / Gram-Schmidt scratch
     void *d_proj = nullptr;
     size_t d_proj_bytes = 0;
+    // adjoint descriptors + partials
+    void *d_adj = nullptr;
+    size_t d_adj_bytes = 0;
     // per-launch profiling
     struct ProfRec {
         std::string name;
@@ -240,6 +244,7 @@ int srom_destroy(srom_handle *h) {
     if (h->d_meta) cudaFree(h->d_meta);
     if (h->d_host_arena) cudaFree(h->d_host_arena);
     if (h->d_proj) cudaFree(h->d_proj);
+    if (h->d_adj) cudaFree(h->d_adj);
     if (h->h_meta) cudaFreeHost(h->h_meta);
     if (h->meta_done) cudaEventDestroy(h->meta_done);
     for (auto &r : h->recs) {
@@ -479,6 +484,92 @@ int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *rowptr, con
         ProfScope ps(h, "vty_dmma", n_rows, 2.0 * (double)n_rows * k * k * n_mats, 0.0);
         SROM_CUDA(h, srom::launch_vty(n_rows, k, Vt, Y, (int64_t)n_rows * k, n_mats, nblk, part, po, h->stream));
     }
+    return SROM_OK;
+}
+
+int srom_sweep_backward(srom_handle *h, const srom_rom_desc *rom, const srom_complex *gbar, int ldg,
+                        const srom_dparam *params, int n_params, double *dJdp, srom_complex *lambda) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    if (!rom) return set_err(h, SROM_ERR_INVALID, "rom is null");
+    int s = validate_desc(h, *rom, 0);
+    if (s) return s;
+    if (n_params < 0 || (n_params > 0 && (!params || !dJdp)))
+        return set_err(h, SROM_ERR_INVALID, "params and dJdp must be non-null");
+    if (rom->n == 0 || rom->F == 0 || rom->r == 0 || n_params == 0) {
+        if (n_params > 0) SROM_CUDA(h, cudaMemsetAsync(dJdp, 0, sizeof(double) * n_params, h->stream));
+        return SROM_OK;
+    }
+    if (!rom->LU || !rom->ipiv) return set_err(h, SROM_ERR_INVALID, "rom->LU / rom->ipiv missing: run srom_sweep with SROM_FLAG_KEEP_FACTORS");
+    if (!gbar || ldg < rom->n) return set_err(h, SROM_ERR_INVALID, "gbar null or ldg < n");
+    std::vector<srom::DParamDev> pd(n_params);
+    std::vector<srom::DParamTerm> terms;
+    for (int j = 0; j < n_params; ++j) {
+        const srom_dparam &p = params[j];
+        srom::DParamDev &d = pd[j];
+        d.kind = p.kind;
+        d.rank = p.rank;
+        d.U = reinterpret_cast<const double2 *>(p.U);
+        d.W = reinterpret_cast<const double2 *>(p.W);
+        d.s = p.s;
+        d.G = reinterpret_cast<const double2 *>(p.G);
+        d.c0 = make_double2(p.c0.re, p.c0.im);
+        d.c1 = make_double2(p.c1.re, p.c1.im);
+        d.c2 = make_double2(p.c2.re, p.c2.im);
+        d.term0 = (int)terms.size();
+        if (p.kind == SROM_DPARAM_LOWRANK) {
+            if (p.rank < 0 || (p.rank > 0 && !p.U)) return set_err(h, SROM_ERR_INVALID, "param %d: U missing", j);
+            for (int k = 0; k < p.rank; ++k) terms.push_back({j, k});
+        } else if (p.kind == SROM_DPARAM_DENSE) {
+            if (!p.G) return set_err(h, SROM_ERR_INVALID, "param %d: G missing", j);
+            terms.push_back({j, 0});
+        } else {
+            return set_err(h, SROM_ERR_INVALID, "param %d: unknown kind %d", j, p.kind);
+        }
+        d.nterm = (int)terms.size() - d.term0;
+    }
+    const size_t smem = srom::adjoint_smem_bytes(rom->n, rom->r, (int)terms.size());
+    if (smem > (size_t)h->max_smem_optin) return set_err(h, SROM_ERR_UNSUPPORTED, "n*r or parameter terms too large");
+    DeviceGuard g(h->device);
+    const size_t o_rom = 0, o_par = align_up(sizeof(RomDev), 256);
+    const size_t o_term = o_par + align_up(sizeof(srom::DParamDev) * n_params, 256);
+    const size_t o_ctr = o_term + align_up(sizeof(srom::DParamTerm) * std::max<size_t>(terms.size(), 1), 256);
+    const size_t o_part = o_ctr + 256;
+    const size_t total = o_part + sizeof(double) * (size_t)rom->F * n_params;
+    if (h->meta_pending) {
+        SROM_CUDA(h, cudaEventSynchronize(h->meta_done));
+        h->meta_pending = false;
+    }
+    s = ensure_host_pinned(h, o_part);
+    if (s) return s;
+    s = ensure_device_buffer(h, &h->d_adj, &h->d_adj_bytes, total);
+    if (s) return s;
+    char *hm = static_cast<char *>(h->h_meta);
+    RomDev rd = to_dev(*rom);
+    memcpy(hm + o_rom, &rd, sizeof rd);
+    memcpy(hm + o_par, pd.data(), sizeof(srom::DParamDev) * n_params);
+    if (!terms.empty()) memcpy(hm + o_term, terms.data(), sizeof(srom::DParamTerm) * terms.size());
+    memset(hm + o_ctr, 0, 256);
+    char *dm = static_cast<char *>(h->d_adj);
+    SROM_CUDA(h, cudaMemcpyAsync(dm, hm, o_part, cudaMemcpyHostToDevice, h->stream));
+    SROM_CUDA(h, cudaEventRecord(h->meta_done, h->stream));
+    h->meta_pending = true;
+    srom::AdjointArgs a{};
+    a.rom = reinterpret_cast<const RomDev *>(dm + o_rom);
+    a.gbar = reinterpret_cast<const double2 *>(gbar);
+    a.ldg = ldg;
+    a.ldg_f = (int64_t)ldg * rom->r;
+    a.params = reinterpret_cast<const srom::DParamDev *>(dm + o_par);
+    a.n_params = n_params;
+    a.terms = reinterpret_cast<const srom::DParamTerm *>(dm + o_term);
+    a.n_terms = (int)terms.size();
+    a.partial = reinterpret_cast<double *>(dm + o_part);
+    a.lambda = reinterpret_cast<double2 *>(lambda);
+    a.counter = reinterpret_cast<int *>(dm + o_ctr);
+    const int grid = std::min(rom->F, h->sm_count * 4);
+    const double n3 = (double)rom->n * rom->n;
+    ProfScope ps(h, "adjoint", rom->F, (8.0 * n3 * rom->r) * rom->F, 0.0);
+    SROM_CUDA(h, srom::launch_adjoint(a, rom->n, rom->r, rom->F, grid, dJdp, h->stream));
     return SROM_OK;
 }
 
