@@ -122,6 +122,29 @@ SROM_API int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, c
  */
 SROM_API int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts);
 
+/* ---- captured sweeps and tuning ------------------------------------------------------- */
+typedef struct srom_graph srom_graph;
+
+/*
+ * Plan a sweep over the given ROMs once (classification, cost-ordered work lists, scratch)
+ * and capture its launches into a CUDA graph owned by the returned object; every
+ * srom_graph_launch replays the whole batched sweep (all ROMs, all frequencies) on the
+ * given stream with no host work.  The descriptors' device pointers must stay valid while
+ * the graph exists; their contents may change between launches.
+ */
+SROM_API int srom_graph_create(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts,
+                               srom_graph **graph);
+SROM_API int srom_graph_launch(srom_graph *graph, void *cuda_stream);
+SROM_API int srom_graph_destroy(srom_graph *graph);
+
+/*
+ * Autotune the FP64 kernel choice (whole system in shared memory vs. blocked LU in global
+ * scratch) for each order in n_values with r right-hand sides: both are timed on a synthetic
+ * system and the faster is used by later sweeps on this handle.  cache_path (or NULL) is a
+ * JSON file of earlier choices for this device, read first and rewritten with new entries.
+ */
+SROM_API int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char *cache_path);
+
 /* ---- adjoint (backward) sweep ---------------------------------------------------------- */
 #define SROM_DPARAM_LOWRANK 0
 #define SROM_DPARAM_DENSE 1

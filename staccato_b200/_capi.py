@@ -33,6 +33,7 @@ EXPORTS = [
     "srom_create", "srom_destroy", "srom_set_stream", "srom_status_string", "srom_last_error",
     "srom_version", "srom_sweep", "srom_sweep_host", "srom_profile_enable", "srom_profile_read",
     "srom_sweep_fp64_noalloc", "srom_project_real", "srom_orthonormalize", "srom_sweep_backward",
+    "srom_graph_create", "srom_graph_launch", "srom_graph_destroy", "srom_tune",
 ]
 
 SROM_DPARAM_LOWRANK = 0
@@ -107,6 +108,14 @@ def lib() -> C.CDLL:
         L.srom_project_real.restype = i
         L.srom_orthonormalize.argtypes = [vp, vp, C.c_int64, i, C.c_int64, i]
         L.srom_orthonormalize.restype = i
+        L.srom_graph_create.argtypes = [vp, C.POINTER(RomDesc), i, C.POINTER(SweepOpts), pp]
+        L.srom_graph_create.restype = i
+        L.srom_graph_launch.argtypes = [vp, vp]
+        L.srom_graph_launch.restype = i
+        L.srom_graph_destroy.argtypes = [vp]
+        L.srom_graph_destroy.restype = i
+        L.srom_tune.argtypes = [vp, C.POINTER(C.c_int), i, i, C.c_char_p]
+        L.srom_tune.restype = i
         L.srom_sweep_backward.argtypes = [vp, C.POINTER(RomDesc), vp, i, C.POINTER(DParam), i, vp, vp]
         L.srom_sweep_backward.restype = i
         L.srom_sweep_fp64_noalloc.argtypes = [C.POINTER(RomDesc), vp, C.c_char_p, i]

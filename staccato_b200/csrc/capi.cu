@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -52,6 +53,8 @@ struct srom_handle {
     };
     bool prof = false;
     std::vector<ProfRec> recs;
+    // FP64 storage class chosen by srom_tune per (n << 16 | r): 0 smem kernel, 1 global kernel
+    std::map<long long, int> tune_fp64;
     std::vector<cudaEvent_t> event_pool;
     std::string err;
 };
@@ -292,9 +295,37 @@ int srom_profile_read(srom_handle *h, srom_kernel_time *out, int max, int *count
     return SROM_OK;
 }
 
-int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts) {
-    if (!h) return SROM_ERR_INVALID;
-    h->err.clear();
+}  // extern "C"
+
+namespace {
+
+// A validated, classified and ordered sweep: the host image of the device metadata
+// (descriptors, cost-ordered work lists, fallback list, zeroed counters) plus launch shapes.
+struct SweepPlan {
+    bool mixed = false;
+    srom_sweep_opts o{};
+    std::vector<char> meta;
+    size_t off_items0 = 0, off_items1 = 0, off_fb = 0, off_ctr = 0;
+    long long n_items[2] = {0, 0};
+    double flops[2] = {0.0, 0.0};
+    size_t smem_max = 0;
+    int g_nmax = 0, g_rmax = 0;
+    long long grid0 = 0, grid1 = 0;
+    int64_t slot_bytes = 0;
+    bool need_scratch = false;
+};
+
+// FP64 storage class of an n x n system with r right-hand sides: 0 smem kernel, 1 global
+// kernel.  The tuning table (srom_tune) overrides the default "smem when it fits".
+int fp64_class(const srom_handle *h, int n, int r) {
+    const bool fits = srom::fp64_smem_bytes(n, r) <= (size_t)h->max_smem_optin;
+    if (!fits) return 1;
+    auto it = h->tune_fp64.find(((long long)n << 16) | r);
+    if (it != h->tune_fp64.end()) return it->second;
+    return 0;
+}
+
+int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts, SweepPlan &P) {
     if (n_roms < 0 || (n_roms > 0 && !roms)) return set_err(h, SROM_ERR_INVALID, "roms is null");
     srom_sweep_opts o = opts ? *opts : srom_sweep_opts{SROM_FP64, 5, 0.0, 0};
     if (o.precision != SROM_FP64 && o.precision != SROM_MIXED_FP32)
@@ -310,60 +341,57 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
         if (mixed && roms[i].r > srom::MIXED_MAX_R)
             return set_err(h, SROM_ERR_UNSUPPORTED, "rom %d: mixed form supports r <= %d", i, srom::MIXED_MAX_R);
     }
-    DeviceGuard g(h->device);
-
-    // ---- classify and order the work ---------------------------------------------------
-    // FP64: systems that fit shared memory use the smem kernel, the rest the global kernel.
-    // Mixed: every system uses the global kernel (FP32 factors + FP64 refinement).
+    P.mixed = mixed;
+    P.o = o;
+    // FP64: systems that fit shared memory use the smem kernel (unless tuned otherwise),
+    // the rest the global kernel.  Mixed: every system uses the global kernel.
     const size_t smem_cap = (size_t)h->max_smem_optin;
     std::vector<RomDev> dev(n_roms);
-    std::vector<int> cls(n_roms, -1);  // 0 smem, 1 global
-    size_t smem_max = 0;
-    int g_nmax = 0, g_rmax = 0;
-    long long n_items[2] = {0, 0};
+    std::vector<int> cls(n_roms, -1);
     for (int i = 0; i < n_roms; ++i) {
         dev[i] = to_dev(roms[i]);
         const srom_rom_desc &d = roms[i];
         if (d.n == 0 || d.F == 0 || d.r == 0) continue;
-        size_t s = srom::fp64_smem_bytes(d.n, d.r);
-        if (!mixed && s <= smem_cap) {
-            cls[i] = 0;
-            smem_max = std::max(smem_max, s);
+        cls[i] = mixed ? 1 : fp64_class(h, d.n, d.r);
+        if (cls[i] == 0) {
+            P.smem_max = std::max(P.smem_max, srom::fp64_smem_bytes(d.n, d.r));
         } else {
-            cls[i] = 1;
-            g_nmax = std::max(g_nmax, d.n);
-            g_rmax = std::max(g_rmax, d.r);
+            P.g_nmax = std::max(P.g_nmax, d.n);
+            P.g_rmax = std::max(P.g_rmax, d.r);
         }
-        n_items[cls[i]] += d.F;
+        P.n_items[cls[i]] += d.F;
+        P.flops[cls[i]] += lu_flops(d.n, d.r) * d.F;
     }
-    if (g_nmax > 0 && (srom::global_rpt(g_nmax) > srom::GLOBAL_MAX_RPT ||
-                       srom::global_smem_bytes(g_nmax, g_rmax) + srom::GLOBAL_STATIC_SMEM > smem_cap))
+    if (P.g_nmax > 0 && (srom::global_rpt(P.g_nmax) > srom::GLOBAL_MAX_RPT ||
+                         srom::global_smem_bytes(P.g_nmax, P.g_rmax) + srom::GLOBAL_STATIC_SMEM > smem_cap))
         return set_err(h, SROM_ERR_UNSUPPORTED, "n=%d with r=%d exceeds the shared-memory panel budget",
-                       g_nmax, g_rmax);
-    if (n_items[0] + n_items[1] > INT32_MAX) return set_err(h, SROM_ERR_UNSUPPORTED, "too many systems");
-
+                       P.g_nmax, P.g_rmax);
+    if (P.n_items[0] + P.n_items[1] > INT32_MAX) return set_err(h, SROM_ERR_UNSUPPORTED, "too many systems");
+    if (P.n_items[0] > 0) {
+        const int bps = srom::fp64_smem_blocks_per_sm(P.smem_max);
+        if (bps <= 0) return set_err(h, SROM_ERR_UNSUPPORTED, "smem kernel cannot be resident (%zu B)", P.smem_max);
+        P.grid0 = std::min<long long>(P.n_items[0], (long long)bps * h->sm_count);
+    }
+    if (P.n_items[1] > 0) {
+        P.grid1 = std::min<long long>(P.n_items[1], h->sm_count);
+        P.slot_bytes = (int64_t)P.g_nmax * P.g_nmax * (int64_t)sizeof(double2);
+        P.need_scratch = mixed;
+        for (int i = 0; i < n_roms; ++i)
+            if (cls[i] == 1 && !roms[i].LU) P.need_scratch = true;
+    }
+    // Work lists: largest systems first (longest-processing-time order for the persistent CTAs).
     std::vector<int> order(n_roms);
     for (int i = 0; i < n_roms; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return roms[a].n > roms[b].n; });
-
-    // ---- stage descriptors + work lists ---------------------------------------------------
-    const size_t off_items0 = align_up(sizeof(RomDev) * std::max(n_roms, 1), 256);
-    const size_t off_items1 = off_items0 + align_up(sizeof(Item) * (size_t)n_items[0] + 1, 256);
-    const size_t off_fb = off_items1 + align_up(sizeof(Item) * (size_t)n_items[1] + 1, 256);
-    const size_t off_ctr = off_fb + (mixed ? align_up(sizeof(Item) * (size_t)n_items[1] + 1, 256) : 0);
-    const size_t meta_bytes = off_ctr + 256;
-    int s = ensure_host_pinned(h, meta_bytes);
-    if (s) return s;
-    if (h->meta_pending) {
-        SROM_CUDA(h, cudaEventSynchronize(h->meta_done));
-        h->meta_pending = false;
-    }
-    s = ensure_device_buffer(h, &h->d_meta, &h->d_meta_bytes, meta_bytes);
-    if (s) return s;
-    char *hm = static_cast<char *>(h->h_meta);
+    P.off_items0 = align_up(sizeof(RomDev) * std::max(n_roms, 1), 256);
+    P.off_items1 = P.off_items0 + align_up(sizeof(Item) * (size_t)P.n_items[0] + 1, 256);
+    P.off_fb = P.off_items1 + align_up(sizeof(Item) * (size_t)P.n_items[1] + 1, 256);
+    P.off_ctr = P.off_fb + (mixed ? align_up(sizeof(Item) * (size_t)P.n_items[1] + 1, 256) : 0);
+    P.meta.assign(P.off_ctr + 256, 0);
+    char *hm = P.meta.data();
     if (n_roms) memcpy(hm, dev.data(), sizeof(RomDev) * n_roms);
-    Item *it0 = reinterpret_cast<Item *>(hm + off_items0);
-    Item *it1 = reinterpret_cast<Item *>(hm + off_items1);
+    Item *it0 = reinterpret_cast<Item *>(hm + P.off_items0);
+    Item *it1 = reinterpret_cast<Item *>(hm + P.off_items1);
     long long k0 = 0, k1 = 0;
     for (int oi = 0; oi < n_roms; ++oi) {
         const int i = order[oi];
@@ -372,60 +400,48 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
         long long &k = cls[i] == 0 ? k0 : k1;
         for (int f = 0; f < roms[i].F; ++f) dst[k++] = Item{i, f};
     }
-    int *ctr = reinterpret_cast<int *>(hm + off_ctr);
-    for (int k = 0; k < 8; ++k) ctr[k] = 0;  // smem, global, fallback count, fallback work
-    SROM_CUDA(h, cudaMemcpyAsync(h->d_meta, h->h_meta, meta_bytes, cudaMemcpyHostToDevice, h->stream));
-    SROM_CUDA(h, cudaEventRecord(h->meta_done, h->stream));
-    h->meta_pending = true;
-    char *dm = static_cast<char *>(h->d_meta);
-    const RomDev *d_roms = reinterpret_cast<const RomDev *>(dm);
-    const Item *d_it0 = reinterpret_cast<const Item *>(dm + off_items0);
-    const Item *d_it1 = reinterpret_cast<const Item *>(dm + off_items1);
-    int *d_ctr = reinterpret_cast<int *>(dm + off_ctr);
+    return SROM_OK;
+}
 
-    // ---- launches ------------------------------------------------------------------------
-    double flops[2] = {0.0, 0.0};
-    for (int i = 0; i < n_roms; ++i)
-        if (cls[i] >= 0) flops[cls[i]] += lu_flops(roms[i].n, roms[i].r) * roms[i].F;
-    if (n_items[0] > 0) {
-        int bps = srom::fp64_smem_blocks_per_sm(smem_max);
-        if (bps <= 0) return set_err(h, SROM_ERR_UNSUPPORTED, "smem kernel cannot be resident (%zu B)", smem_max);
-        long long grid = std::min<long long>(n_items[0], (long long)bps * h->sm_count);
-        ProfScope ps(h, "fp64_smem", n_items[0], flops[0], 0.0);
-        SROM_CUDA(h, srom::launch_fp64_smem(d_roms, d_it0, (int)n_items[0], d_ctr, smem_max, (int)grid, h->stream));
+// Counters (smem, global, fallback count, fallback work) live at off_ctr and must be zero
+// when the launches start: the metadata copy zeroes them, or zero_counters does.
+int enqueue_plan(srom_handle *h, const SweepPlan &P, char *dm, void *scratch, cudaStream_t st, bool zero_counters,
+                 bool profile) {
+    const RomDev *d_roms = reinterpret_cast<const RomDev *>(dm);
+    const Item *d_it0 = reinterpret_cast<const Item *>(dm + P.off_items0);
+    const Item *d_it1 = reinterpret_cast<const Item *>(dm + P.off_items1);
+    int *d_ctr = reinterpret_cast<int *>(dm + P.off_ctr);
+    if (zero_counters) SROM_CUDA(h, cudaMemsetAsync(d_ctr, 0, 8 * sizeof(int), st));
+    const bool prof_prev = h->prof;
+    if (!profile) h->prof = false;
+    int rc = SROM_OK;
+    if (P.n_items[0] > 0) {
+        ProfScope ps(h, "fp64_smem", P.n_items[0], P.flops[0], 0.0);
+        cudaError_t e = srom::launch_fp64_smem(d_roms, d_it0, (int)P.n_items[0], d_ctr, P.smem_max, (int)P.grid0, st);
+        if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "fp64 smem launch: %s", cudaGetErrorString(e));
     }
-    if (n_items[1] > 0) {
-        long long grid = std::min<long long>(n_items[1], h->sm_count);
-        bool all_keep = !mixed;
-        for (int i = 0; i < n_roms; ++i)
-            if (cls[i] == 1 && !roms[i].LU) all_keep = false;
-        const int64_t slot_bytes = (int64_t)g_nmax * g_nmax * (int64_t)sizeof(double2);
-        void *scr = nullptr;
-        if (!all_keep) {
-            s = ensure_device_buffer(h, &h->scratch, &h->scratch_bytes, (size_t)slot_bytes * grid);
-            if (s) return s;
-            scr = h->scratch;
-        }
+    if (rc == SROM_OK && P.n_items[1] > 0) {
         srom::GlobalArgs a{};
         a.roms = d_roms;
         a.items = d_it1;
-        a.n_items = (int)n_items[1];
+        a.n_items = (int)P.n_items[1];
         a.counter = d_ctr + 1;
-        a.scratch = static_cast<unsigned char *>(scr);
-        a.slot_bytes = slot_bytes;
-        a.n_max = g_nmax;
-        a.r_max = g_rmax;
-        a.max_refine = o.max_refine;
-        a.tol = o.tol;
-        if (mixed && (o.flags & SROM_FLAG_FALLBACK_FP64)) {
-            a.fb_items = reinterpret_cast<Item *>(dm + off_fb);
+        a.scratch = static_cast<unsigned char *>(scratch);
+        a.slot_bytes = P.slot_bytes;
+        a.n_max = P.g_nmax;
+        a.r_max = P.g_rmax;
+        a.max_refine = P.o.max_refine;
+        a.tol = P.o.tol;
+        if (P.mixed && (P.o.flags & SROM_FLAG_FALLBACK_FP64)) {
+            a.fb_items = reinterpret_cast<Item *>(dm + P.off_fb);
             a.fb_count = d_ctr + 2;
         }
         {
-            ProfScope ps(h, mixed ? "mixed_global" : "fp64_global", n_items[1], flops[1], 0.0);
-            SROM_CUDA(h, srom::launch_global(mixed, a, (int)grid, h->stream));
+            ProfScope ps(h, P.mixed ? "mixed_global" : "fp64_global", P.n_items[1], P.flops[1], 0.0);
+            cudaError_t e = srom::launch_global(P.mixed, a, (int)P.grid1, st);
+            if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "global launch: %s", cudaGetErrorString(e));
         }
-        if (a.fb_items) {
+        if (rc == SROM_OK && a.fb_items) {
             // FP64 re-solve of the systems the mixed kernel could not refine; the item count
             // stays on the device, so the launch needs no host synchronisation.
             srom::GlobalArgs b = a;
@@ -436,9 +452,120 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
             b.fb_count = nullptr;
             b.steps_value = -1;
             ProfScope ps(h, "fp64_fallback", 0, 0.0, 0.0);
-            SROM_CUDA(h, srom::launch_global(false, b, (int)grid, h->stream));
+            cudaError_t e = srom::launch_global(false, b, (int)P.grid1, st);
+            if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "fallback launch: %s", cudaGetErrorString(e));
         }
     }
+    h->prof = prof_prev;
+    return rc;
+}
+
+}  // namespace
+
+struct srom_graph {
+    srom_handle *h = nullptr;
+    void *d_meta = nullptr;
+    void *scratch = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" {
+
+int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    SweepPlan P;
+    int s = make_plan(h, roms, n_roms, opts, P);
+    if (s) return s;
+    DeviceGuard g(h->device);
+    s = ensure_host_pinned(h, P.meta.size());
+    if (s) return s;
+    if (h->meta_pending) {
+        SROM_CUDA(h, cudaEventSynchronize(h->meta_done));
+        h->meta_pending = false;
+    }
+    s = ensure_device_buffer(h, &h->d_meta, &h->d_meta_bytes, P.meta.size());
+    if (s) return s;
+    void *scr = nullptr;
+    if (P.need_scratch) {
+        s = ensure_device_buffer(h, &h->scratch, &h->scratch_bytes, (size_t)P.slot_bytes * P.grid1);
+        if (s) return s;
+        scr = h->scratch;
+    }
+    memcpy(h->h_meta, P.meta.data(), P.meta.size());
+    SROM_CUDA(h, cudaMemcpyAsync(h->d_meta, h->h_meta, P.meta.size(), cudaMemcpyHostToDevice, h->stream));
+    SROM_CUDA(h, cudaEventRecord(h->meta_done, h->stream));
+    h->meta_pending = true;
+    return enqueue_plan(h, P, static_cast<char *>(h->d_meta), scr, h->stream, false, true);
+}
+
+int srom_graph_create(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts,
+                      srom_graph **out) {
+    if (!h || !out) return SROM_ERR_INVALID;
+    *out = nullptr;
+    h->err.clear();
+    SweepPlan P;
+    int s = make_plan(h, roms, n_roms, opts, P);
+    if (s) return s;
+    DeviceGuard g(h->device);
+    srom_graph *G = new srom_graph();
+    G->h = h;
+    auto fail = [&](int code) {
+        if (G->d_meta) cudaFree(G->d_meta);
+        if (G->scratch) cudaFree(G->scratch);
+        if (G->exec) cudaGraphExecDestroy(G->exec);
+        if (G->graph) cudaGraphDestroy(G->graph);
+        delete G;
+        return code;
+    };
+    cudaError_t e = cudaMalloc(&G->d_meta, P.meta.size());
+    if (e != cudaSuccess) return fail(set_err(h, SROM_ERR_ALLOC, "graph metadata: %s", cudaGetErrorString(e)));
+    if (P.need_scratch && (e = cudaMalloc(&G->scratch, (size_t)P.slot_bytes * P.grid1)) != cudaSuccess)
+        return fail(set_err(h, SROM_ERR_ALLOC, "graph scratch: %s", cudaGetErrorString(e)));
+    if ((e = cudaMemcpy(G->d_meta, P.meta.data(), P.meta.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(set_err(h, SROM_ERR_CUDA, "graph metadata copy: %s", cudaGetErrorString(e)));
+    cudaStream_t cs;
+    if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(set_err(h, SROM_ERR_CUDA, "capture stream: %s", cudaGetErrorString(e)));
+    // Kernel attributes are set before capture (the launchers set them on every call).
+    if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return fail(set_err(h, SROM_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e)));
+    }
+    s = enqueue_plan(h, P, static_cast<char *>(G->d_meta), G->scratch, cs, true, false);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    if (s) {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(s);
+    }
+    if (e != cudaSuccess) return fail(set_err(h, SROM_ERR_CUDA, "end capture: %s", cudaGetErrorString(e)));
+    G->graph = graph;
+    if ((e = cudaGraphInstantiate(&G->exec, graph, 0)) != cudaSuccess)
+        return fail(set_err(h, SROM_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e)));
+    *out = G;
+    return SROM_OK;
+}
+
+int srom_graph_launch(srom_graph *G, void *stream) {
+    if (!G || !G->exec) return SROM_ERR_INVALID;
+    DeviceGuard g(G->h->device);
+    cudaError_t e = cudaGraphLaunch(G->exec, reinterpret_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return set_err(G->h, SROM_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+    return SROM_OK;
+}
+
+int srom_graph_destroy(srom_graph *G) {
+    if (!G) return SROM_OK;
+    DeviceGuard g(G->h->device);
+    cudaDeviceSynchronize();
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->graph) cudaGraphDestroy(G->graph);
+    if (G->d_meta) cudaFree(G->d_meta);
+    if (G->scratch) cudaFree(G->scratch);
+    delete G;
     return SROM_OK;
 }
 
@@ -665,6 +792,129 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
         if (d.berr) SROM_CUDA(h, cudaMemcpyAsync(d.berr, e.berr, sizeof(double) * d.F, D2H, h->stream));
     }
     SROM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return SROM_OK;
+}
+
+int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char *cache_path) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    if (count < 0 || (count > 0 && !n_values) || r < 1) return set_err(h, SROM_ERR_INVALID, "bad tuning request");
+    DeviceGuard g(h->device);
+    cudaDeviceProp prop;
+    SROM_CUDA(h, cudaGetDeviceProperties(&prop, h->device));
+    // 1) cached choices for this device
+    if (cache_path) {
+        if (FILE *fp = fopen(cache_path, "r")) {
+            char line[512], dev[256] = {0};
+            bool same_dev = false;
+            while (fgets(line, sizeof line, fp)) {
+                if (sscanf(line, " \"device\": \"%255[^\"]\"", dev) == 1) same_dev = strcmp(dev, prop.name) == 0;
+                int n = 0, rr = 0;
+                char kern[32] = {0};
+                if (same_dev && sscanf(line, " {\"precision\": \"fp64\", \"n\": %d, \"r\": %d, \"kernel\": \"%31[^\"]\"",
+                                       &n, &rr, kern) == 3)
+                    h->tune_fp64[((long long)n << 16) | rr] = strcmp(kern, "smem") == 0 ? 0 : 1;
+            }
+            fclose(fp);
+        }
+    }
+    // 2) time both storage classes for every requested n that has no entry yet
+    struct Entry {
+        int n, r, cls;
+        float ms[2];
+    };
+    std::vector<Entry> measured;
+    for (int q = 0; q < count; ++q) {
+        const int n = n_values[q];
+        if (n <= 0) continue;
+        const long long key = ((long long)n << 16) | r;
+        if (h->tune_fp64.count(key)) continue;
+        if (srom::fp64_smem_bytes(n, r) > (size_t)h->max_smem_optin) continue;  // only the global kernel fits
+        const int F = 2 * h->sm_count;
+        std::vector<srom_complex> K((size_t)n * n), M((size_t)n * n), B((size_t)n * r);
+        std::vector<double> om(F);
+        uint64_t state = 0x9E3779B97F4A7C15ull ^ (uint64_t)n;
+        auto rnd = [&]() {
+            state ^= state << 13;
+            state ^= state >> 7;
+            state ^= state << 17;
+            return (double)(state >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+        };
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                K[i + (size_t)j * n] = {rnd() + (i == j ? 2.0 * n : 0.0), rnd()};
+                M[i + (size_t)j * n] = {i == j ? 1.0 : 0.0, 0.0};
+            }
+        for (auto &b : B) b = {rnd(), rnd()};
+        for (int f = 0; f < F; ++f) om[f] = 0.1 + 0.01 * f;
+        const size_t nn = sizeof(srom_complex) * (size_t)n * n;
+        char *buf = nullptr;
+        const size_t tot = 2 * nn + sizeof(srom_complex) * (size_t)n * r + sizeof(double) * F +
+                           sizeof(srom_complex) * (size_t)F * n * r;
+        cudaError_t e = cudaMalloc(&buf, tot);
+        if (e != cudaSuccess) return set_err(h, SROM_ERR_ALLOC, "tuning buffers: %s", cudaGetErrorString(e));
+        srom_rom_desc d{};
+        d.n = n;
+        d.r = r;
+        d.F = F;
+        d.ldk = n;
+        d.ldb = n;
+        d.K = reinterpret_cast<srom_complex *>(buf);
+        d.M = reinterpret_cast<srom_complex *>(buf + nn);
+        d.rhs = reinterpret_cast<srom_complex *>(buf + 2 * nn);
+        d.omega = reinterpret_cast<double *>(buf + 2 * nn + sizeof(srom_complex) * (size_t)n * r);
+        d.X = reinterpret_cast<srom_complex *>(buf + 2 * nn + sizeof(srom_complex) * (size_t)n * r + sizeof(double) * F);
+        cudaMemcpy((void *)d.K, K.data(), nn, cudaMemcpyHostToDevice);
+        cudaMemcpy((void *)d.M, M.data(), nn, cudaMemcpyHostToDevice);
+        cudaMemcpy((void *)d.rhs, B.data(), sizeof(srom_complex) * (size_t)n * r, cudaMemcpyHostToDevice);
+        cudaMemcpy((void *)d.omega, om.data(), sizeof(double) * F, cudaMemcpyHostToDevice);
+        Entry ent{n, r, 0, {0.f, 0.f}};
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        int rc = SROM_OK;
+        for (int c = 0; c < 2 && rc == SROM_OK; ++c) {
+            h->tune_fp64[key] = c;
+            srom_sweep_opts o{SROM_FP64, 5, 0.0, 0};
+            rc = srom_sweep(h, &d, 1, &o);  // warm-up
+            cudaEventRecord(a, h->stream);
+            for (int rep = 0; rep < 3 && rc == SROM_OK; ++rep) rc = srom_sweep(h, &d, 1, &o);
+            cudaEventRecord(b, h->stream);
+            cudaEventSynchronize(b);
+            cudaEventElapsedTime(&ent.ms[c], a, b);
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaStreamSynchronize(h->stream);
+        cudaFree(buf);
+        if (rc != SROM_OK) {
+            h->tune_fp64.erase(key);
+            return rc;
+        }
+        ent.cls = ent.ms[1] < ent.ms[0] ? 1 : 0;
+        h->tune_fp64[key] = ent.cls;
+        measured.push_back(ent);
+    }
+    // 3) rewrite the cache with every entry the handle knows
+    if (cache_path && !measured.empty()) {
+        FILE *fp = fopen(cache_path, "w");
+        if (!fp) return set_err(h, SROM_ERR_INVALID, "cannot write %s", cache_path);
+        fprintf(fp, "{\n  \"device\": \"%s\",\n  \"entries\": [\n", prop.name);
+        size_t k = 0;
+        for (const auto &kv : h->tune_fp64) {
+            const int n = (int)(kv.first >> 16), rr = (int)(kv.first & 0xffff);
+            float ms0 = -1.f, ms1 = -1.f;
+            for (const auto &m : measured)
+                if (m.n == n && m.r == rr) {
+                    ms0 = m.ms[0];
+                    ms1 = m.ms[1];
+                }
+            fprintf(fp, "    {\"precision\": \"fp64\", \"n\": %d, \"r\": %d, \"kernel\": \"%s\", \"ms_smem\": %.4f, \"ms_global\": %.4f}%s\n",
+                    n, rr, kv.second == 0 ? "smem" : "global", ms0, ms1, ++k < h->tune_fp64.size() ? "," : "");
+        }
+        fprintf(fp, "  ]\n}\n");
+        fclose(fp);
+    }
     return SROM_OK;
 }
 

@@ -154,3 +154,37 @@ def sweep_host(handle: _capi.Handle, roms: Sequence[HostRom], precision: int = _
     arr = (RomDesc * max(len(roms), 1))(*[r.desc() for r in roms])
     o = opts(precision, max_refine, tol, flags)
     check(handle.ptr, _capi.lib().srom_sweep_host(handle.ptr, arr, len(roms), C.byref(o)))
+
+
+class Graph:
+    """A planned batched sweep captured as a CUDA graph (``srom_graph_create``)."""
+
+    def __init__(self, handle: _capi.Handle, roms: Sequence[DeviceRom], precision: int = _capi.SROM_FP64,
+                 max_refine: int = 5, tol: float = 0.0, flags: int = 0):
+        self.handle = handle
+        self._g = C.c_void_p()
+        self._roms = list(roms)  # keep the buffers alive
+        arr = (RomDesc * max(len(roms), 1))(*[r.desc() for r in roms])
+        o = opts(precision, max_refine, tol, flags)
+        check(handle.ptr, _capi.lib().srom_graph_create(handle.ptr, arr, len(roms), C.byref(o), C.byref(self._g)))
+
+    def launch(self, stream_ptr: int = 0) -> None:
+        check(self.handle.ptr, _capi.lib().srom_graph_launch(self._g, C.c_void_p(stream_ptr)))
+
+    def close(self) -> None:
+        if self._g:
+            _capi.lib().srom_graph_destroy(self._g)
+            self._g = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tune(handle: _capi.Handle, n_values, r: int = 1, cache_path: Optional[str] = None) -> None:
+    """Autotune the FP64 kernel choice per order n (``srom_tune``), optionally with a JSON cache."""
+    ns = (C.c_int * max(len(n_values), 1))(*[int(v) for v in n_values])
+    check(handle.ptr, _capi.lib().srom_tune(handle.ptr, ns, len(n_values), int(r),
+                                            None if cache_path is None else cache_path.encode()))
