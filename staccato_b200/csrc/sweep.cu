@@ -45,6 +45,7 @@ constexpr int CW = 4;      // trailing columns per warp group
 constexpr int RQ = 4;      // Schur rows per lane per pass
 constexpr int NB64 = 16;   // FP64 panel width
 constexpr int NB32 = 32;   // FP32 panel width
+constexpr int RMAX_SOLVE = 16;  // right-hand sides per solve (register accumulators)
 
 // ====================================================================================
 // smem class (FP64)
@@ -119,6 +120,81 @@ __device__ void panel_factor_smem(double2 *P, int ldp, int m, int ncols, int *ip
     }
 }
 
+// Asynchronous global -> shared copies (each thread stages only the values it will use).
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
+
+// One row of the blocked substitution: b[i, c] -= sum_j A[i, j] b[j, c] over the block's
+// columns j (increasing for the forward sweep, decreasing for the backward one), all
+// right-hand sides.  With a stage (global A), the row's block entries are copied into the
+// thread's own shared-memory column (stage[t * NT + tid]) by cp.async in two alternating
+// batches of CB, so the whole batch is in flight before it is used; without a stage
+// (A in shared memory) the entries are read directly.
+template <typename T, bool BACKWARD>
+__device__ __forceinline__ void solve_row_block_chunk(const T *A, int64_t lda, T *B, int ldb, int nrhs, int i,
+                                                      int jb, int je, T *stage, int CB) {
+    using C = CT<T>;
+    const int bs = je - jb;
+    const int tid = threadIdx.x;
+    auto col = [&](int t) { return BACKWARD ? je - 1 - t : jb + t; };
+    T acc[RMAX_SOLVE];
+#pragma unroll
+    for (int cc = 0; cc < RMAX_SOLVE; ++cc) acc[cc] = cc < nrhs ? B[i + (int64_t)cc * ldb] : C::zero();
+    if (stage) {
+        const int nb = (bs + CB - 1) / CB;
+        auto issue = [&](int b) {
+            T *dst = stage + (b & 1) * CB * NT;
+            for (int t = 0; t < CB && b * CB + t < bs; ++t) cp_async_elem(dst + t * NT + tid, A + i + col(b * CB + t) * lda);
+            cp_async_commit();
+        };
+        issue(0);
+        for (int b = 0; b < nb; ++b) {
+            if (b + 1 < nb) {
+                issue(b + 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            const T *src = stage + (b & 1) * CB * NT;
+            for (int t = 0; t < CB && b * CB + t < bs; ++t) {
+                const T a = src[t * NT + tid];
+                const int j = col(b * CB + t);
+#pragma unroll
+                for (int cc = 0; cc < RMAX_SOLVE; ++cc)
+                    if (cc < nrhs) acc[cc] = C::subm(acc[cc], a, B[j + (int64_t)cc * ldb]);
+            }
+        }
+    } else {
+        for (int t = 0; t < bs; ++t) {
+            const int j = col(t);
+            const T a = A[i + j * lda];
+#pragma unroll
+            for (int cc = 0; cc < RMAX_SOLVE; ++cc)
+                if (cc < nrhs) acc[cc] = C::subm(acc[cc], a, B[j + (int64_t)cc * ldb]);
+        }
+    }
+#pragma unroll
+    for (int cc = 0; cc < RMAX_SOLVE; ++cc)
+        if (cc < nrhs) B[i + (int64_t)cc * ldb] = acc[cc];
+}
+
+template <typename T, bool BACKWARD>
+__device__ __forceinline__ void solve_row_block(const T *A, int64_t lda, T *B, int ldb, int nrhs, int i, int jb,
+                                                int je, T *stage, int CB) {
+    for (int c0 = 0; c0 < nrhs; c0 += RMAX_SOLVE)
+        solve_row_block_chunk<T, BACKWARD>(A, lda, B + (int64_t)c0 * ldb, ldb, min(RMAX_SOLVE, nrhs - c0), i, jb, je,
+                                           stage, CB);
+}
+
 // zgetrs 'N' on an in-place LU (A, lda) with B (n x nrhs, ldb) in shared memory; the row
 // interchanges have already been applied to B.  32-row blocks: the block's diagonal triangle
 // is staged in shared memory (tile, 32 x 33) when A lives in global memory, one warp per
@@ -126,7 +202,8 @@ __device__ void panel_factor_smem(double2 *P, int ldp, int m, int ncols, int *ip
 // takes rows below (above) the block and applies the block to all right-hand sides of the
 // row.  Every entry of B receives its updates in the oracle's order.
 template <typename T>
-__device__ void lu_solve(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs, T *tile) {
+__device__ void lu_solve(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs, T *tile, T *stage = nullptr,
+                         int stage_cb = 0) {
     using C = CT<T>;
     constexpr int LDT = 33;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -151,24 +228,7 @@ __device__ void lu_solve(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs
             if (lane < bs) b[lane] = v;
         }
         __syncthreads();
-        for (int i = je + tid; i < n; i += NT) {
-            for (int c0 = 0; c0 < nrhs; c0 += 4) {
-                const int nc = min(4, nrhs - c0);
-                T acc[4];
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc) acc[cc] = cc < nc ? B[i + (int64_t)(c0 + cc) * ldb] : C::zero();
-#pragma unroll 8
-                for (int j = jb; j < je; ++j) {
-                    const T a = A[i + j * lda];
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc)
-                        if (cc < nc) acc[cc] = C::subm(acc[cc], a, B[j + (int64_t)(c0 + cc) * ldb]);
-                }
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc)
-                    if (cc < nc) B[i + (int64_t)(c0 + cc) * ldb] = acc[cc];
-            }
-        }
+        for (int i = je + tid; i < n; i += NT) solve_row_block<T, false>(A, lda, B, ldb, nrhs, i, jb, je, stage, stage_cb);
         __syncthreads();
     }
     for (int jend = n; jend > 0; jend -= 32) {
@@ -193,22 +253,126 @@ __device__ void lu_solve(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs
             if (lane < bs) b[lane] = v;
         }
         __syncthreads();
-        for (int i = tid; i < jb; i += NT) {
+        for (int i = tid; i < jb; i += NT) solve_row_block<T, true>(A, lda, B, ldb, nrhs, i, jb, jend, stage, stage_cb);
+        __syncthreads();
+    }
+}
+
+// zgetrs 'N' for a factor in global memory, streamed through shared memory: the SW columns
+// of each block, from the block's first row (forward) or row 0 (backward) to the last row
+// needed, are copied by cp.async into one of two strip buffers while the previous block is
+// being processed.  One warp per right-hand side solves the block's triangle from the strip,
+// then every thread updates its rows.  B (n x nrhs, ldb) is in shared memory with the
+// interchanges already applied; the per-entry update order is the oracle's.
+template <typename T, int SW>
+__device__ void lu_solve_strips(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs, T *strips) {
+    using C = CT<T>;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nblk = (n + SW - 1) / SW;
+    // ---- forward: unit lower triangle ----
+    auto issue_f = [&](int blk) {
+        const int jb = blk * SW, bs = min(SW, n - jb), rows = n - jb;
+        T *dst = strips + (blk & 1) * (SW * n);
+        for (int e = tid; e < rows * bs; e += NT) {
+            const int r = e % rows, c = e / rows;
+            cp_async_elem(dst + c * n + r, A + (jb + r) + (int64_t)(jb + c) * lda);
+        }
+        cp_async_commit();
+    };
+    issue_f(0);
+    for (int blk = 0; blk < nblk; ++blk) {
+        const int jb = blk * SW, bs = min(SW, n - jb), je = jb + bs, rows = n - jb;
+        if (blk + 1 < nblk) {
+            issue_f(blk + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const T *S = strips + (blk & 1) * (SW * n);  // S[c * n + r] = A[jb + r, jb + c]
+        for (int c = warp; c < nrhs; c += NW) {
+            T *b = B + (int64_t)c * ldb + jb;
+            T v = lane < bs ? b[lane] : C::zero();
+            for (int j = 0; j < bs; ++j) {
+                const T bj = C::shfl(v, j, 32);
+                if (lane > j && lane < bs) v = C::subm(v, S[j * n + lane], bj);
+            }
+            if (lane < bs) b[lane] = v;
+        }
+        __syncthreads();
+        for (int r = bs + tid; r < rows; r += NT) {
             for (int c0 = 0; c0 < nrhs; c0 += 4) {
                 const int nc = min(4, nrhs - c0);
                 T acc[4];
 #pragma unroll
-                for (int cc = 0; cc < 4; ++cc) acc[cc] = cc < nc ? B[i + (int64_t)(c0 + cc) * ldb] : C::zero();
-#pragma unroll 8
-                for (int j = jend - 1; j >= jb; --j) {
-                    const T a = A[i + j * lda];
+                for (int cc = 0; cc < 4; ++cc) acc[cc] = cc < nc ? B[jb + r + (int64_t)(c0 + cc) * ldb] : C::zero();
 #pragma unroll
-                    for (int cc = 0; cc < 4; ++cc)
-                        if (cc < nc) acc[cc] = C::subm(acc[cc], a, B[j + (int64_t)(c0 + cc) * ldb]);
+                for (int j = 0; j < SW; ++j) {
+                    if (j < bs) {
+                        const T a = S[j * n + r];
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc)
+                            if (cc < nc) acc[cc] = C::subm(acc[cc], a, B[jb + j + (int64_t)(c0 + cc) * ldb]);
+                    }
                 }
 #pragma unroll
                 for (int cc = 0; cc < 4; ++cc)
-                    if (cc < nc) B[i + (int64_t)(c0 + cc) * ldb] = acc[cc];
+                    if (cc < nc) B[jb + r + (int64_t)(c0 + cc) * ldb] = acc[cc];
+            }
+        }
+        __syncthreads();
+    }
+    // ---- backward: upper triangle, blocks from the last ----
+    auto issue_b = [&](int q) {  // q-th block from the end
+        const int jend = n - q * SW, jb = max(jend - SW, 0), bs = jend - jb, rows = jend;
+        T *dst = strips + (q & 1) * (SW * n);
+        for (int e = tid; e < rows * bs; e += NT) {
+            const int r = e % rows, c = e / rows;
+            cp_async_elem(dst + c * n + r, A + r + (int64_t)(jb + c) * lda);
+        }
+        cp_async_commit();
+    };
+    issue_b(0);
+    for (int q = 0; q < nblk; ++q) {
+        const int jend = n - q * SW, jb = max(jend - SW, 0), bs = jend - jb;
+        if (q + 1 < nblk) {
+            issue_b(q + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const T *S = strips + (q & 1) * (SW * n);  // S[c * n + r] = A[r, jb + c]
+        for (int c = warp; c < nrhs; c += NW) {
+            T *b = B + (int64_t)c * ldb + jb;
+            T v = lane < bs ? b[lane] : C::zero();
+            for (int j = bs - 1; j >= 0; --j) {
+                if (lane == j) v = C::div(v, S[j * n + jb + j]);
+                const T bj = C::shfl(v, j, 32);
+                if (lane < j) v = C::subm(v, S[j * n + jb + lane], bj);
+            }
+            if (lane < bs) b[lane] = v;
+        }
+        __syncthreads();
+        for (int r = tid; r < jb; r += NT) {
+            for (int c0 = 0; c0 < nrhs; c0 += 4) {
+                const int nc = min(4, nrhs - c0);
+                T acc[4];
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) acc[cc] = cc < nc ? B[r + (int64_t)(c0 + cc) * ldb] : C::zero();
+#pragma unroll
+                for (int jj = 0; jj < SW; ++jj) {
+                    const int j = bs - 1 - jj;
+                    if (j >= 0) {
+                        const T a = S[j * n + r];
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc)
+                            if (cc < nc) acc[cc] = C::subm(acc[cc], a, B[jb + j + (int64_t)(c0 + cc) * ldb]);
+                    }
+                }
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc)
+                    if (cc < nc) B[r + (int64_t)(c0 + cc) * ldb] = acc[cc];
             }
         }
         __syncthreads();
@@ -412,7 +576,20 @@ __device__ void panel_factor_par(T *P, int ldp, int m, int ncols, int *s_perm, i
                 l = C::mul(l, inv);
                 P[ph + (int64_t)jj * ldp] = l;
             }
-            for (int c = jj + 1; c < ncols; ++c)
+            // rank-1 update of this row, four columns per batch so the shared-memory loads
+            // overlap (each entry still receives exactly this column's update)
+            int c = jj + 1;
+            for (; c + 4 <= ncols; c += 4) {
+                T v[4], u[4];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    v[t] = P[ph + (int64_t)(c + t) * ldp];
+                    u[t] = P[bp + (int64_t)(c + t) * ldp];
+                }
+#pragma unroll
+                for (int t = 0; t < 4; ++t) P[ph + (int64_t)(c + t) * ldp] = C::subm(v[t], l, u[t]);
+            }
+            for (; c < ncols; ++c)
                 P[ph + (int64_t)c * ldp] = C::subm(P[ph + (int64_t)c * ldp], l, P[bp + (int64_t)c * ldp]);
         }
     }
@@ -757,6 +934,13 @@ __device__ void apply_correction(double2 *X, const float2 *B32, int n, int nrhs,
 constexpr int RMAX_MIXED = 16;
 constexpr int SROM_INFO_NOT_CONVERGED_DEV = -1;
 
+// Columns per cp.async batch in the solves: two batches of NT rows fit the panel region.
+template <typename T>
+__host__ __device__ constexpr int stage_cb(int ldp) {
+    const int cb = (int)(((size_t)ldp * 256) / (2 * NT * sizeof(T)));
+    return cb < 1 ? 1 : (cb > 32 ? 32 : cb);
+}
+
 // Global-class kernel.  MIXED: complex-FP32 factors + FP64 refinement; systems that do not
 // converge are appended to a.fb_items (when given) for the FP64 kernel launched after it.
 // FP64: the bit-exact path; a.n_items_dev (when given) holds the item count (fallback list).
@@ -804,10 +988,9 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
             __syncthreads();
             const double tol_x = a.tol > 0.0 ? a.tol : 1.1641532182693481e-10;  // 2^-33
             bool conv = false;
-            float2 *tile = reinterpret_cast<float2 *>(sm + L.tile);
             for (int s = 0;; ++s) {
                 if (s > 0) residual64<RPT>(R, w, X, B32, s_pos);
-                lu_solve<float2>(A32, n, n, B32, n, R.r, tile);
+                lu_solve_strips<float2, 16>(A32, n, n, B32, n, R.r, reinterpret_cast<float2 *>(sm + L.panel));
                 apply_correction(X, B32, n, R.r, s_dx);
                 if (s > 0) {
                     double worst = 0.0;
@@ -835,7 +1018,7 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
             __syncthreads();
             factor_global<double2, NB64, RPT>(A64, n, n, a.ldp, sm, L, B, R.r, PL, Xx, s_pivlg);
             info = PL.info;
-            lu_solve<double2>(A64, n, n, B, n, R.r, reinterpret_cast<double2 *>(sm + L.tile));
+            lu_solve_strips<double2, 8>(A64, n, n, B, n, R.r, reinterpret_cast<double2 *>(sm + L.panel));
             store_solution(B, n, R, wi.f);
             steps = a.steps_value;
             if (R.ipiv)
