@@ -83,7 +83,7 @@ typedef struct {
     srom_complex *X;        /* F blocks of n x r (ld n): x(w_f) = A(w_f)^-1 rhs      */
     int *info;              /* F ints or NULL                                        */
     int *steps;             /* F ints or NULL: refinement steps taken (-1: FP64 fallback) */
-    double *berr;           /* F doubles or NULL: last relative correction ||d||/||x|| (mixed) */
+    double *berr;           /* F doubles or NULL: estimated relative error left (mixed) */
     srom_complex *LU;       /* F blocks of n x n or NULL (SROM_FLAG_KEEP_FACTORS)    */
     int *ipiv;              /* F blocks of n ints (1-based) or NULL                  */
 } srom_rom_desc;
@@ -91,7 +91,7 @@ typedef struct {
 typedef struct {
     int precision;   /* SROM_FP64 / SROM_MIXED_FP32 / SROM_MIXED_TF32                */
     int max_refine;  /* refinement steps for the mixed forms (default 5 when <= 0)   */
-    double tol;      /* stop refining when ||d||_inf <= tol * ||x||_inf for every RHS; 0 = 2^-33 */
+    double tol;      /* stop refining when the error estimate 2 (||d_s||/||d_s-1||) ||d_s||/||x|| <= tol; 0 = 2^-33 */
     int flags;       /* SROM_FLAG_*                                                  */
 } srom_sweep_opts;
 

@@ -41,8 +41,7 @@ namespace srom {
 
 constexpr int NT = 256;
 constexpr int NW = NT / 32;
-constexpr int CW = 4;      // trailing columns per warp group
-constexpr int RQ = 4;      // Schur rows per lane per pass
+constexpr int CWG = 8;     // trailing columns per warp group
 constexpr int NB64 = 16;   // FP64 panel width
 constexpr int NB32 = 32;   // FP32 panel width
 constexpr int RMAX_SOLVE = 16;  // right-hand sides per solve (register accumulators)
@@ -474,6 +473,7 @@ struct PivotXchg {
 struct PanelLists {
     int nmoved;
     int info;
+    int grp;  // next trailing column group of the current panel
 };
 
 // Factor the m x ncols panel P (physical row order, leading dimension ldp) with partial
@@ -615,8 +615,10 @@ __device__ void panel_factor_par(T *P, int ldp, int m, int ncols, int *s_perm, i
 template <typename T, int NB>
 __device__ void trailing_update(T *A, int64_t lda, int n, int j0, int nbc, const T *P, int ldp,
                                 const int *s_perm, const int *s_mdst, const int *s_msrc, int nmoved,
-                                T *s_u, T *B, int ldbs, int nrhs) {
+                                T *s_u, T *B, int ldbs, int nrhs, int *s_grp) {
     using C = CT<T>;
+    constexpr int CW = CWG;                       // trailing columns per warp group
+    constexpr int RQ = 2;                         // Schur rows per lane per pass
     constexpr int MV = (2 * NB + 31) / 32;
     constexpr int TR = 32 / NB;  // row segments per warp in the triangle solve
     constexpr int TC = CW / TR;  // columns per lane in the triangle solve
@@ -657,7 +659,13 @@ __device__ void trailing_update(T *A, int64_t lda, int n, int j0, int nbc, const
 
     T *u = s_u + warp * NB * CW;
     const int trow = lane % NB, tgrp = lane / NB;
-    for (int c0 = j0 + nbc + warp * CW; c0 < n; c0 += NW * CW) {
+    // column groups are handed out dynamically so that warps finish a panel together
+    for (;;) {
+        int gi = 0;
+        if (lane == 0) gi = atomicAdd(s_grp, 1);
+        gi = __shfl_sync(FULL_MASK, gi, 0);
+        const int c0 = j0 + nbc + gi * CW;
+        if (c0 >= n) break;
         T mv[MV][CW];
         T uv[TC];
 #pragma unroll
@@ -765,8 +773,8 @@ struct GlobalSmem {
     static __host__ __device__ size_t up(size_t b) { return (b + 255) / 256 * 256; }
     __host__ __device__ GlobalSmem(int ldp, int n_max, int r_max) {
         panel = 0;                                         // ldp x 16 double2 == ldp x 32 float2
-        u = panel + up((size_t)ldp * 256);                 // per warp NB x CW complex
-        work64 = u + up((size_t)NW * 1024);
+        u = panel + up((size_t)ldp * 256);                 // per warp NB x CWG complex
+        work64 = u + up((size_t)NW * 2048);
         work32 = work64 + up((size_t)n_max * r_max * 16);
         perm = work32 + up((size_t)n_max * r_max * 8);
         ptot = perm + up((size_t)ldp * 4);
@@ -800,7 +808,10 @@ __device__ void factor_global(T *A, int64_t lda, int n, int ldp, unsigned char *
         const int m = n - j0;
         for (int c = warp; c < nbc; c += NW)
             for (int i = lane; i < m; i += 32) P[i + (int64_t)c * ldp] = A[(j0 + i) + (j0 + c) * lda];
-        if (tid == 0) PL.nmoved = 0;
+        if (tid == 0) {
+            PL.nmoved = 0;
+            PL.grp = 0;
+        }
         __syncthreads();
         panel_factor_par<T, RPT>(P, ldp, m, nbc, s_perm, s_pivlg, s_mdst, s_msrc, PL, j0, X);
         const int nmoved = PL.nmoved;
@@ -822,7 +833,7 @@ __device__ void factor_global(T *A, int64_t lda, int n, int ldp, unsigned char *
             }
             __syncwarp();
         }
-        trailing_update<T, NB>(A, lda, n, j0, nbc, P, ldp, s_perm, s_mdst, s_msrc, nmoved, s_u, B, n, nrhs);
+        trailing_update<T, NB>(A, lda, n, j0, nbc, P, ldp, s_perm, s_mdst, s_msrc, nmoved, s_u, B, n, nrhs, &PL.grp);
         __syncthreads();
     }
 }
@@ -988,15 +999,20 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
             __syncthreads();
             const double tol_x = a.tol > 0.0 ? a.tol : 1.1641532182693481e-10;  // 2^-33
             bool conv = false;
+            double prev = 1.0;  // relative size of the previous correction (the first is x itself)
             for (int s = 0;; ++s) {
                 if (s > 0) residual64<RPT>(R, w, X, B32, s_pos);
                 lu_solve_strips<float2, 16>(A32, n, n, B32, n, R.r, reinterpret_cast<float2 *>(sm + L.panel));
                 apply_correction(X, B32, n, R.r, s_dx);
                 if (s > 0) {
+                    // error left after this correction ~ rho * ||d||, rho ~ ||d_s|| / ||d_{s-1}||
+                    // (the contraction of the iteration), taken twice for safety
                     double worst = 0.0;
                     for (int c = 0; c < R.r; ++c) worst = fmax(worst, s_dx[c]);
-                    berr = worst;
-                    conv = worst <= tol_x;
+                    const double rho = fmin(1.0, 2.0 * worst / prev);
+                    berr = worst * rho;
+                    conv = berr <= tol_x;
+                    prev = worst;
                 }
                 steps = s;
                 if (conv || s >= a.max_refine) break;
