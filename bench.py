@@ -45,6 +45,8 @@ def parse():
                    help="CPU baseline sweeps every k-th frequency of every ROM")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the projection and adjoint side measurements")
     return p.parse_args()
 
 
@@ -199,6 +201,90 @@ def cpu_baseline_leg(roms, stride, gpu_solutions):
                "vs_xref_median": float(np.median(e_ref)), "checked_systems": int(e_ref.size),
                "gate_1e-10": bool(e_ref.max() <= 1e-10)}
     return base, acc
+
+
+# ----------------------------------------------------------------------------- side legs
+
+def projection_leg(torch, dev, h, peaks, reps=5):
+    """V^T K V and V^T M V on the 107,163-DOF Tet10 block (k = 96) and the FP64 Gram-Schmidt
+    of the basis: device time and algorithmic HBM bytes (values + colind + rowptr + V once)."""
+    from staccato_b200 import fe_tet10
+    from staccato_b200.project import DeviceCsr, orthonormalize, project
+
+    m = fe_tet10.clamped_block()
+    k = 96
+    V0 = fe_tet10.basis(m.n_dof, k, seed=1)
+    Vt = torch.from_numpy(np.ascontiguousarray(V0.T)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    orthonormalize(h, Vt.clone(), passes=2)
+    e0.record(stream)
+    orthonormalize(h, Vt, passes=2)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    gs_ms = e0.elapsed_time(e1)
+    csr = DeviceCsr.from_host(m.indptr, m.indices)
+    Kv = torch.from_numpy(m.K).to(dev)
+    Mv = torch.from_numpy(m.M).to(dev)
+    project(h, csr, [Kv, Mv], Vt)
+    torch.cuda.synchronize(dev)
+    h.profile(True)
+    h.read_profile()
+    e0.record(stream)
+    for _ in range(reps):
+        project(h, csr, [Kv, Mv], Vt)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    h.profile(False)
+    recs, _ = h.read_profile()
+    ms = e0.elapsed_time(e1) / reps
+    nnz, N = int(m.indices.shape[0]), m.n_dof
+    alg_bytes = 2 * 8 * nnz + 4 * nnz + 8 * (N + 1) + 8 * N * k
+    flops = 2 * (2 * nnz * k) + 2 * (2 * N * k * k)
+    kms = {}
+    for name, t, *_ in recs:
+        kms[name] = kms.get(name, 0.0) + t / reps
+    hbm = float(peaks.get("hbm_gbs", 0.0)) or None
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    return {"workload": "Tet10 block 10x10x40, h=0.01 m, steel, z=0 clamped; N=107,163, nnz=%d; V 107,163 x 96 seeded N(0,1)" % nnz,
+            "ms_per_projection": ms, "kernels_ms": kms, "gram_schmidt_ms": gs_ms,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": (achieved / hbm) if hbm else None, "traffic": None,
+                         "algorithmic_bytes": alg_bytes,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)"},
+            "fp64_tflops": flops / (ms * 1e-3) / 1e12}
+
+
+def adjoint_leg(torch, dev, h):
+    """Forward FP64 sweep with kept factors + backward call on the differentiation workload
+    (n = 128, 2000 frequencies, 16 stiffness scales + loss factor)."""
+    from staccato_b200 import workloads as W
+    from staccato_b200.adjoint import backward, forward_J, modal_params
+
+    prob = W.adjoint_rom()
+    params = modal_params(prob, device=dev)
+    J0, gbar, d = forward_J(h, prob, keep=True, device=dev)
+    backward(h, d, gbar, params)
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    J0, gbar, d = forward_J(h, prob, keep=True, device=dev)
+    e1.record(stream)
+    g = backward(h, d, gbar, params)
+    e2.record(stream)
+    torch.cuda.synchronize(dev)
+    fwd, bwd = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    # central difference of J in p_0 and eta (relative step 1e-6) against the adjoint
+    gh = g.cpu().numpy()
+    hp = 1e-6
+    pp, pm = prob.p.copy(), prob.p.copy()
+    pp[0] += hp
+    pm[0] -= hp
+    fd0 = (forward_J(h, prob, p=pp, device=dev)[0] - forward_J(h, prob, p=pm, device=dev)[0]) / (2 * hp)
+    return {"workload": "n=128, 2000 freq 1-1500 Hz, 16 stiffness scales + eta, J = sum |c^H x|^2",
+            "forward_ms": fwd, "backward_ms": bwd, "backward_freq_per_s": prob.rom.F / (bwd * 1e-3),
+            "grad_p0": float(gh[0]), "fd_p0": float(fd0), "rel_diff_p0": float(abs(gh[0] - fd0) / abs(fd0))}
 
 
 # ----------------------------------------------------------------------------- arms
@@ -385,6 +471,11 @@ def run_ours(args):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "api": "srom_sweep_host (host buffers in, host results out)"}
 
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        extras["projection"] = projection_leg(torch, dev, h, measured_peaks())
+        extras["adjoint"] = adjoint_leg(torch, dev, h)
+
     cpu = acc = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         def gpu_solutions(i, idx):
@@ -415,6 +506,8 @@ def run_ours(args):
             "e2e": e2e,
             "clocks": clk.summary(),
             "gpu_launches": int(nrec),
+            "projection": extras.get("projection"),
+            "adjoint": extras.get("adjoint"),
         }
         print(json.dumps(line), flush=True)
     if pg is not None:
