@@ -585,7 +585,7 @@ int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *rowptr, con
     if (ldv < n_rows) return set_err(h, SROM_ERR_INVALID, "ldv < n_rows");
     DeviceGuard g(h->device);
     const int kp = (k + 7) & ~7;
-    const int nblk = h->sm_count * 2;
+    const int nblk = h->sm_count;  // one V^T Y CTA per SM
     const size_t vt_b = align_up(sizeof(double) * (size_t)n_rows * k, 256);
     const size_t y_b = align_up(sizeof(double) * (size_t)n_rows * k * n_mats, 256);
     const size_t p_b = align_up(sizeof(double) * (size_t)nblk * n_mats * kp * kp, 256);

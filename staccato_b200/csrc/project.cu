@@ -41,44 +41,154 @@ __global__ void transpose_kernel(const double *__restrict__ V, int64_t N, int k,
 }
 
 // ---- Y_m = A_m V  (full CSR pattern, shared by the n_mats value arrays) -----------------
-template <int CPL>
-__global__ void spmm_full_kernel(int64_t N, const int64_t *__restrict__ rowptr, const int *__restrict__ colind,
-                                 int base, ProjVals vals, int n_mats, const double *__restrict__ Vt, int k,
-                                 double *__restrict__ Y, int64_t y_stride) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t row = warp; row < N; row += nwarp) {
-        double acc[PRJ_MAX_MATS][CPL];
+// A warp takes three consecutive rows.  FE matrices numbered node by node give the three
+// DOF rows of a node the same column pattern; when the warp finds that (equal lengths and
+// equal column lists, checked with a warp vote), every gathered Vt row feeds all three rows
+// and all matrices, cutting the Vt gathers -- the dominant L2 traffic -- by three.  Otherwise
+// the rows are processed one after the other.  The column indices and values of a row are
+// staged 32 entries at a time in the warp's shared-memory slot (coalesced loads), so that
+// the Vt gathers of SPMM_DEPTH consecutive entries are independent loads in flight together.
+// Every Y entry is the sequential FMA chain over the row's entries in storage order.
+constexpr int SPMM_THREADS = 256;
+constexpr int SPMM_WARPS = SPMM_THREADS / 32;
+constexpr int SPMM_DEPTH = 4;
+
+struct SpmmStage {
+    int col[32];
+    double val[3 * PRJ_MAX_MATS][32];
+};
+
+template <int CPL, int NMAT, int NR>
+__device__ __forceinline__ void spmm_rows(int64_t row, const int64_t *__restrict__ rowptr,
+                                          const int *__restrict__ colind, int base, const ProjVals &vals,
+                                          const double *__restrict__ Vt, int k, double *__restrict__ Y,
+                                          int64_t y_stride, int lane, SpmmStage &st) {
+    const int64_t e0 = rowptr[row] - base, e1 = rowptr[row + 1] - base;
+    int64_t off[NR];
 #pragma unroll
-        for (int m = 0; m < PRJ_MAX_MATS; ++m)
+    for (int r = 0; r < NR; ++r) off[r] = (rowptr[row + r] - base) - e0;
+    double acc[NR][NMAT][CPL];
 #pragma unroll
-            for (int q = 0; q < CPL; ++q) acc[m][q] = 0.0;
-        const int64_t e0 = rowptr[row] - base, e1 = rowptr[row + 1] - base;
-        for (int64_t e = e0; e < e1; ++e) {
-            const int64_t col = colind[e] - base;
-            double a[PRJ_MAX_MATS];
+    for (int r = 0; r < NR; ++r)
 #pragma unroll
-            for (int m = 0; m < PRJ_MAX_MATS; ++m) a[m] = m < n_mats ? vals.v[m][e] : 0.0;
-            const double *vr = Vt + col * k;
+        for (int m = 0; m < NMAT; ++m)
+#pragma unroll
+            for (int q = 0; q < CPL; ++q) acc[r][m][q] = 0.0;
+    for (int64_t c0 = e0; c0 < e1; c0 += 32) {
+        const int cnt = (int)min((int64_t)32, e1 - c0);
+        __syncwarp();
+        if (lane < cnt) {
+            st.col[lane] = colind[c0 + lane] - base;
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+#pragma unroll
+                for (int m = 0; m < NMAT; ++m) st.val[r * NMAT + m][lane] = vals.v[m][c0 + lane + off[r]];
+        }
+        __syncwarp();
+        int j = 0;
+        for (; j + SPMM_DEPTH <= cnt; j += SPMM_DEPTH) {
+            double v[SPMM_DEPTH][CPL];
+#pragma unroll
+            for (int u = 0; u < SPMM_DEPTH; ++u) {
+                const double *vr = Vt + (int64_t)st.col[j + u] * k;
+#pragma unroll
+                for (int q = 0; q < CPL; ++q) {
+                    const int c = lane + 32 * q;
+                    v[u][q] = c < k ? vr[c] : 0.0;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < SPMM_DEPTH; ++u)
+#pragma unroll
+                for (int r = 0; r < NR; ++r)
+#pragma unroll
+                    for (int m = 0; m < NMAT; ++m) {
+                        const double a = st.val[r * NMAT + m][j + u];
+#pragma unroll
+                        for (int q = 0; q < CPL; ++q) acc[r][m][q] = fma(a, v[u][q], acc[r][m][q]);
+                    }
+        }
+        for (; j < cnt; ++j) {
+            const double *vr = Vt + (int64_t)st.col[j] * k;
 #pragma unroll
             for (int q = 0; q < CPL; ++q) {
                 const int c = lane + 32 * q;
                 const double v = c < k ? vr[c] : 0.0;
 #pragma unroll
-                for (int m = 0; m < PRJ_MAX_MATS; ++m) acc[m][q] = fma(a[m], v, acc[m][q]);
-            }
-        }
+                for (int r = 0; r < NR; ++r)
 #pragma unroll
-        for (int m = 0; m < PRJ_MAX_MATS; ++m) {
-            if (m >= n_mats) break;
-#pragma unroll
-            for (int q = 0; q < CPL; ++q) {
-                const int c = lane + 32 * q;
-                if (c < k) Y[m * y_stride + row * k + c] = acc[m][q];
+                    for (int m = 0; m < NMAT; ++m) acc[r][m][q] = fma(st.val[r * NMAT + m][j], v, acc[r][m][q]);
             }
         }
     }
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+#pragma unroll
+        for (int m = 0; m < NMAT; ++m)
+#pragma unroll
+            for (int q = 0; q < CPL; ++q) {
+                const int c = lane + 32 * q;
+                if (c < k) Y[m * y_stride + (row + r) * k + c] = acc[r][m][q];
+            }
+}
+
+template <int CPL, int NMAT>
+__global__ void __launch_bounds__(SPMM_THREADS) spmm_full_kernel(int64_t N, const int64_t *__restrict__ rowptr,
+                                                                 const int *__restrict__ colind, int base,
+                                                                 ProjVals vals, const double *__restrict__ Vt, int k,
+                                                                 double *__restrict__ Y, int64_t y_stride) {
+    __shared__ SpmmStage stage[SPMM_WARPS];
+    const int lane = threadIdx.x & 31;
+    SpmmStage &st = stage[threadIdx.x >> 5];
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r0 = warp * 3; r0 < N; r0 += nwarp * 3) {
+        const int nr = (int)min((int64_t)3, N - r0);
+        bool same = nr == 3;
+        if (same) {
+            const int64_t a0 = rowptr[r0], a1 = rowptr[r0 + 1], a2 = rowptr[r0 + 2], a3 = rowptr[r0 + 3];
+            const int64_t len = a1 - a0;
+            same = (a2 - a1) == len && (a3 - a2) == len;
+            // the trip count is warp-uniform, so every lane takes part in every vote
+            for (int64_t t0 = 0; same && t0 < len; t0 += 32) {
+                const int64_t t = t0 + lane;
+                bool eq = true;
+                if (t < len) {
+                    const int c0 = colind[a0 - base + t];
+                    eq = c0 == colind[a1 - base + t] && c0 == colind[a2 - base + t];
+                }
+                same = __all_sync(0xffffffffu, eq);
+            }
+        }
+        if (same) {
+            spmm_rows<CPL, NMAT, 3>(r0, rowptr, colind, base, vals, Vt, k, Y, y_stride, lane, st);
+        } else {
+            for (int r = 0; r < nr; ++r)
+                spmm_rows<CPL, NMAT, 1>(r0 + r, rowptr, colind, base, vals, Vt, k, Y, y_stride, lane, st);
+        }
+    }
+}
+
+// grid = at most one wave of resident CTAs (the row loop is grid-strided)
+template <int CPL, int NMAT>
+static void spmm_full_launch(int grid, cudaStream_t st, int64_t N, const int64_t *rowptr, const int *colind,
+                             int base, const ProjVals &vals, const double *Vt, int k, double *Y, int64_t y_stride) {
+    int per_sm = 0, dev = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmm_full_kernel<CPL, NMAT>, SPMM_THREADS, 0) ==
+            cudaSuccess &&
+        cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && per_sm > 0)
+        grid = std::min(grid, per_sm * sms);
+    spmm_full_kernel<CPL, NMAT><<<grid, SPMM_THREADS, 0, st>>>(N, rowptr, colind, base, vals, Vt, k, Y, y_stride);
+}
+
+template <int CPL>
+static void launch_spmm_full(int grid, cudaStream_t st, int64_t N, const int64_t *rowptr, const int *colind,
+                             int base, const ProjVals &vals, int n_mats, const double *Vt, int k, double *Y,
+                             int64_t y_stride) {
+    if (n_mats == 1) spmm_full_launch<CPL, 1>(grid, st, N, rowptr, colind, base, vals, Vt, k, Y, y_stride);
+    else if (n_mats == 2) spmm_full_launch<CPL, 2>(grid, st, N, rowptr, colind, base, vals, Vt, k, Y, y_stride);
+    else spmm_full_launch<CPL, 3>(grid, st, N, rowptr, colind, base, vals, Vt, k, Y, y_stride);
 }
 
 // Upper-triangle storage of a symmetric matrix (the reference's CSR,
@@ -105,71 +215,98 @@ __global__ void spmm_upper_mirror_kernel(int64_t N, const int64_t *__restrict__ 
 }
 
 // ---- R_m partial = Vt[rows]^T Y_m[rows] on FP64 tensor cores ------------------------------
-// One warp per 8-row band of R (kp/8 warps), 8x8 tiles across the band; rows of Vt / Y are
-// staged 32 at a time in shared memory (leading dimension kp + 4 keeps the fragment loads
-// free of bank conflicts).
-template <int NMAT>
-__global__ void __launch_bounds__(512) vty_partial_kernel(int64_t N, int k, const double *__restrict__ Vt, const double *__restrict__ Y,
-                                   int64_t y_stride, int64_t rows_per_cta, double *__restrict__ partial) {
+// One launch covers nm matrices.  Warp w owns matrix w / ntile and the 8-row band w % ntile
+// of its R (ntile = kp / 8 bands, 8x8 tiles across the band).  The rows of Vt and of the nm
+// Y's are staged 32 at a time in shared memory (leading dimension kp + 4 keeps the fragment
+// loads free of bank conflicts); the Vt chunk is staged once for all nm matrices, and the
+// chunks are double-buffered with cp.async so the loads of chunk c + 1 overlap the MMAs of
+// chunk c.  Each CTA takes a contiguous range of chunks and writes a private k x k partial.
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src));
+}
+
+template <int TMAX, int MAXT>
+__global__ void __launch_bounds__(MAXT) vty_partial_kernel(int64_t N, int k, const double *__restrict__ Vt,
+                                                           const double *__restrict__ Y, int64_t y_stride, int nm,
+                                                           int64_t chunks_per_cta, double *__restrict__ partial) {
     extern __shared__ double sh[];
     const int kp = (k + 7) & ~7;
     const int ld = kp + 4;
-    double *sV = sh;
-    double *sY = sh + 32 * ld;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ntile = kp / 8;
-    const int64_t r_begin = (int64_t)blockIdx.x * rows_per_cta;
-    const int64_t r_end = min(N, r_begin + rows_per_cta);
-    double acc[NMAT][16][2];
+    const int stage = (1 + nm) * 32 * ld;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int mloc = warp / ntile, band = warp % ntile;
+    const bool active = mloc < nm;
+    const int64_t n_chunks = (N + 31) / 32;
+    const int64_t c_begin = (int64_t)blockIdx.x * chunks_per_cta;
+    const int64_t c_end = min(n_chunks, c_begin + chunks_per_cta);
+    const int per_mat = 32 * kp;
+    const int total = (1 + nm) * per_mat;
+
+    auto issue = [&](int64_t ch, int buf) {
+        double *dst0 = sh + buf * stage;
+        const int64_t r0 = ch * 32;
+        const int nr = (int)min((int64_t)32, N - r0);
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+            const int mat = e / per_mat, rem = e - mat * per_mat;
+            const int rr = rem / kp, c = rem - rr * kp;
+            double *dst = dst0 + mat * 32 * ld + rr * ld + c;
+            if (rr < nr && c < k) {
+                const double *src = mat == 0 ? Vt + (r0 + rr) * k + c : Y + (mat - 1) * y_stride + (r0 + rr) * k + c;
+                cp_async8(dst, src);
+            } else {
+                *dst = 0.0;
+            }
+        }
+        asm volatile("cp.async.commit_group;");
+    };
+
+    double acc[TMAX][2];
 #pragma unroll
-    for (int m = 0; m < NMAT; ++m)
-#pragma unroll
-        for (int t = 0; t < 16; ++t) acc[m][t][0] = acc[m][t][1] = 0.0;
-    for (int64_t r0 = r_begin; r0 < r_end; r0 += 32) {
-        const int nr = (int)min((int64_t)32, r_end - r0);
-        for (int e = threadIdx.x; e < 32 * kp; e += blockDim.x) {
-            const int rr = e / kp, c = e % kp;
-            const bool ok = rr < nr && c < k;
-            sV[rr * ld + c] = ok ? Vt[(r0 + rr) * k + c] : 0.0;
-#pragma unroll
-            for (int m = 0; m < NMAT; ++m) sY[m * 32 * ld + rr * ld + c] = ok ? Y[m * y_stride + (r0 + rr) * k + c] : 0.0;
+    for (int t = 0; t < TMAX; ++t) acc[t][0] = acc[t][1] = 0.0;
+    if (c_begin < c_end) issue(c_begin, 0);
+    for (int64_t ch = c_begin; ch < c_end; ++ch) {
+        const int buf = (int)((ch - c_begin) & 1);
+        if (ch + 1 < c_end) {
+            issue(ch + 1, buf ^ 1);
+            asm volatile("cp.async.wait_group 1;");
+        } else {
+            asm volatile("cp.async.wait_group 0;");
         }
         __syncthreads();
-        if (warp < ntile) {
+        if (active) {
+            const double *sV = sh + buf * stage;
+            const double *sY = sV + (1 + mloc) * 32 * ld;
 #pragma unroll
             for (int kk = 0; kk < 8; ++kk) {
                 const int rr = 4 * kk + (lane & 3);
-                const double a = sV[rr * ld + 8 * warp + (lane >> 2)];
+                const double a = sV[rr * ld + 8 * band + (lane >> 2)];
 #pragma unroll
-                for (int t = 0; t < 16; ++t) {
+                for (int t = 0; t < TMAX; ++t) {
                     if (t < ntile) {
-#pragma unroll
-                        for (int m = 0; m < NMAT; ++m) {
-                            const double b = sY[m * 32 * ld + rr * ld + 8 * t + (lane >> 2)];
-                            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-                                         : "+d"(acc[m][t][0]), "+d"(acc[m][t][1])
-                                         : "d"(a), "d"(b));
-                        }
+                        const double b = sY[rr * ld + 8 * t + (lane >> 2)];
+                        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                                     : "+d"(acc[t][0]), "+d"(acc[t][1])
+                                     : "d"(a), "d"(b));
                     }
                 }
             }
         }
         __syncthreads();
     }
-    if (warp < ntile) {
-        // lane holds D[row = lane/4][col = 2*(lane%4) + {0,1}] of tile (warp, t)
-        const int ra = 8 * warp + (lane >> 2);
+    if (active) {
+        // lane holds D[row = lane/4][col = 2*(lane%4) + {0,1}] of tile (band, t)
+        const int ra = 8 * band + (lane >> 2);
+        double *P = partial + ((int64_t)mloc * gridDim.x + blockIdx.x) * kp * kp;
 #pragma unroll
-        for (int m = 0; m < NMAT; ++m)
-#pragma unroll
-            for (int t = 0; t < 16; ++t) {
-                if (t < ntile) {
-                    const int cb = 8 * t + 2 * (lane & 3);
-                    double *P = partial + ((int64_t)m * gridDim.x + blockIdx.x) * kp * kp;
-                    P[ra + (int64_t)cb * kp] = acc[m][t][0];
-                    P[ra + (int64_t)(cb + 1) * kp] = acc[m][t][1];
-                }
+        for (int t = 0; t < TMAX; ++t) {
+            if (t < ntile) {
+                const int cb = 8 * t + 2 * (lane & 3);
+                P[ra + (int64_t)cb * kp] = acc[t][0];
+                P[ra + (int64_t)(cb + 1) * kp] = acc[t][1];
             }
+        }
     }
 }
 
@@ -246,39 +383,61 @@ cudaError_t launch_transpose(const double *V, int64_t N, int k, int64_t ldv, dou
 
 cudaError_t launch_spmm(int64_t N, const int64_t *rowptr, const int *colind, int base, int upper, ProjVals vals,
                         int n_mats, const double *Vt, int k, double *Y, int64_t y_stride, int sms, cudaStream_t st) {
-    const int threads = 256;
-    const int64_t warps_needed = N;
+    const int threads = SPMM_THREADS;
+    const int64_t warps_needed = (N + 2) / 3;
     int grid = (int)std::min<int64_t>((warps_needed * 32 + threads - 1) / threads, (int64_t)sms * 8);
-    if (k <= 32) spmm_full_kernel<1><<<grid, threads, 0, st>>>(N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
-    else if (k <= 64) spmm_full_kernel<2><<<grid, threads, 0, st>>>(N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
-    else if (k <= 96) spmm_full_kernel<3><<<grid, threads, 0, st>>>(N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
-    else spmm_full_kernel<4><<<grid, threads, 0, st>>>(N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
+    if (k <= 32) launch_spmm_full<1>(grid, st, N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
+    else if (k <= 64) launch_spmm_full<2>(grid, st, N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
+    else if (k <= 96) launch_spmm_full<3>(grid, st, N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
+    else launch_spmm_full<4>(grid, st, N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !upper) return e;
     spmm_upper_mirror_kernel<<<grid, threads, 0, st>>>(N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
     return cudaGetLastError();
 }
 
+// matrices per launch: 24 warps at most for up to 12 bands (<= 80 registers a thread),
+// one matrix of up to 16 bands (512 threads)
+static int vty_group(int k, int n_mats) {
+    const int ntile = ((k + 7) & ~7) / 8;
+    return ntile > 12 ? 1 : std::max(1, std::min(n_mats, 24 / ntile));
+}
+
 size_t vty_smem_bytes(int k, int n_mats) {
-    (void)n_mats;
     const int kp = (k + 7) & ~7;
-    return sizeof(double) * (size_t)32 * (kp + 4) * 2;
+    return sizeof(double) * (size_t)2 * (1 + vty_group(k, n_mats)) * 32 * (kp + 4);
+}
+
+template <int TMAX, int MAXT>
+static cudaError_t vty_launch(int64_t N, int k, const double *Vt, const double *Y, int64_t y_stride, int nm,
+                              int nblk, double *partial, cudaStream_t st) {
+    const int kp = (k + 7) & ~7;
+    const int threads = 32 * nm * (kp / 8);
+    const size_t smem = sizeof(double) * (size_t)2 * (1 + nm) * 32 * (kp + 4);
+    auto kf = vty_partial_kernel<TMAX, MAXT>;
+    cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int64_t n_chunks = (N + 31) / 32;
+    const int64_t per = (n_chunks + nblk - 1) / nblk;
+    kf<<<nblk, threads, smem, st>>>(N, k, Vt, Y, y_stride, nm, per, partial);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_vty(int64_t N, int k, const double *Vt, const double *Y, int64_t y_stride, int n_mats,
                        int nblk, double *partial, ProjOut out, cudaStream_t st) {
     const int kp = (k + 7) & ~7;
-    const int threads = 32 * (kp / 8);
-    const int64_t rows_per = (N + nblk - 1) / nblk;
-    const size_t smem = vty_smem_bytes(k, n_mats);
-    // one launch per matrix: the k x k accumulators of one matrix already take ~100 registers
-    auto kf = vty_partial_kernel<1>;
-    cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    for (int m = 0; m < n_mats; ++m) {
-        kf<<<nblk, threads, smem, st>>>(N, k, Vt, Y + m * y_stride, y_stride,
-                                        rows_per, partial + (int64_t)m * nblk * kp * kp);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int ntile = kp / 8;
+    const int group = vty_group(k, n_mats);
+    for (int m0 = 0; m0 < n_mats; m0 += group) {
+        const int nm = std::min(group, n_mats - m0);
+        const double *Ym = Y + m0 * y_stride;
+        double *Pm = partial + (int64_t)m0 * nblk * kp * kp;
+        cudaError_t e;
+        if (ntile <= 4) e = vty_launch<4, 768>(N, k, Vt, Ym, y_stride, nm, nblk, Pm, st);
+        else if (ntile <= 8) e = vty_launch<8, 768>(N, k, Vt, Ym, y_stride, nm, nblk, Pm, st);
+        else if (ntile <= 12) e = vty_launch<12, 768>(N, k, Vt, Ym, y_stride, nm, nblk, Pm, st);
+        else e = vty_launch<16, 512>(N, k, Vt, Ym, y_stride, nm, nblk, Pm, st);
+        if (e != cudaSuccess) return e;
     }
     reduce_partials_kernel<<<(n_mats * k * k + 255) / 256, 256, 0, st>>>(partial, nblk, n_mats, k, kp, out);
     return cudaGetLastError();

@@ -56,6 +56,35 @@ def test_projection_random(handle, k, base, upper):
         assert np.abs(R - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("k", [17, 96])
+def test_projection_node_blocked_pattern(handle, k):
+    """3x3-blocked pattern (rows of a node share their columns) with some node triples broken
+    (one entry dropped) and a trailing partial node: both SpMM row paths in one matrix."""
+    nn = 701
+    P = sp.random(nn, nn, density=0.03, random_state=11, format="csr")
+    P = (P + P.T + sp.eye(nn)).tocsr()
+    A = sp.kron(P, np.ones((3, 3)), format="csr")[: 3 * nn - 1, : 3 * nn - 1].tocsr()
+    A.sort_indices()
+    A = A.tolil()
+    rng = np.random.default_rng(5)
+    for node in rng.choice(nn - 1, 40, replace=False):
+        row = 3 * node + int(rng.integers(3))
+        cols = A.rows[row]
+        if len(cols) > 1:
+            A[row, cols[-1]] = 0.0
+    A = A.tocsr()
+    A.eliminate_zeros()
+    A.sort_indices()
+    n = A.shape[0]
+    va, vb = rng.standard_normal(A.nnz), rng.standard_normal(A.nnz)
+    V = np.asfortranarray(rng.standard_normal((n, k)))
+    csr = DeviceCsr.from_host(A.indptr, A.indices)
+    RA, RB = project(handle, csr, [_dev(va), _dev(vb)], _dev(np.ascontiguousarray(V.T)))
+    for R, vals in ((RA, va), (RB, vb)):
+        ref = O.project(A.indptr, A.indices, vals, V)
+        assert np.abs(R.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
 def test_projection_identity_basis_extracts_block(handle):
     n, k = 400, 24
     A, B = _rand_sym_csr(n, 0.05, 3)
