@@ -193,11 +193,14 @@ SROM_API int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *ro
                                double *const *R);
 
 /*
- * FP64 Gram-Schmidt orthonormalisation of V (n_rows x k, column-major, ldv) in place:
- * each column is projected out of the previous ones `passes` times (classical projections,
- * two passes keep the basis orthonormal to rounding level) and normalised -- the column-wise
- * form of the reference's block Gram-Schmidt with re-orthogonalisation
- * (KrylovROMSubstructure.cpp:433-454, :513-534).
+ * FP64 block Gram-Schmidt orthonormalisation of V (n_rows x k, column-major, ldv) in place,
+ * the reference's block scheme with re-orthogonalisation (KrylovROMSubstructure.cpp:433-475,
+ * :513-534): the columns are taken in panels of 32; each pass projects the panel out of the
+ * orthonormal columns before it and orthonormalises it through the Cholesky factor of its
+ * projected Gram matrix.  `passes` passes are made per panel (0 is taken as 1; two keep the
+ * basis orthonormal to rounding level for condition numbers up to about 1e7).  The result is
+ * the Q of V = Q R with a positive diagonal R.  Columns that are linearly dependent on the
+ * ones before them come out non-finite (no rank revealing).
  */
 SROM_API int srom_orthonormalize(srom_handle *h, double *V, int64_t n_rows, int k, int64_t ldv, int passes);
 

@@ -710,13 +710,12 @@ int srom_orthonormalize(srom_handle *h, double *V, int64_t n_rows, int k, int64_
     if (k > n_rows) return set_err(h, SROM_ERR_INVALID, "k > n_rows: columns cannot be orthonormal");
     DeviceGuard g(h->device);
     const int nblk = h->sm_count;
-    const size_t need = sizeof(double) * ((size_t)nblk * (k + 1) + (k + 1));
+    const size_t need = sizeof(double) * srom::gs_workspace_doubles(k, nblk);
     int s = ensure_device_buffer(h, &h->d_proj, &h->d_proj_bytes, need);
     if (s) return s;
-    double *part = static_cast<double *>(h->d_proj);
-    double *hv = part + (size_t)nblk * (k + 1);
     ProfScope ps(h, "gram_schmidt", k, 4.0 * (double)n_rows * k * k * std::max(passes, 1), 0.0);
-    SROM_CUDA(h, srom::launch_gram_schmidt(V, n_rows, k, ldv, passes, part, hv, nblk, h->stream));
+    SROM_CUDA(h, srom::launch_gram_schmidt(V, n_rows, k, ldv, passes, static_cast<double *>(h->d_proj), nblk,
+                                           h->stream));
     return SROM_OK;
 }
 

@@ -323,55 +323,223 @@ __global__ void reduce_partials_kernel(const double *__restrict__ partial, int n
     }
 }
 
-// ---- classical Gram-Schmidt with re-orthogonalisation, one column at a time ---------------
-// h = V[:, :j]^T v_j (per-CTA partials + fixed-order reduction), v_j -= V[:, :j] h; twice;
-// then v_j /= ||v_j||.  Column-major V (N x k, ldv).
-__global__ void gs_dots_kernel(const double *__restrict__ V, int64_t N, int64_t ldv, int j,
-                               double *__restrict__ part) {
-    // part[blk * (j+1) + i] = sum over this CTA's rows of V[r, i] * V[r, j], i <= j
-    extern __shared__ double red[];
-    const int64_t rows_per = (N + gridDim.x - 1) / gridDim.x;
-    const int64_t r0 = (int64_t)blockIdx.x * rows_per, r1 = min(N, r0 + rows_per);
-    const int nw = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = 0; i <= j; ++i) {
-        double s = 0.0;
-        for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) s = fma(V[r + i * ldv], V[r + j * ldv], s);
+// ---- block Gram-Schmidt with re-orthogonalisation --------------------------------------
+// The columns of V (column-major, N x k, ldv) are taken in panels P of GS_B columns.  One pass
+// over a panel with the orthonormal columns Q = V[:, :j0] before it:
+//     C = [Q P]^T P                 (one reduction: H = Q^T P on top, G = P^T P below)
+//     R^T R = G - H^T H             (Cholesky; the Gram matrix of P - Q H by Pythagoras)
+//     P <- (P - Q H) R^-1
+// and `passes` passes are made (two keep the basis orthonormal to rounding level).  This is
+// the reference's block scheme -- block projection against V repeated, then an orthonormal
+// basis of the block (KrylovROMSubstructure.cpp:433-475, :513-534) -- with the QR of the block
+// taken through its Gram matrix so that every pass is one reduction and one row update.
+constexpr int GS_B = 32;        // panel width
+constexpr int GS_WIN = 128;     // columns of [Q P] per reduction launch (16 bands of 8)
+constexpr int GS_LDR = 36;      // staged column stride (32 rows + 4: conflict-free fragments)
+constexpr int GS_THREADS = 512;
+constexpr int GS_HCHUNK = 128;  // rows of H staged per round of the row update
+
+// part[blk][x0 + i][c] = sum over this CTA's rows of V[r, x0 + i] * V[r, j0 + c]
+// (i < w, c < b), on the FP64 tensor cores; chunks of 32 rows double-buffered with cp.async.
+__global__ void __launch_bounds__(GS_THREADS) gs_gram_kernel(const double *__restrict__ V, int64_t N, int64_t ldv,
+                                                             int x0, int w, int j0, int b, int rows_c,
+                                                             int64_t chunks_per_cta, double *__restrict__ part) {
+    extern __shared__ double sh[];
+    const int wp = (w + 7) & ~7, bp = (b + 7) & ~7;
+    const int stage = (wp + bp) * GS_LDR;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nband = wp / 8, ntile = bp / 8;
+    const int64_t n_chunks = (N + 31) / 32;
+    const int64_t c_begin = (int64_t)blockIdx.x * chunks_per_cta;
+    const int64_t c_end = min(n_chunks, c_begin + chunks_per_cta);
+    const int total = (wp + bp) * 32;
+
+    auto issue = [&](int64_t ch, int buf) {
+        double *dst0 = sh + buf * stage;
+        const int64_t r0 = ch * 32;
+        const int nr = (int)min((int64_t)32, N - r0);
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+            const int col = e >> 5, rr = e & 31;  // staged column col: X for col < wp, P after
+            const bool isx = col < wp;
+            const int cc = isx ? col : col - wp;
+            const bool ok = rr < nr && (isx ? cc < w : cc < b);
+            double *dst = dst0 + col * GS_LDR + rr;
+            if (ok) {
+                const int64_t vc = isx ? x0 + cc : j0 + cc;
+                const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(V + r0 + rr + vc * ldv));
+            } else {
+                *dst = 0.0;
+            }
+        }
+        asm volatile("cp.async.commit_group;");
+    };
+
+    double acc[4][2];
 #pragma unroll
-        for (int off = 16; off; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-        if (lane == 0) red[warp] = s;
+    for (int t = 0; t < 4; ++t) acc[t][0] = acc[t][1] = 0.0;
+    if (c_begin < c_end) issue(c_begin, 0);
+    for (int64_t ch = c_begin; ch < c_end; ++ch) {
+        const int buf = (int)((ch - c_begin) & 1);
+        if (ch + 1 < c_end) {
+            issue(ch + 1, buf ^ 1);
+            asm volatile("cp.async.wait_group 1;");
+        } else {
+            asm volatile("cp.async.wait_group 0;");
+        }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            double t = 0.0;
-            for (int w = 0; w < nw; ++w) t += red[w];
-            part[(int64_t)blockIdx.x * (j + 1) + i] = t;
+        if (warp < nband) {
+            const double *sX = sh + buf * stage;
+            const double *sP = sX + wp * GS_LDR;
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {
+                const int rr = 4 * kk + (lane & 3);
+                const double a = sX[(8 * warp + (lane >> 2)) * GS_LDR + rr];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    if (t < ntile) {
+                        const double bv = sP[(8 * t + (lane >> 2)) * GS_LDR + rr];
+                        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                                     : "+d"(acc[t][0]), "+d"(acc[t][1])
+                                     : "d"(a), "d"(bv));
+                    }
+                }
+            }
         }
         __syncthreads();
     }
+    if (warp < nband) {
+        const int i = x0 + 8 * warp + (lane >> 2);
+        double *P = part + (int64_t)blockIdx.x * rows_c * GS_B;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int c = 8 * t + 2 * (lane & 3);
+            if (i < rows_c) {  // tiles past b hold zeros
+                P[(int64_t)i * GS_B + c] = acc[t][0];
+                P[(int64_t)i * GS_B + c + 1] = acc[t][1];
+            }
+        }
+    }
 }
 
-__global__ void gs_reduce_kernel(const double *__restrict__ part, int nblk, int j, double *__restrict__ h) {
-    for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+// C[i][c] = sum_blk part[blk][i][c] in CTA order (deterministic)
+__global__ void gs_reduce_kernel(const double *__restrict__ part, int nblk, int rows_c, double *__restrict__ Cm) {
+    const int64_t tot = (int64_t)rows_c * GS_B;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
         double s = 0.0;
-        for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * (j + 1) + i];
-        h[i] = s;
+        for (int blk = 0; blk < nblk; ++blk) s += part[(int64_t)blk * tot + e];
+        Cm[e] = s;
     }
 }
 
-__global__ void gs_update_kernel(double *__restrict__ V, int64_t N, int64_t ldv, int j, const double *__restrict__ h) {
-    extern __shared__ double hs[];
-    for (int i = threadIdx.x; i < j; i += blockDim.x) hs[i] = h[i];
+// One CTA: G' = G - H^T H, Cholesky R^T R = G', Rinv = R^-1 (upper), written to rinv[a][c].
+__global__ void gs_chol_kernel(const double *__restrict__ Cm, int j0, int b, double *__restrict__ rinv) {
+    __shared__ double G[GS_B][GS_B + 1];
+    __shared__ double R[GS_B][GS_B + 1];
+    for (int e = threadIdx.x; e < GS_B * GS_B; e += blockDim.x) {
+        const int a = e / GS_B, c = e % GS_B;
+        double g = 0.0;
+        if (a < b && c < b) {
+            g = Cm[(int64_t)(j0 + a) * GS_B + c];
+            double s = 0.0;
+            for (int i = 0; i < j0; ++i) s = fma(Cm[(int64_t)i * GS_B + a], Cm[(int64_t)i * GS_B + c], s);
+            g -= s;
+        }
+        G[a][c] = g;
+        R[a][c] = 0.0;
+    }
     __syncthreads();
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x) {
-        double v = V[r + j * ldv];
-        for (int i = 0; i < j; ++i) v = fma(-hs[i], V[r + i * ldv], v);
-        V[r + j * ldv] = v;
+    // right-looking Cholesky of the symmetric G' (upper factor R, row by row)
+    for (int j = 0; j < b; ++j) {
+        const double d = sqrt(G[j][j]);
+        __syncthreads();
+        for (int c = j + threadIdx.x; c < b; c += blockDim.x) R[j][c] = c == j ? d : G[j][c] / d;
+        __syncthreads();
+        for (int e = threadIdx.x; e < (b - j - 1) * (b - j - 1); e += blockDim.x) {
+            const int a = j + 1 + e / (b - j - 1), c = j + 1 + e % (b - j - 1);
+            G[a][c] = fma(-R[j][a], R[j][c], G[a][c]);
+        }
+        __syncthreads();
+    }
+    // Rinv column c by back substitution: R x = e_c, one thread per column
+    for (int c = threadIdx.x; c < GS_B; c += blockDim.x) {
+        double x[GS_B];
+#pragma unroll
+        for (int i = 0; i < GS_B; ++i) x[i] = 0.0;
+        if (c < b) {
+            for (int i = c; i >= 0; --i) {
+                double s = i == c ? 1.0 : 0.0;
+                for (int l = i + 1; l <= c; ++l) s = fma(-R[i][l], x[l], s);
+                x[i] = s / R[i][i];
+            }
+        }
+        for (int i = 0; i < GS_B; ++i) rinv[i * GS_B + c] = x[i];
     }
 }
 
-__global__ void gs_scale_kernel(double *__restrict__ V, int64_t N, int64_t ldv, int j, const double *__restrict__ h) {
-    const double s = 1.0 / sqrt(h[j]);
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x)
-        V[r + j * ldv] *= s;
+// Two threads per row, 16 panel columns each: p <- (p - q H) Rinv with q = V[r, :j0] and
+// p = V[r, j0:j0+b].  Lane l of a warp takes row (l & 15) and columns 16 (l >> 4) ...; the
+// upper half reads the lower half's p through shuffles for the triangular product.
+constexpr int GS_HALF = GS_B / 2;
+__global__ void __launch_bounds__(256, 2) gs_update_kernel(double *__restrict__ V, int64_t N, int64_t ldv, int j0, int b,
+                                                        const double *__restrict__ Cm, const double *__restrict__ rinv) {
+    __shared__ __align__(16) double Hs[GS_HCHUNK * GS_B];
+    __shared__ __align__(16) double Rs[GS_B * GS_B];
+    for (int e = threadIdx.x; e < GS_B * GS_B; e += blockDim.x) Rs[e] = rinv[e];
+    const int lane = threadIdx.x & 31, half = lane >> 4;
+    const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x - lane) / 2 + (lane & 15);
+    const bool live = r < N;
+    const int cb = half * GS_HALF;
+    double p[GS_HALF];
+#pragma unroll
+    for (int c = 0; c < GS_HALF; ++c) p[c] = (live && cb + c < b) ? V[r + (int64_t)(j0 + cb + c) * ldv] : 0.0;
+    for (int i0 = 0; i0 < j0; i0 += GS_HCHUNK) {
+        const int ni = min(GS_HCHUNK, j0 - i0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < ni * GS_B; e += blockDim.x) Hs[e] = Cm[(int64_t)i0 * GS_B + e];
+        __syncthreads();
+        if (live) {
+#pragma unroll 4
+            for (int i = 0; i < ni; ++i) {
+                const double q = V[r + (int64_t)(i0 + i) * ldv];
+                const double2 *h2 = reinterpret_cast<const double2 *>(Hs + i * GS_B + cb);
+#pragma unroll
+                for (int c2 = 0; c2 < GS_HALF / 2; ++c2) {
+                    const double2 hv = h2[c2];
+                    p[2 * c2] = fma(-q, hv.x, p[2 * c2]);
+                    p[2 * c2 + 1] = fma(-q, hv.y, p[2 * c2 + 1]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // p <- p Rinv (upper): column c takes the row's p[0..c]
+    double o[GS_HALF];
+#pragma unroll
+    for (int u = 0; u < GS_HALF; ++u) o[u] = 0.0;
+#pragma unroll
+    for (int i = 0; i < GS_HALF; ++i) {
+        const double lo = __shfl_sync(0xffffffffu, p[i], lane & 15);  // the row's p[i], i < 16
+#pragma unroll
+        for (int u = 0; u < GS_HALF; ++u) {
+            if (half == 0) {
+                if (i <= u) o[u] = fma(lo, Rs[i * GS_B + u], o[u]);
+            } else {
+                o[u] = fma(lo, Rs[i * GS_B + GS_HALF + u], o[u]);
+            }
+        }
+    }
+    if (half == 1) {
+#pragma unroll
+        for (int i = 0; i < GS_HALF; ++i)
+#pragma unroll
+            for (int u = 0; u < GS_HALF; ++u)
+                if (i <= u) o[u] = fma(p[i], Rs[(GS_HALF + i) * GS_B + GS_HALF + u], o[u]);
+    }
+    if (!live) return;
+#pragma unroll
+    for (int c = 0; c < GS_HALF; ++c)
+        if (cb + c < b) V[r + (int64_t)(j0 + cb + c) * ldv] = o[c];
 }
 
 // ---- host launchers -------------------------------------------------------------------------
@@ -443,21 +611,38 @@ cudaError_t launch_vty(int64_t N, int k, const double *Vt, const double *Y, int6
     return cudaGetLastError();
 }
 
-cudaError_t launch_gram_schmidt(double *V, int64_t N, int k, int64_t ldv, int passes, double *part, double *h,
-                                int nblk, cudaStream_t st) {
-    const int threads = 256;
-    int ugrid = (int)std::min<int64_t>((N + threads - 1) / threads, (int64_t)nblk * 4);
-    for (int j = 0; j < k; ++j) {
-        for (int p = 0; p < passes && j > 0; ++p) {
-            gs_dots_kernel<<<nblk, threads, sizeof(double) * (threads / 32), st>>>(V, N, ldv, j - 1 + 1, part);
-            gs_reduce_kernel<<<1, 256, 0, st>>>(part, nblk, j, h);
-            gs_update_kernel<<<ugrid, threads, sizeof(double) * (size_t)j, st>>>(V, N, ldv, j, h);
+size_t gs_workspace_doubles(int k, int nblk) {
+    const size_t rows_c = (size_t)((k + 7) & ~7) + GS_B;
+    return (size_t)nblk * rows_c * GS_B + rows_c * GS_B + (size_t)GS_B * GS_B;
+}
+
+cudaError_t launch_gram_schmidt(double *V, int64_t N, int k, int64_t ldv, int passes, double *work, int nblk,
+                                cudaStream_t st) {
+    const int rows_max = ((k + 7) & ~7) + GS_B;
+    double *part = work;
+    double *Cm = part + (size_t)nblk * rows_max * GS_B;
+    double *rinv = Cm + (size_t)rows_max * GS_B;
+    const size_t smem = sizeof(double) * (size_t)2 * (GS_WIN + GS_B) * GS_LDR;
+    cudaError_t e = cudaFuncSetAttribute(gs_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int64_t n_chunks = (N + 31) / 32;
+    const int64_t per = (n_chunks + nblk - 1) / nblk;
+    const int ugrid = (int)((N + 127) / 128);  // 128 rows per 256-thread CTA
+    passes = std::max(passes, 1);
+    for (int j0 = 0; j0 < k; j0 += GS_B) {
+        const int b = std::min(GS_B, k - j0);
+        const int rows_c = j0 + ((b + 7) & ~7);  // rows of C: Q's j0 columns, then P's (padded)
+        for (int pass = 0; pass < passes; ++pass) {
+            for (int x0 = 0; x0 < j0 + b; x0 += GS_WIN) {
+                const int w = std::min(GS_WIN, j0 + b - x0);
+                gs_gram_kernel<<<nblk, GS_THREADS, smem, st>>>(V, N, ldv, x0, w, j0, b, rows_c, per, part);
+            }
+            const int64_t tot = (int64_t)rows_c * GS_B;
+            gs_reduce_kernel<<<(int)std::min<int64_t>((tot + 255) / 256, 1024), 256, 0, st>>>(part, nblk, rows_c, Cm);
+            gs_chol_kernel<<<1, 256, 0, st>>>(Cm, j0, b, rinv);
+            gs_update_kernel<<<ugrid, 256, 0, st>>>(V, N, ldv, j0, b, Cm, rinv);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
-        gs_dots_kernel<<<nblk, threads, sizeof(double) * (threads / 32), st>>>(V, N, ldv, j, part);
-        gs_reduce_kernel<<<1, 256, 0, st>>>(part, nblk, j, h);
-        gs_scale_kernel<<<ugrid, threads, 0, st>>>(V, N, ldv, j, h);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
 }

@@ -21,7 +21,8 @@ cudaError_t launch_spmm(int64_t N, const int64_t *rowptr, const int *colind, int
 size_t vty_smem_bytes(int k, int n_mats);
 cudaError_t launch_vty(int64_t N, int k, const double *Vt, const double *Y, int64_t y_stride, int n_mats, int nblk,
                        double *partial, ProjOut out, cudaStream_t st);
-cudaError_t launch_gram_schmidt(double *V, int64_t N, int k, int64_t ldv, int passes, double *part, double *h,
-                                int nblk, cudaStream_t st);
+size_t gs_workspace_doubles(int k, int nblk);
+cudaError_t launch_gram_schmidt(double *V, int64_t N, int k, int64_t ldv, int passes, double *work, int nblk,
+                                cudaStream_t st);
 
 }  // namespace srom

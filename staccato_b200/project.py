@@ -56,7 +56,7 @@ def project(handle: _capi.Handle, csr: DeviceCsr, values: Sequence, V) -> List:
 
 
 def orthonormalize(handle: _capi.Handle, V, passes: int = 2) -> None:
-    """In-place Gram-Schmidt (two projection passes) of an n x k column-major basis given as a
-    contiguous (k, n) float64 tensor."""
+    """In-place block Gram-Schmidt (``passes`` projection passes per 32-column panel) of an
+    n x k column-major basis given as a contiguous (k, n) float64 tensor."""
     k, n = int(V.shape[0]), int(V.shape[1])
     check(handle.ptr, _capi.lib().srom_orthonormalize(handle.ptr, C.c_void_p(V.data_ptr()), n, k, n, passes))

@@ -140,3 +140,46 @@ def test_gram_schmidt_full_basis(handle, block_model):
     assert np.abs(Vg.T @ Vg - np.eye(96)).max() <= 1e-13
     Vo = O.mgs(V0, passes=2)
     assert np.abs(Vg - Vo).max() <= 1e-12
+
+
+def _gs_device(handle, V0, passes=2, pad=0):
+    """Run srom_orthonormalize on a column-major copy of V0 with leading dimension n + pad."""
+    import ctypes as C
+
+    import torch
+
+    n, k = V0.shape
+    buf = np.zeros((k, n + pad))
+    buf[:, :n] = V0.T
+    d = _dev(buf)
+    check = _capi.check
+    check(handle.ptr, _capi.lib().srom_orthonormalize(handle.ptr, C.c_void_p(d.data_ptr()), n, k, n + pad, passes))
+    torch.cuda.synchronize()
+    out = d.cpu().numpy()
+    assert np.array_equal(out[:, n:], buf[:, n:])  # the padding rows are not touched
+    return out[:, :n].T
+
+
+@pytest.mark.parametrize("n,k,pad", [(5000, 200, 0), (3001, 40, 7)])
+def test_gram_schmidt_wide_and_padded(handle, n, k, pad):
+    """k > 128 takes several reduction windows per panel; ldv > n leaves the padding alone."""
+    V0 = np.random.default_rng(n).standard_normal((n, k))
+    Q = _gs_device(handle, V0, pad=pad)
+    assert np.abs(Q.T @ Q - np.eye(k)).max() <= 1e-13
+    assert np.abs(Q - O.mgs(V0, passes=2)).max() <= 1e-12
+
+
+def test_gram_schmidt_ill_conditioned(handle):
+    """Singular values from 1 down to 1e-6: two passes still give an orthonormal basis of the
+    same nested spans (the unique Q with a positive diagonal R, like the oracle's MGS)."""
+    n, k = 4000, 48
+    rng = np.random.default_rng(3)
+    U, _ = np.linalg.qr(rng.standard_normal((n, k)))
+    W, _ = np.linalg.qr(rng.standard_normal((k, k)))
+    V0 = (U * np.logspace(0, -6, k)) @ W.T
+    Q = _gs_device(handle, V0)
+    assert np.abs(Q.T @ Q - np.eye(k)).max() <= 1e-13
+    Qo = O.mgs(V0, passes=2)
+    assert np.abs(Q - Qo).max() <= 1e-8
+    # V0 lies in span(Q): the projection residual is at rounding level
+    assert np.linalg.norm(V0 - Q @ (Q.T @ V0)) <= 1e-12 * np.linalg.norm(V0)
