@@ -54,7 +54,8 @@ typedef struct {
 /* ---- precision of the factorisation ---------------------------------------------- */
 #define SROM_FP64 0        /* all-FP64 complex LU, bit-identical to the restated zgetrf */
 #define SROM_MIXED_FP32 1  /* complex FP32 LU + FP64 residual refinement               */
-#define SROM_MIXED_TF32 2  /* complex LU with 3xTF32 tensor-core trailing updates + FP64 refinement */
+#define SROM_MIXED_TF32 2  /* reserved: 3xTF32 tensor-core LU + FP64 refinement; this build returns
+                              SROM_ERR_UNSUPPORTED for it                                       */
 
 /* ---- sweep flags ---------------------------------------------------------------------- */
 #define SROM_FLAG_FALLBACK_FP64 1 /* re-solve non-converged frequencies with the FP64 kernel */
@@ -86,6 +87,13 @@ typedef struct {
     double *berr;           /* F doubles or NULL: estimated relative error left (mixed) */
     srom_complex *LU;       /* F blocks of n x n or NULL (SROM_FLAG_KEEP_FACTORS)    */
     int *ipiv;              /* F blocks of n ints (1-based) or NULL                  */
+    /* Back-projection (optional): y(w_f) = C x(w_f), the output of backTransformKMOR
+     * (z_freq = C_R * z_krylov_freq, KrylovROMSubstructure.cpp:1446-1449).  With rhs = B_R
+     * the same call yields the transfer functions H_R(w) = C_R A(w)^-1 B_R (:1433-1441). */
+    int n_out;              /* rows of C (output DOFs); 0 = no back-projection       */
+    int ldc;                /* leading dimension of C (>= n_out)                     */
+    const srom_complex *C;  /* n_out x n or NULL                                     */
+    srom_complex *Y;        /* F blocks of n_out x r (ld n_out) or NULL              */
 } srom_rom_desc;
 
 typedef struct {
@@ -217,7 +225,7 @@ SROM_API int srom_orthonormalize(srom_handle *h, double *V, int64_t n_rows, int 
  * The first call on each device looks up the array's device address; make that first call
  * before any stream capture.  Every call reuses the array (the work counter is cleared on
  * each call): calls whose work overlaps on the GPU race and must be serialised by the caller.
- * Results are bit-identical to srom_sweep with SROM_FP64.
+ * Results (x and, when n_out > 0, y = C x) are bit-identical to srom_sweep with SROM_FP64.
  */
 SROM_API int srom_sweep_fp64_noalloc(const srom_rom_desc *rom, void *cuda_stream, char *err, int err_len);
 

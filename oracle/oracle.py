@@ -58,6 +58,7 @@ def lib() -> C.CDLL:
         L.oracle_csr_spmm.argtypes = [_I, _P, _P, _P, _I, _I, _P, _I, _I64, _P]
         L.oracle_gemm_tn.argtypes = [_I, _I, _P, _I64, _P, _P]
         L.oracle_mgs.argtypes = [_I, _I, _P, _I64, _I]
+        L.oracle_backproject.argtypes = [_I, _I, _I, _I, _I, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -132,6 +133,19 @@ def x_ref(K, M, D, eta: float, rhs, omega, iters: int = 3):
         lib().oracle_refine_ld(n, r, _ptr(A), _ptr(rhs), n, iters, _ptr(X))
         out[f] = X
     return out
+
+
+def backproject(C, X) -> np.ndarray:
+    """Y[f] = C X[f] for X of shape (F, n, r): returns (F, n_out, r), summed over j in
+    increasing order with the GPU kernel's FMA pattern."""
+    C = _cf(C)
+    X = np.asarray(X, dtype=np.complex128)
+    F, n, r = X.shape
+    n_out = C.shape[0]
+    Xc = np.ascontiguousarray(X.transpose(0, 2, 1))  # (F, r, n): blocks of n x r, ld n
+    Y = np.empty((F, r, n_out), dtype=np.complex128)
+    lib().oracle_backproject(n, r, F, n_out, n_out, _ptr(C), _ptr(Xc), _ptr(Y))
+    return np.ascontiguousarray(Y.transpose(0, 2, 1))
 
 
 def rel_err(X, Xref) -> np.ndarray:

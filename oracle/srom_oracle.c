@@ -244,6 +244,35 @@ void oracle_sweep(int n, int nrhs, const double *K, const double *M, const doubl
     free(ipiv);
 }
 
+/* ---------------------------------------------------------------------------------------
+ * Back-projection y = C_R x per frequency: z_freq = C_R * z_krylov_freq, cblas_zgemm in
+ * backTransformKMOR (src/analysis/KrylovROMSubstructure.cpp:1446-1449); with B_R as the
+ * right-hand sides the same product gives H_R = C_R A^-1 B_R (:1433-1441).  MKL does not
+ * specify zgemm's summation order; the restatement fixes it: y_ic is the sum over
+ * j = 0 .. n-1 in increasing order of C_ij x_jc, each term added with two FMAs per component
+ * (the order the GPU kernel uses).  C: n_out x n (ld ldc); X: F blocks of n x r (ld n);
+ * Y: F blocks of n_out x r (ld n_out).
+ * --------------------------------------------------------------------------------------- */
+void oracle_backproject(int n, int r, int F, int n_out, int ldc, const double *Cd, const double *Xd,
+                        double *Yd) {
+    const cplx *C = (const cplx *)Cd, *X = (const cplx *)Xd;
+    cplx *Y = (cplx *)Yd;
+    for (int f = 0; f < F; ++f)
+        for (int c = 0; c < r; ++c)
+            for (int i = 0; i < n_out; ++i) {
+                cplx acc = {0.0, 0.0};
+                const cplx *x = X + ((int64_t)f * r + c) * n;
+                for (int j = 0; j < n; ++j) {
+                    const cplx a = C[i + (int64_t)j * ldc], b = x[j];
+                    cplx o;
+                    o.re = fma(a.re, b.re, fma(-a.im, b.im, acc.re));
+                    o.im = fma(a.re, b.im, fma(a.im, b.re, acc.im));
+                    acc = o;
+                }
+                Y[((int64_t)f * r + c) * n_out + i] = acc;
+            }
+}
+
 /* x_ref for one frequency: FP64 LU solution refined with long-double residuals.
  * A: assembled n x n (ld n), B: n x nrhs (ld ldb), X out n x nrhs (ld n).
  * Returns the LAPACK info of the factorisation. */

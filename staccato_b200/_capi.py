@@ -63,6 +63,7 @@ class RomDesc(C.Structure):
         ("omega", C.c_void_p),
         ("X", C.c_void_p), ("info", C.c_void_p), ("steps", C.c_void_p), ("berr", C.c_void_p),
         ("LU", C.c_void_p), ("ipiv", C.c_void_p),
+        ("n_out", C.c_int), ("ldc", C.c_int), ("C", C.c_void_p), ("Y", C.c_void_p),
     ]
 
 

@@ -166,7 +166,27 @@ int validate_desc(srom_handle *h, const srom_rom_desc &d, int idx) {
     if (d.ldb < d.n) return set_err(h, SROM_ERR_INVALID, "rom %d: ldb (%d) < n (%d)", idx, d.ldb, d.n);
     if ((d.LU == nullptr) != (d.ipiv == nullptr))
         return set_err(h, SROM_ERR_INVALID, "rom %d: LU and ipiv must be given together", idx);
+    if (d.n_out < 0) return set_err(h, SROM_ERR_INVALID, "rom %d: negative n_out", idx);
+    if (d.n_out > 0) {
+        if (!d.C || !d.Y) return set_err(h, SROM_ERR_INVALID, "rom %d: n_out > 0 needs C and Y", idx);
+        if (d.ldc < d.n_out) return set_err(h, SROM_ERR_INVALID, "rom %d: ldc (%d) < n_out (%d)", idx, d.ldc, d.n_out);
+    }
     return SROM_OK;
+}
+
+// Back-projection launch parameters of a descriptor (n_out = 0: none).
+srom::BackProj backproj_of(const srom_rom_desc &d) {
+    srom::BackProj b{};
+    if (d.n_out <= 0 || d.n == 0 || d.F == 0 || d.r == 0) return b;
+    b.n = d.n;
+    b.r = d.r;
+    b.F = d.F;
+    b.n_out = d.n_out;
+    b.ldc = d.ldc;
+    b.C = reinterpret_cast<const double2 *>(d.C);
+    b.X = reinterpret_cast<const double2 *>(d.X);
+    b.Y = reinterpret_cast<double2 *>(d.Y);
+    return b;
 }
 
 RomDev to_dev(const srom_rom_desc &d) {
@@ -313,6 +333,7 @@ struct SweepPlan {
     long long grid0 = 0, grid1 = 0;
     int64_t slot_bytes = 0;
     bool need_scratch = false;
+    std::vector<srom::BackProj> backproj;  // ROMs whose solutions are projected onto outputs
 };
 
 // FP64 storage class of an n x n system with r right-hand sides: 0 smem kernel, 1 global
@@ -350,6 +371,8 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
     std::vector<int> cls(n_roms, -1);
     for (int i = 0; i < n_roms; ++i) {
         dev[i] = to_dev(roms[i]);
+        if (roms[i].n_out > 0 && roms[i].n > 0 && roms[i].F > 0 && roms[i].r > 0)
+            P.backproj.push_back(backproj_of(roms[i]));
         const srom_rom_desc &d = roms[i];
         if (d.n == 0 || d.F == 0 || d.r == 0) continue;
         cls[i] = mixed ? 1 : fp64_class(h, d.n, d.r);
@@ -455,6 +478,12 @@ int enqueue_plan(srom_handle *h, const SweepPlan &P, char *dm, void *scratch, cu
             cudaError_t e = srom::launch_global(false, b, (int)P.grid1, st);
             if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "fallback launch: %s", cudaGetErrorString(e));
         }
+    }
+    for (size_t i = 0; rc == SROM_OK && i < P.backproj.size(); ++i) {
+        const srom::BackProj &b = P.backproj[i];
+        ProfScope ps(h, "backproject", b.F, 8.0 * (double)b.n_out * b.n * b.r * b.F, 0.0);
+        cudaError_t e = srom::launch_backproject(b, h->sm_count, st);
+        if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "back-projection launch: %s", cudaGetErrorString(e));
     }
     h->prof = prof_prev;
     return rc;
@@ -729,7 +758,7 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
     }
     DeviceGuard g(h->device);
     // Lay out every input and output of every ROM in one device arena.
-    std::vector<size_t> offs(n_roms * 10, 0);
+    std::vector<size_t> offs(n_roms * 11, 0);
     size_t total = 0;
     auto take = [&](size_t bytes) {
         size_t o = total;
@@ -740,7 +769,7 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
         const srom_rom_desc &d = roms[i];
         if (d.n == 0 || d.F == 0 || d.r == 0) continue;
         const size_t nn = (size_t)d.ldk * d.n, cz = sizeof(srom_complex);
-        size_t *o = &offs[i * 10];
+        size_t *o = &offs[i * 11];
         o[0] = take(cz * nn);
         o[1] = take(cz * nn);
         o[2] = d.D ? take(cz * nn) : 0;
@@ -750,6 +779,10 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
         o[6] = d.info ? take(sizeof(int) * d.F) : 0;
         o[7] = d.steps ? take(sizeof(int) * d.F) : 0;
         o[8] = d.berr ? take(sizeof(double) * d.F) : 0;
+        if (d.n_out > 0) {
+            o[9] = take(cz * (size_t)d.ldc * d.n);
+            o[10] = take(cz * (size_t)d.F * d.n_out * d.r);
+        }
     }
     int s = ensure_device_buffer(h, &h->d_host_arena, &h->d_host_arena_bytes, std::max<size_t>(total, 256));
     if (s) return s;
@@ -760,7 +793,7 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
         const srom_rom_desc &d = roms[i];
         if (d.n == 0 || d.F == 0 || d.r == 0) continue;
         const size_t nn = (size_t)d.ldk * d.n, cz = sizeof(srom_complex);
-        size_t *o = &offs[i * 10];
+        size_t *o = &offs[i * 11];
         srom_rom_desc &e = dd[i];
         e.K = reinterpret_cast<const srom_complex *>(base + o[0]);
         e.M = reinterpret_cast<const srom_complex *>(base + o[1]);
@@ -773,6 +806,11 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
         e.berr = d.berr ? reinterpret_cast<double *>(base + o[8]) : nullptr;
         e.LU = nullptr;
         e.ipiv = nullptr;
+        if (d.n_out > 0) {
+            e.C = reinterpret_cast<const srom_complex *>(base + o[9]);
+            e.Y = reinterpret_cast<srom_complex *>(base + o[10]);
+            SROM_CUDA(h, cudaMemcpyAsync((void *)e.C, d.C, cz * (size_t)d.ldc * d.n, H2D, h->stream));
+        }
         SROM_CUDA(h, cudaMemcpyAsync((void *)e.K, d.K, cz * nn, H2D, h->stream));
         SROM_CUDA(h, cudaMemcpyAsync((void *)e.M, d.M, cz * nn, H2D, h->stream));
         if (d.D) SROM_CUDA(h, cudaMemcpyAsync((void *)e.D, d.D, cz * nn, H2D, h->stream));
@@ -789,6 +827,9 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
         if (d.info) SROM_CUDA(h, cudaMemcpyAsync(d.info, e.info, sizeof(int) * d.F, D2H, h->stream));
         if (d.steps) SROM_CUDA(h, cudaMemcpyAsync(d.steps, e.steps, sizeof(int) * d.F, D2H, h->stream));
         if (d.berr) SROM_CUDA(h, cudaMemcpyAsync(d.berr, e.berr, sizeof(double) * d.F, D2H, h->stream));
+        if (d.n_out > 0)
+            SROM_CUDA(h, cudaMemcpyAsync(d.Y, e.Y, sizeof(srom_complex) * (size_t)d.F * d.n_out * d.r, D2H,
+                                         h->stream));
     }
     SROM_CUDA(h, cudaStreamSynchronize(h->stream));
     return SROM_OK;

@@ -85,6 +85,8 @@ extern "C" int srom_sweep_fp64_noalloc(const srom_rom_desc *d, void *cuda_stream
     if (d->ldk < d->n || d->ldb < d->n) return fail(err, err_len, SROM_ERR_INVALID, "ldk and ldb must be >= n");
     if ((d->LU == nullptr) != (d->ipiv == nullptr))
         return fail(err, err_len, SROM_ERR_INVALID, "LU and ipiv must be given together");
+    if (d->n_out < 0 || (d->n_out > 0 && (!d->C || !d->Y || d->ldc < d->n_out)))
+        return fail(err, err_len, SROM_ERR_INVALID, "n_out > 0 needs C, Y and ldc >= n_out");
     if (d->n > NOALLOC_MAX_N) {
         char b[96];
         snprintf(b, sizeof b, "n = %d exceeds the limit of %d", d->n, NOALLOC_MAX_N);
@@ -143,5 +145,11 @@ extern "C" int srom_sweep_fp64_noalloc(const srom_rom_desc *d, void *cuda_stream
     auto *slot_base = reinterpret_cast<double2 *>(base + NOALLOC_HDR_BYTES + NOALLOC_ITEM_BYTES);
     e = srom::launch_fp64_global(roms, items, d->F, ctr, slot_base, slot, d->n, d->r, (int)grid, st);
     if (e != cudaSuccess) return fail(err, err_len, SROM_ERR_CUDA, "sweep launch", cudaGetErrorString(e));
+    if (d->n_out > 0) {
+        srom::BackProj b{d->n, d->r, d->F, d->n_out, d->ldc, reinterpret_cast<const double2 *>(d->C),
+                         reinterpret_cast<const double2 *>(d->X), reinterpret_cast<double2 *>(d->Y)};
+        e = srom::launch_backproject(b, sms, st);
+        if (e != cudaSuccess) return fail(err, err_len, SROM_ERR_CUDA, "back-projection launch", cudaGetErrorString(e));
+    }
     return SROM_OK;
 }

@@ -43,4 +43,13 @@ cudaError_t launch_fp64_global(const RomDev *roms, const Item *items, int n_item
                                double2 *scratch, int64_t slot_elems, int n_max, int r_max,
                                int grid, cudaStream_t st);
 
+// Back-projection Y_f = C X_f of one ROM's solutions (F blocks of n x r -> n_out x r).
+struct BackProj {
+    int n, r, F, n_out, ldc;
+    const double2 *C;
+    const double2 *X;
+    double2 *Y;
+};
+cudaError_t launch_backproject(const BackProj &p, int sms, cudaStream_t st);
+
 }  // namespace srom

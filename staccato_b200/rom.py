@@ -59,10 +59,24 @@ class KrylovROMSubstructure:
         return R
 
     # --------------------------------------------------------------- frequency sweep
+    def _device_rom(self, rhs, omega, with_c: bool) -> DeviceRom:
+        import torch
+
+        n, r = int(rhs.shape[0]), int(rhs.shape[1])
+        cm = lambda a: a.t().contiguous().reshape(-1)  # column-major flat copy
+        rom = DeviceRom(n=n, r=r, F=len(omega), K=cm(self.K_r), M=cm(self.M_r),
+                        D=None if self.D_r is None else cm(self.D_r), rhs=cm(rhs),
+                        omega=torch.as_tensor(omega, device=self.K_r.device), eta=self.eta)
+        if with_c and self.C_r is not None:
+            rom.C, rom.n_out = cm(self.C_r), int(self.C_r.shape[0])
+        rom.allocate_outputs(self.K_r.device)
+        return rom
+
     def back_transform_kmor(self, freq_hz, input_load, precision: int = _capi.SROM_FP64,
                             flags: int = _capi.SROM_FLAG_FALLBACK_FP64, max_refine: int = 5):
         """y(w) = C_r A(w)^-1 B_r F per frequency; returns (Y, info) with Y of shape
-        (F, n_out, r) (x itself when C_r is None)."""
+        (F, n_out, r) (x itself when C_r is None).  The back-projection y = C_r x runs on the
+        device right after the sweep (srom_rom_desc.C / .Y)."""
         import torch
 
         freq = np.asarray(freq_hz, dtype=np.float64)
@@ -71,14 +85,26 @@ class KrylovROMSubstructure:
         if F_load.ndim == 1:
             F_load = F_load[:, None]
         rhs = F_load if self.B_r is None else self.B_r @ F_load
-        n, r = int(rhs.shape[0]), int(rhs.shape[1])
-        rom = DeviceRom(n=n, r=r, F=len(omega),
-                        K=self.K_r.t().contiguous().reshape(-1), M=self.M_r.t().contiguous().reshape(-1),
-                        D=None if self.D_r is None else self.D_r.t().contiguous().reshape(-1),
-                        rhs=rhs.t().contiguous().reshape(-1),
-                        omega=torch.as_tensor(omega, device=self.K_r.device), eta=self.eta)
-        rom.allocate_outputs(self.K_r.device)
+        rom = self._device_rom(rhs, omega, with_c=True)
         sweep(self.handle, [rom], precision=precision, flags=flags, max_refine=max_refine)
-        X = rom.X.reshape(rom.F, r, n).transpose(1, 2)  # (F, n, r)
-        Y = X if self.C_r is None else torch.matmul(self.C_r, X)
+        if rom.n_out > 0:
+            Y = rom.Y.reshape(rom.F, rom.r, rom.n_out).transpose(1, 2)  # (F, n_out, r)
+        else:
+            Y = rom.X.reshape(rom.F, rom.r, rom.n).transpose(1, 2)  # (F, n, r)
         return Y, rom.info
+
+    def transfer_functions(self, freq_hz, precision: int = _capi.SROM_FP64,
+                           flags: int = _capi.SROM_FLAG_FALLBACK_FP64, max_refine: int = 5):
+        """H_R(w) = C_r A(w)^-1 B_r per frequency (KrylovROMSubstructure.cpp:1433-1441): the
+        sweep with B_r as right-hand sides and C_r as output matrix.  Returns (H, info) with H
+        of shape (F, n_out, n_in) (A^-1 B_r when C_r is None)."""
+        if self.B_r is None:
+            raise ValueError("transfer functions need B_r")
+        omega = 2.0 * math.pi * np.asarray(freq_hz, dtype=np.float64)
+        rom = self._device_rom(self.B_r, omega, with_c=True)
+        sweep(self.handle, [rom], precision=precision, flags=flags, max_refine=max_refine)
+        if rom.n_out > 0:
+            H = rom.Y.reshape(rom.F, rom.r, rom.n_out).transpose(1, 2)
+        else:
+            H = rom.X.reshape(rom.F, rom.r, rom.n).transpose(1, 2)
+        return H, rom.info

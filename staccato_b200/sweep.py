@@ -46,10 +46,13 @@ class DeviceRom:
     berr: Optional["object"] = None
     LU: Optional["object"] = None
     ipiv: Optional["object"] = None
+    C: Optional["object"] = None      # n_out x n output matrix (flat column-major) or None
+    Y: Optional["object"] = None      # F blocks of n_out x r: y(w) = C x(w)
+    n_out: int = 0
 
     @classmethod
     def from_host(cls, K, M, D, rhs, omega, eta: float = 0.0, device="cuda",
-                  keep_factors: bool = False) -> "DeviceRom":
+                  keep_factors: bool = False, C=None) -> "DeviceRom":
         torch = _torch()
         K = np.asarray(K)
         n = int(K.shape[0])
@@ -62,6 +65,9 @@ class DeviceRom:
         t = lambda a: torch.from_numpy(colmajor(a)).to(device)
         rom = cls(n=n, r=r, F=F, K=t(K), M=t(M), D=None if D is None else t(D), rhs=t(rhs),
                   omega=torch.from_numpy(omega).to(device), eta=float(eta))
+        if C is not None:
+            C = np.asarray(C)
+            rom.C, rom.n_out = t(C), int(C.shape[0])
         rom.allocate_outputs(device, keep_factors)
         return rom
 
@@ -74,18 +80,26 @@ class DeviceRom:
         if keep_factors:
             self.LU = torch.empty(self.F * self.n * self.n, dtype=torch.complex128, device=device)
             self.ipiv = torch.empty(self.F * self.n, dtype=torch.int32, device=device)
+        if self.n_out > 0:
+            self.Y = torch.empty(self.F * self.n_out * self.r, dtype=torch.complex128, device=device)
 
     def desc(self) -> RomDesc:
         p = lambda t: None if t is None else C.c_void_p(t.data_ptr())
         return RomDesc(n=self.n, r=self.r, F=self.F, ldk=self.n, K=p(self.K), M=p(self.M),
                        D=p(self.D), eta=self.eta, rhs=p(self.rhs), ldb=self.n,
                        omega=p(self.omega), X=p(self.X), info=p(self.info), steps=p(self.steps),
-                       berr=p(self.berr), LU=p(self.LU), ipiv=p(self.ipiv))
+                       berr=p(self.berr), LU=p(self.LU), ipiv=p(self.ipiv),
+                       n_out=self.n_out, ldc=max(self.n_out, 1), C=p(self.C), Y=p(self.Y))
 
     def solutions(self) -> np.ndarray:
         """X as a numpy array of shape (F, n, r)."""
         x = self.X.cpu().numpy().reshape(self.F, self.r, self.n)
         return np.ascontiguousarray(x.transpose(0, 2, 1))
+
+    def outputs(self) -> np.ndarray:
+        """Y = C X as a numpy array of shape (F, n_out, r)."""
+        y = self.Y.cpu().numpy().reshape(self.F, self.r, self.n_out)
+        return np.ascontiguousarray(y.transpose(0, 2, 1))
 
 
 def opts(precision: int = _capi.SROM_FP64, max_refine: int = 5, tol: float = 0.0,
@@ -115,6 +129,8 @@ class HostRom:
     info: Optional[np.ndarray] = None
     steps: Optional[np.ndarray] = None
     berr: Optional[np.ndarray] = None
+    C: Optional[np.ndarray] = None
+    Y: Optional[np.ndarray] = None
 
     def __post_init__(self):
         self.K = colmajor(self.K)
@@ -136,16 +152,26 @@ class HostRom:
             self.steps = np.empty(self.F, dtype=np.int32)
         if self.berr is None:
             self.berr = np.empty(self.F, dtype=np.float64)
+        self.n_out = 0
+        if self.C is not None:
+            self.n_out = int(np.asarray(self.C).shape[0])
+            self.C = colmajor(self.C)
+            if self.Y is None:
+                self.Y = np.empty(self.F * self.n_out * self.r, dtype=np.complex128)
 
     def desc(self) -> RomDesc:
         p = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
         return RomDesc(n=self.n, r=self.r, F=self.F, ldk=self.n, K=p(self.K), M=p(self.M),
                        D=p(self.D), eta=self.eta, rhs=p(self.rhs), ldb=self.n,
                        omega=p(self.omega), X=p(self.X), info=p(self.info), steps=p(self.steps),
-                       berr=p(self.berr), LU=None, ipiv=None)
+                       berr=p(self.berr), LU=None, ipiv=None,
+                       n_out=self.n_out, ldc=max(self.n_out, 1), C=p(self.C), Y=p(self.Y))
 
     def solutions(self) -> np.ndarray:
         return np.ascontiguousarray(self.X.reshape(self.F, self.r, self.n).transpose(0, 2, 1))
+
+    def outputs(self) -> np.ndarray:
+        return np.ascontiguousarray(self.Y.reshape(self.F, self.r, self.n_out).transpose(0, 2, 1))
 
 
 def sweep_host(handle: _capi.Handle, roms: Sequence[HostRom], precision: int = _capi.SROM_FP64,

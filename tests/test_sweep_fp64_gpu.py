@@ -40,7 +40,7 @@ def _assert_bitexact(a, b, what):
         pytest.fail(f"{what}: {int((~same).sum())} of {len(same)} systems differ; first #{bad} rel {err:.3e}")
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 5, 31, 32, 33, 64, 65, 100, 112, 113, 128, 200, 257, 512])
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 31, 32, 33, 64, 65, 100, 112, 113, 128, 200, 257, 449, 480, 512])
 def test_fp64_matches_oracle_bitwise(handle, n):
     rng = np.random.default_rng(1000 + n)
     r = 1 if n > 300 else (3 if n % 2 else 8)

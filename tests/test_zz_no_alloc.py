@@ -75,3 +75,25 @@ def test_noalloc_rejects_sizes_beyond_its_limit(handle):
     st = _capi.lib().srom_sweep_fp64_noalloc(C.byref(d), None, err, 256)
     assert st == _capi.SROM_ERR_UNSUPPORTED and b"65536" in err.value
     torch.cuda.synchronize()
+
+
+def test_noalloc_backprojection_matches_srom_sweep(handle):
+    """With n_out > 0 the entry point also writes y = C x, bit-identical to srom_sweep."""
+    import torch
+
+    stream = torch.cuda.current_stream().cuda_stream
+    handle.set_stream(stream)
+    rng = np.random.default_rng(21)
+    n, r, F, n_out = 120, 2, 13, 9
+    c = lambda s: rng.standard_normal(s) + 1j * rng.standard_normal(s)
+    rom = DeviceRom.from_host(c((n, n)) * 10.0 + 3.0 * np.eye(n), c((n, n)), None, c((n, r)),
+                              rng.uniform(0.1, 3.0, size=F), C=c((n_out, n)))
+    sweep(handle, [rom])
+    torch.cuda.synchronize()
+    Y = rom.outputs().copy()
+    rom.Y.fill_(float("nan"))
+    st, msg = _noalloc(rom, stream)
+    assert st == _capi.SROM_OK, msg
+    torch.cuda.synchronize()
+    assert _same(rom.outputs(), Y)
+
