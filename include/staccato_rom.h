@@ -229,6 +229,27 @@ SROM_API int srom_orthonormalize(srom_handle *h, double *V, int64_t n_rows, int 
  */
 SROM_API int srom_sweep_fp64_noalloc(const srom_rom_desc *rom, void *cuda_stream, char *err, int err_len);
 
+/* ---- dense ROM files (host only; no handle, no GPU work) ------------------------------- */
+/*
+ * Read a dense Matrix Market file, the format of the reference's ROM test inputs
+ * (io::readMtxDense, test/krylovTestGPU/matrixInSingleLoop/gpu/src/io/io.cu:20-80): '%' lines,
+ * "rows cols", then rows*cols entries column after column, each "re im" (complex, the default
+ * and the reference's files) or one value ("%%MatrixMarket ... real" banner).  A banner with
+ * "row major" (AuxiliaryFunctions.cpp:91) means entries row after row.  A is filled column-major
+ * (ld rows); with A == NULL only *rows and *cols are set.  Short or over-long files and a
+ * capacity below rows*cols return SROM_ERR_INVALID with the reason in err.
+ */
+SROM_API int srom_mtx_read_dense(const char *path, int64_t *rows, int64_t *cols, srom_complex *A, int64_t capacity,
+                                 char *err, int err_len);
+/* Write A (rows x cols, column-major, lda) in the reference's dense complex format
+ * (AuxiliaryFunctions::writeMKLComplexDenseMatrixMtxFormat, src/tools/AuxiliaryFunctions.cpp:80-110),
+ * 17 significant digits so that srom_mtx_read_dense returns the same bits. */
+SROM_API int srom_mtx_write_dense(const char *path, int64_t rows, int64_t cols, const srom_complex *A, int64_t lda,
+                                  char *err, int err_len);
+/* Write a solution vector as the reference's "Real Imag" table (io::writeSolVecComplex,
+ * io.cu:83-106: width-25 columns, CRLF lines), with 17 significant digits instead of 16. */
+SROM_API int srom_write_solution(const char *path, const srom_complex *x, int64_t count, char *err, int err_len);
+
 /* ---- per-launch timing -------------------------------------------------------------- */
 /* One record per kernel launch issued while profiling is enabled: CUDA events recorded on
  * the handle's stream around the launch, plus the algorithmic work the launch performs

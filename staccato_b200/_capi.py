@@ -34,6 +34,7 @@ EXPORTS = [
     "srom_version", "srom_sweep", "srom_sweep_host", "srom_profile_enable", "srom_profile_read",
     "srom_sweep_fp64_noalloc", "srom_project_real", "srom_orthonormalize", "srom_sweep_backward",
     "srom_graph_create", "srom_graph_launch", "srom_graph_destroy", "srom_tune",
+    "srom_mtx_read_dense", "srom_mtx_write_dense", "srom_write_solution",
 ]
 
 SROM_DPARAM_LOWRANK = 0
@@ -121,6 +122,13 @@ def lib() -> C.CDLL:
         L.srom_sweep_backward.restype = i
         L.srom_sweep_fp64_noalloc.argtypes = [C.POINTER(RomDesc), vp, C.c_char_p, i]
         L.srom_sweep_fp64_noalloc.restype = i
+        i64, cp = C.c_int64, C.c_char_p
+        L.srom_mtx_read_dense.argtypes = [cp, C.POINTER(i64), C.POINTER(i64), vp, i64, cp, i]
+        L.srom_mtx_read_dense.restype = i
+        L.srom_mtx_write_dense.argtypes = [cp, i64, i64, vp, i64, cp, i]
+        L.srom_mtx_write_dense.restype = i
+        L.srom_write_solution.argtypes = [cp, vp, i64, cp, i]
+        L.srom_write_solution.restype = i
         for name in ("srom_sweep", "srom_sweep_host"):
             fn = getattr(L, name)
             fn.argtypes = [vp, C.POINTER(RomDesc), i, C.POINTER(SweepOpts)]
