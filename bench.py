@@ -116,6 +116,16 @@ class ClockSampler:
 
 # ----------------------------------------------------------------------------- peaks
 
+# DRAM bytes (read + write) per launch of the dominant kernels on this bench's default
+# workload (the 64-ROM batching draw of rank 0), from a one-pass ncu capture of
+# dram__bytes_read.sum + dram__bytes_write.sum over
+# `bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-e2e --no-extras` (mean of 4 launches).
+MEASURED_TRAFFIC = {"mixed_global": 544.3e9 + 443.4e9, "fp64_global": 1753.3e9 + 1807.7e9}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, one-pass capture of this "
+                  "workload with the current kernels; compare with the bytes the matrices alone need "
+                  "(8 n^2 B per FP32 system, 16 n^2 B per FP64 system)")
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -416,7 +426,8 @@ def run_ours(args):
         achieved = kfl / (kms * 1e-3) / 1e12
         tot = sum(x[0] for x in per.values())
         return {"bound": "tensor" if form == "fp64" else "fma", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "kernel": dom,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": MEASURED_TRAFFIC.get(dom),
+                "traffic_source": TRAFFIC_SOURCE, "kernel": dom,
                 "peak_source": peak_source,
                 "algorithmic": "8/3 n^3 + 8 n^2 r real flops per system (LU + solve, both forms)",
                 "kernels": {k: {"ms_per_launch": v[0] / v[3], "launches": v[3],
