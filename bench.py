@@ -502,7 +502,7 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "systems_per_gpu": systems,
                        "tflop_per_step_per_gpu": flops / 1e12, "precision": headline,
-                       "refine": "complex-FP32 LU, FP64 residuals, <=5 corrections, stop at ||d||<=2^-33||x||, FP64 fallback",
+                       "refine": "complex-FP32 LU, FP64 residuals, <=5 corrections, stop when the predicted error rho*||d||/||x|| <= 2^-34, back substitution by reciprocals of diag(U), FP64 fallback",
                        "l2": "inputs 167 MB + outputs 1.6 GB per step exceed L2; no flush",
                        "parallelism": f"independent batch per GPU x{world} (seed 3 + 1000003*rank)"},
             "roofline": info.get("roofline"),

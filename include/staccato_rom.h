@@ -99,7 +99,7 @@ typedef struct {
 typedef struct {
     int precision;   /* SROM_FP64 / SROM_MIXED_FP32 / SROM_MIXED_TF32                */
     int max_refine;  /* refinement steps for the mixed forms (default 5 when <= 0)   */
-    double tol;      /* stop refining when the error estimate 2 (||d_s||/||d_s-1||) ||d_s||/||x|| <= tol; 0 = 2^-33 */
+    double tol;      /* stop refining when the error estimate 2 (||d_s||/||d_s-1||) ||d_s||/||x|| <= tol; 0 = 2^-34 */
     int flags;       /* SROM_FLAG_*                                                  */
 } srom_sweep_opts;
 

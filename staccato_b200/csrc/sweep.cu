@@ -22,11 +22,13 @@
 //   MIXED (float2 factors, NB = 32): the FP64-assembled matrix is rounded to complex FP32
 //          and factored; the solution is refined with residuals r = b - A(w) x computed in
 //          FP64 from K, M, D on the fly (the same assembly arithmetic) and corrections solved
-//          with the FP32 factors, until every right-hand side's last correction satisfies
-//          ||d||_inf <= tol ||x||_inf (default tol = 2^-33; the error left is about rho*tol,
-//          rho the contraction of the iteration), at most max_refine corrections after the
-//          first solve.  Frequencies that do not converge are re-solved in FP64 by the same
-//          CTA when asked (steps = -1).
+//          with the FP32 factors (back substitution by the reciprocals of U's diagonal), until
+//          the predicted error rho * ||d_s|| / ||x||, rho = 2 ||d_s|| / ||d_s-1|| the observed
+//          contraction, is at most tol for every right-hand side (default tol = 2^-34, which
+//          keeps the true error below 1e-10 with a factor-2 margin on the test workloads), at
+//          most max_refine corrections after the first solve.  Frequencies that do not
+//          converge are listed on the device and re-solved by a second, FP64 launch when asked
+//          (steps = -1).
 //
 // Reference sequence: src/analysis/KrylovROMSubstructure.cpp:1403-1453 (host, MKL), the
 // cuBLAS batched sweep of test/krylovMidsizeTest/gpu/concurrent/batchedLU/src/main.cu:223-267
@@ -262,9 +264,12 @@ __device__ void lu_solve(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs
 // needed, are copied by cp.async into one of two strip buffers while the previous block is
 // being processed.  One warp per right-hand side solves the block's triangle from the strip,
 // then every thread updates its rows.  B (n x nrhs, ldb) is in shared memory with the
-// interchanges already applied; the per-entry update order is the oracle's.
+// interchanges already applied; the per-entry update order is the oracle's.  With dinv (the
+// mixed form's correction solves) the back substitution multiplies by the reciprocals of
+// U's diagonal instead of dividing: the divisions were the critical path of the triangle.
 template <typename T, int SW>
-__device__ void lu_solve_strips(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs, T *strips) {
+__device__ void lu_solve_strips(const T *A, int64_t lda, int n, T *B, int ldb, int nrhs, T *strips,
+                                const T *dinv = nullptr) {
     using C = CT<T>;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nblk = (n + SW - 1) / SW;
@@ -346,7 +351,7 @@ __device__ void lu_solve_strips(const T *A, int64_t lda, int n, T *B, int ldb, i
             T *b = B + (int64_t)c * ldb + jb;
             T v = lane < bs ? b[lane] : C::zero();
             for (int j = bs - 1; j >= 0; --j) {
-                if (lane == j) v = C::div(v, S[j * n + jb + j]);
+                if (lane == j) v = dinv ? C::mul(v, dinv[jb + j]) : C::div(v, S[j * n + jb + j]);
                 const T bj = C::shfl(v, j, 32);
                 if (lane < j) v = C::subm(v, S[j * n + jb + lane], bj);
             }
@@ -769,7 +774,7 @@ __device__ void trailing_update(T *A, int64_t lda, int n, int j0, int nbc, const
 
 // Shared-memory carve-up of the global-class kernels (bytes from the dynamic base).
 struct GlobalSmem {
-    size_t panel, u, work64, work32, perm, ptot, pos, ipiv, moved, tile, total;
+    size_t panel, u, work64, work32, perm, ptot, pos, ipiv, moved, dinv, total;
     static __host__ __device__ size_t up(size_t b) { return (b + 255) / 256 * 256; }
     __host__ __device__ GlobalSmem(int ldp, int n_max, int r_max) {
         panel = 0;                                         // ldp x 16 double2 == ldp x 32 float2
@@ -781,8 +786,8 @@ struct GlobalSmem {
         pos = ptot + up((size_t)ldp * 4);
         ipiv = pos + up((size_t)ldp * 4);
         moved = ipiv + up((size_t)ldp * 4);
-        tile = moved + up((size_t)2 * 2 * NB32 * 4);
-        total = tile + up((size_t)32 * 33 * 16);          // diagonal block of the solves
+        dinv = moved + up((size_t)2 * 2 * NB32 * 4);
+        total = dinv + up((size_t)ldp * 16);              // reciprocals of diag(U), mixed form
     }
 };
 
@@ -988,7 +993,11 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
             __syncthreads();
             factor_global<float2, NB32, RPT>(A32, n, n, a.ldp, sm, L, nullptr, 0, PL, Xx, s_pivlg);
             info = PL.info;
-            for (int l = tid; l < n; l += NT) s_pos[s_ptot[l]] = l;
+            float2 *s_dinv = reinterpret_cast<float2 *>(sm + L.dinv);
+            for (int l = tid; l < n; l += NT) {
+                s_pos[s_ptot[l]] = l;
+                s_dinv[l] = CT<float2>::recip(A32[l + (int64_t)l * n]);
+            }
             __syncthreads();
             for (int e = tid; e < n * R.r; e += NT) {
                 const int i = e % n, c = e / n;
@@ -997,12 +1006,12 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
                 B32[s_pos[i] + (int64_t)c * n] = make_float2(__double2float_rn(b.x), __double2float_rn(b.y));
             }
             __syncthreads();
-            const double tol_x = a.tol > 0.0 ? a.tol : 1.1641532182693481e-10;  // 2^-33
+            const double tol_x = a.tol > 0.0 ? a.tol : 5.820766091346741e-11;  // 2^-34
             bool conv = false;
             double prev = 1.0;  // relative size of the previous correction (the first is x itself)
             for (int s = 0;; ++s) {
                 if (s > 0) residual64<RPT>(R, w, X, B32, s_pos);
-                lu_solve_strips<float2, 16>(A32, n, n, B32, n, R.r, reinterpret_cast<float2 *>(sm + L.panel));
+                lu_solve_strips<float2, 16>(A32, n, n, B32, n, R.r, reinterpret_cast<float2 *>(sm + L.panel), s_dinv);
                 apply_correction(X, B32, n, R.r, s_dx);
                 if (s > 0) {
                     // error left after this correction ~ rho * ||d||, rho ~ ||d_s|| / ||d_{s-1}||

@@ -38,12 +38,12 @@ def test_mixed_random_wellconditioned(handle, n):
     steps = d.steps.cpu().numpy()
     assert (steps >= 0).all() and (steps <= 5).all()
     assert (d.info.cpu().numpy() == 0).all()
-    assert (d.berr.cpu().numpy() <= 2.0 ** -33).all()
+    assert (d.berr.cpu().numpy() <= 2.0 ** -34).all()
 
 
 def test_mixed_plain_workload(handle):
     rom = W.plain_rom()
-    sel = rom.omega[::10]
+    sel = rom.omega  # all 500 frequencies: the gate is on the maximum
     d = _run(handle, rom, sel)
     xr = O.x_ref(rom.K, rom.M, rom.D, 0.0, rom.rhs, sel)
     assert O.rel_err(d.solutions(), xr).max() <= 1e-10
