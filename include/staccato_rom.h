@@ -75,7 +75,7 @@ typedef struct {
     int F;                  /* number of frequencies                                 */
     int ldk;                /* leading dimension of K, M, D (>= n)                   */
     const srom_complex *K;  /* n x n                                                 */
-    const srom_complex *M;  /* n x n                                                 */
+    const srom_complex *M;  /* n x n or NULL (no mass term: A = (1+i eta) K + i w D)   */
     const srom_complex *D;  /* n x n or NULL                                         */
     double eta;             /* hysteretic loss factor applied to K; 0 keeps K as is  */
     const srom_complex *rhs;/* n x r, leading dimension ldb (= B_r * F)              */

@@ -73,7 +73,8 @@ def _cf(a) -> np.ndarray:
 
 def assemble(K, M, D, eta: float, omega: float) -> np.ndarray:
     """A(w) in the reference's zaxpy order, bit-identical to the GPU assembly."""
-    K, M = _cf(K), _cf(M)
+    K = _cf(K)
+    M = None if M is None else _cf(M)
     D = None if D is None else _cf(D)
     n = K.shape[0]
     A = np.empty((n, n), dtype=np.complex128, order="F")
@@ -104,7 +105,8 @@ def zgetrs(LU, ipiv, B, conj: bool = False) -> np.ndarray:
 
 def sweep(K, M, D, eta: float, rhs, omega):
     """Reference sequence for every frequency: X[f] (n x r) and info[f]."""
-    K, M = _cf(K), _cf(M)
+    K = _cf(K)
+    M = None if M is None else _cf(M)
     D = None if D is None else _cf(D)
     rhs = _cf(rhs)
     if rhs.ndim == 1:
@@ -251,7 +253,8 @@ def cpu_lib(use_openblas: bool = True) -> C.CDLL:
 
 
 def cpu_sweep(K, M, D, eta, rhs, omega, f0: int, f1: int, threads: int = 0) -> np.ndarray:
-    K, M = _cf(K), _cf(M)
+    K = _cf(K)
+    M = None if M is None else _cf(M)
     D = None if D is None else _cf(D)
     rhs = _cf(rhs)
     if rhs.ndim == 1:

@@ -111,10 +111,12 @@ void oracle_assemble(int n, const double *K, const double *M, const double *D,
             kh.im = kk.im + t2;
             kk = kh;
         }
-        double mr = s * m[e].re, mi = s * m[e].im;
-        cplx v;
-        v.re = kk.re + mr;
-        v.im = kk.im + mi;
+        cplx v = kk;  /* no mass term when M is NULL (explicit matrices, damped statics) */
+        if (m) {
+            double mr = s * m[e].re, mi = s * m[e].im;
+            v.re = kk.re + mr;
+            v.im = kk.im + mi;
+        }
         if (d) {
             double dr = omega * d[e].im, di = omega * d[e].re;
             v.re = v.re - dr;

@@ -44,6 +44,9 @@ struct srom_handle {
     // adjoint descriptors + partials
     void *d_adj = nullptr;
     size_t d_adj_bytes = 0;
+    // zeros standing in for M when a descriptor has none (see SweepPlan::null_m)
+    void *d_zero = nullptr;
+    size_t d_zero_bytes = 0;
     // per-launch profiling
     struct ProfRec {
         std::string name;
@@ -160,8 +163,8 @@ double lu_flops(int n, int r) { return 8.0 / 3.0 * (double)n * n * n + 8.0 * (do
 int validate_desc(srom_handle *h, const srom_rom_desc &d, int idx) {
     if (d.n < 0 || d.r < 0 || d.F < 0) return set_err(h, SROM_ERR_INVALID, "rom %d: negative size", idx);
     if (d.n == 0 || d.F == 0 || d.r == 0) return SROM_OK;
-    if (!d.K || !d.M || !d.rhs || !d.omega || !d.X)
-        return set_err(h, SROM_ERR_INVALID, "rom %d: K, M, rhs, omega and X must be non-null", idx);
+    if (!d.K || !d.rhs || !d.omega || !d.X)
+        return set_err(h, SROM_ERR_INVALID, "rom %d: K, rhs, omega and X must be non-null", idx);
     if (d.ldk < d.n) return set_err(h, SROM_ERR_INVALID, "rom %d: ldk (%d) < n (%d)", idx, d.ldk, d.n);
     if (d.ldb < d.n) return set_err(h, SROM_ERR_INVALID, "rom %d: ldb (%d) < n (%d)", idx, d.ldb, d.n);
     if ((d.LU == nullptr) != (d.ipiv == nullptr))
@@ -268,6 +271,7 @@ int srom_destroy(srom_handle *h) {
     if (h->d_host_arena) cudaFree(h->d_host_arena);
     if (h->d_proj) cudaFree(h->d_proj);
     if (h->d_adj) cudaFree(h->d_adj);
+    if (h->d_zero) cudaFree(h->d_zero);
     if (h->h_meta) cudaFreeHost(h->h_meta);
     if (h->meta_done) cudaEventDestroy(h->meta_done);
     for (auto &r : h->recs) {
@@ -334,7 +338,18 @@ struct SweepPlan {
     int64_t slot_bytes = 0;
     bool need_scratch = false;
     std::vector<srom::BackProj> backproj;  // ROMs whose solutions are projected onto outputs
+    // ROMs without a mass matrix.  Their descriptors point M at a zero matrix instead: for any
+    // finite w, K + (-w^2)*0 adds -0, which leaves every value (and the sign of zero) as it is,
+    // so the kernels compute (1 + i eta) K + i w D bit for bit without a second code path.
+    std::vector<int> null_m;
+    size_t zero_bytes = 0;
 };
+
+// Point the mass matrix of every ROM in P.null_m at the zero buffer (host image of the metadata).
+void patch_null_m(SweepPlan &P, const void *zero) {
+    RomDev *rd = reinterpret_cast<RomDev *>(P.meta.data());
+    for (int i : P.null_m) rd[i].M = static_cast<const double2 *>(zero);
+}
 
 // FP64 storage class of an n x n system with r right-hand sides: 0 smem kernel, 1 global
 // kernel.  The tuning table (srom_tune) overrides the default "smem when it fits".
@@ -371,6 +386,10 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
     std::vector<int> cls(n_roms, -1);
     for (int i = 0; i < n_roms; ++i) {
         dev[i] = to_dev(roms[i]);
+        if (!roms[i].M && roms[i].n > 0 && roms[i].F > 0 && roms[i].r > 0) {
+            P.null_m.push_back(i);
+            P.zero_bytes = std::max(P.zero_bytes, sizeof(srom_complex) * (size_t)roms[i].ldk * roms[i].n);
+        }
         if (roms[i].n_out > 0 && roms[i].n > 0 && roms[i].F > 0 && roms[i].r > 0)
             P.backproj.push_back(backproj_of(roms[i]));
         const srom_rom_desc &d = roms[i];
@@ -495,6 +514,7 @@ struct srom_graph {
     srom_handle *h = nullptr;
     void *d_meta = nullptr;
     void *scratch = nullptr;
+    void *d_zero = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -522,6 +542,13 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
         if (s) return s;
         scr = h->scratch;
     }
+    if (P.zero_bytes > 0) {
+        const size_t before = h->d_zero_bytes;
+        s = ensure_device_buffer(h, &h->d_zero, &h->d_zero_bytes, P.zero_bytes);
+        if (s) return s;
+        if (h->d_zero_bytes != before) SROM_CUDA(h, cudaMemsetAsync(h->d_zero, 0, h->d_zero_bytes, h->stream));
+        patch_null_m(P, h->d_zero);
+    }
     memcpy(h->h_meta, P.meta.data(), P.meta.size());
     SROM_CUDA(h, cudaMemcpyAsync(h->d_meta, h->h_meta, P.meta.size(), cudaMemcpyHostToDevice, h->stream));
     SROM_CUDA(h, cudaEventRecord(h->meta_done, h->stream));
@@ -543,6 +570,7 @@ int srom_graph_create(srom_handle *h, const srom_rom_desc *roms, int n_roms, con
     auto fail = [&](int code) {
         if (G->d_meta) cudaFree(G->d_meta);
         if (G->scratch) cudaFree(G->scratch);
+        if (G->d_zero) cudaFree(G->d_zero);
         if (G->exec) cudaGraphExecDestroy(G->exec);
         if (G->graph) cudaGraphDestroy(G->graph);
         delete G;
@@ -552,6 +580,13 @@ int srom_graph_create(srom_handle *h, const srom_rom_desc *roms, int n_roms, con
     if (e != cudaSuccess) return fail(set_err(h, SROM_ERR_ALLOC, "graph metadata: %s", cudaGetErrorString(e)));
     if (P.need_scratch && (e = cudaMalloc(&G->scratch, (size_t)P.slot_bytes * P.grid1)) != cudaSuccess)
         return fail(set_err(h, SROM_ERR_ALLOC, "graph scratch: %s", cudaGetErrorString(e)));
+    if (P.zero_bytes > 0) {
+        if ((e = cudaMalloc(&G->d_zero, P.zero_bytes)) != cudaSuccess)
+            return fail(set_err(h, SROM_ERR_ALLOC, "graph zero matrix: %s", cudaGetErrorString(e)));
+        if ((e = cudaMemset(G->d_zero, 0, P.zero_bytes)) != cudaSuccess)
+            return fail(set_err(h, SROM_ERR_CUDA, "graph zero matrix: %s", cudaGetErrorString(e)));
+        patch_null_m(P, G->d_zero);
+    }
     if ((e = cudaMemcpy(G->d_meta, P.meta.data(), P.meta.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(set_err(h, SROM_ERR_CUDA, "graph metadata copy: %s", cudaGetErrorString(e)));
     cudaStream_t cs;
@@ -594,6 +629,7 @@ int srom_graph_destroy(srom_graph *G) {
     if (G->graph) cudaGraphDestroy(G->graph);
     if (G->d_meta) cudaFree(G->d_meta);
     if (G->scratch) cudaFree(G->scratch);
+    if (G->d_zero) cudaFree(G->d_zero);
     delete G;
     return SROM_OK;
 }
@@ -771,7 +807,7 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
         const size_t nn = (size_t)d.ldk * d.n, cz = sizeof(srom_complex);
         size_t *o = &offs[i * 11];
         o[0] = take(cz * nn);
-        o[1] = take(cz * nn);
+        o[1] = d.M ? take(cz * nn) : 0;
         o[2] = d.D ? take(cz * nn) : 0;
         o[3] = take(cz * (size_t)d.ldb * d.r);
         o[4] = take(sizeof(double) * d.F);
@@ -796,7 +832,7 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
         size_t *o = &offs[i * 11];
         srom_rom_desc &e = dd[i];
         e.K = reinterpret_cast<const srom_complex *>(base + o[0]);
-        e.M = reinterpret_cast<const srom_complex *>(base + o[1]);
+        e.M = d.M ? reinterpret_cast<const srom_complex *>(base + o[1]) : nullptr;
         e.D = d.D ? reinterpret_cast<const srom_complex *>(base + o[2]) : nullptr;
         e.rhs = reinterpret_cast<const srom_complex *>(base + o[3]);
         e.omega = reinterpret_cast<const double *>(base + o[4]);
@@ -812,7 +848,7 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
             SROM_CUDA(h, cudaMemcpyAsync((void *)e.C, d.C, cz * (size_t)d.ldc * d.n, H2D, h->stream));
         }
         SROM_CUDA(h, cudaMemcpyAsync((void *)e.K, d.K, cz * nn, H2D, h->stream));
-        SROM_CUDA(h, cudaMemcpyAsync((void *)e.M, d.M, cz * nn, H2D, h->stream));
+        if (d.M) SROM_CUDA(h, cudaMemcpyAsync((void *)e.M, d.M, cz * nn, H2D, h->stream));
         if (d.D) SROM_CUDA(h, cudaMemcpyAsync((void *)e.D, d.D, cz * nn, H2D, h->stream));
         SROM_CUDA(h, cudaMemcpyAsync((void *)e.rhs, d.rhs, cz * (size_t)d.ldb * d.r, H2D, h->stream));
         SROM_CUDA(h, cudaMemcpyAsync((void *)e.omega, d.omega, sizeof(double) * d.F, H2D, h->stream));

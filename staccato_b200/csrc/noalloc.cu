@@ -81,7 +81,7 @@ extern "C" int srom_sweep_fp64_noalloc(const srom_rom_desc *d, void *cuda_stream
     if (d->n < 0 || d->r < 0 || d->F < 0) return fail(err, err_len, SROM_ERR_INVALID, "negative size");
     if (d->n == 0 || d->r == 0 || d->F == 0) return SROM_OK;
     if (!d->K || !d->M || !d->rhs || !d->omega || !d->X)
-        return fail(err, err_len, SROM_ERR_INVALID, "K, M, rhs, omega and X must be non-null");
+        return fail(err, err_len, SROM_ERR_INVALID, "K, M, rhs, omega and X must be non-null (M = NULL needs srom_sweep)");
     if (d->ldk < d->n || d->ldb < d->n) return fail(err, err_len, SROM_ERR_INVALID, "ldk and ldb must be >= n");
     if ((d->LU == nullptr) != (d->ipiv == nullptr))
         return fail(err, err_len, SROM_ERR_INVALID, "LU and ipiv must be given together");

@@ -63,7 +63,7 @@ class DeviceRom:
         omega = np.ascontiguousarray(omega, dtype=np.float64)
         F = int(omega.shape[0])
         t = lambda a: torch.from_numpy(colmajor(a)).to(device)
-        rom = cls(n=n, r=r, F=F, K=t(K), M=t(M), D=None if D is None else t(D), rhs=t(rhs),
+        rom = cls(n=n, r=r, F=F, K=t(K), M=None if M is None else t(M), D=None if D is None else t(D), rhs=t(rhs),
                   omega=torch.from_numpy(omega).to(device), eta=float(eta))
         if C is not None:
             C = np.asarray(C)
@@ -115,6 +115,48 @@ def sweep(handle: _capi.Handle, roms: Sequence[DeviceRom], precision: int = _cap
     check(handle.ptr, _capi.lib().srom_sweep(handle.ptr, arr, len(roms), C.byref(o)))
 
 
+def solve_batched(handle: _capi.Handle, A, B, precision: int = _capi.SROM_FP64,
+                  flags: int = _capi.SROM_FLAG_FALLBACK_FP64, max_refine: int = 5):
+    """Solve A_i X_i = B_i for a batch of given complex matrices: the batched
+    getrf + getrs of the reference's coupling and batched-LU programs
+    (test/IJCSA/src/IJSA.cu:1198-1206, test/krylovMidsizeTest/gpu/concurrent/batchedLU/
+    src/main.cu:254-259, cublasZgetrfBatched / cublasZgetrsBatched, there without pivoting).
+
+    Each matrix goes through the sweep kernels as a one-frequency system with K = A_i and no
+    mass or damping term (M = D = NULL), so it is factored with partial pivoting exactly like a
+    swept system.  A: (count, n, n) and B: (count, n, r) or (n, r), numpy or torch (any
+    device).  Returns (X, info) as device tensors of shape (count, n, r) and (count,)."""
+    torch = _torch()
+    dev = torch.device("cuda", handle.device)
+    A = torch.as_tensor(A, dtype=torch.complex128)
+    if A.ndim != 3 or A.shape[1] != A.shape[2]:
+        raise ValueError("A must have shape (count, n, n)")
+    count, n = int(A.shape[0]), int(A.shape[1])
+    B = torch.as_tensor(B, dtype=torch.complex128)
+    if B.ndim == 1:
+        B = B[:, None]
+    if B.ndim == 2:
+        B = B.unsqueeze(0).expand(count, -1, -1)
+    r = int(B.shape[2])
+    Acm = A.transpose(1, 2).contiguous().to(dev)  # column-major blocks
+    Bcm = B.transpose(1, 2).contiguous().to(dev)
+    X = torch.empty((count, r, n), dtype=torch.complex128, device=dev)
+    info = torch.empty(count, dtype=torch.int32, device=dev)
+    omega = torch.zeros(1, dtype=torch.float64, device=dev)
+    zb = 16  # bytes per complex128
+    descs = []
+    for i in range(count):
+        descs.append(RomDesc(n=n, r=r, F=1, ldk=n, K=C.c_void_p(Acm.data_ptr() + i * n * n * zb), M=None, D=None,
+                             eta=0.0, rhs=C.c_void_p(Bcm.data_ptr() + i * n * r * zb), ldb=n,
+                             omega=C.c_void_p(omega.data_ptr()), X=C.c_void_p(X.data_ptr() + i * n * r * zb),
+                             info=C.c_void_p(info.data_ptr() + 4 * i), steps=None, berr=None, LU=None, ipiv=None))
+    arr = (RomDesc * max(count, 1))(*descs)
+    o = opts(precision, max_refine, 0.0, flags)
+    check(handle.ptr, _capi.lib().srom_sweep(handle.ptr, arr, count, C.byref(o)))
+    torch.cuda.synchronize(dev)  # the staged copies above must outlive the kernels
+    return X.transpose(1, 2), info
+
+
 @dataclasses.dataclass
 class HostRom:
     """Host (numpy) buffers for ``sweep_host``; outputs are filled in place."""
@@ -134,7 +176,7 @@ class HostRom:
 
     def __post_init__(self):
         self.K = colmajor(self.K)
-        self.M = colmajor(self.M)
+        self.M = None if self.M is None else colmajor(self.M)
         self.D = None if self.D is None else colmajor(self.D)
         rhs = np.asarray(self.rhs, dtype=np.complex128)
         if rhs.ndim == 1:
