@@ -120,7 +120,7 @@ class ClockSampler:
 # workload (the 64-ROM batching draw of rank 0), from a one-pass ncu capture of
 # dram__bytes_read.sum + dram__bytes_write.sum over
 # `bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-e2e --no-extras` (mean of 4 launches).
-MEASURED_TRAFFIC = {"mixed_global": 544.3e9 + 443.4e9, "fp64_global": 1753.3e9 + 1807.7e9}
+MEASURED_TRAFFIC = {"mixed_global": 571.6e9 + 454.7e9, "fp64_global": 1742.5e9 + 1799.0e9}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, one-pass capture of this "
                   "workload with the current kernels; compare with the bytes the matrices alone need "
                   "(8 n^2 B per FP32 system, 16 n^2 B per FP64 system)")
