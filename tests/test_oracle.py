@@ -94,3 +94,23 @@ def test_cpu_baseline_matches_oracle():
     Xc = O.cpu_sweep(rom.K, rom.M, rom.D, 0.0, rom.rhs, rom.omega, 0, 20, threads=2)
     Xo, _ = O.sweep(rom.K, rom.M, rom.D, 0.0, rom.rhs, rom.omega[:20])
     assert O.rel_err(Xc, Xo).max() < 1e-9
+
+
+def test_oracle_no_mass_term_equals_zero_mass():
+    """M = NULL leaves the mass term out; a zero M adds -0 = (-w^2)*0 to every entry, which is
+    an exact identity for finite w -- the library relies on this when it gives the kernels a
+    zero matrix in place of a missing M."""
+    rng = np.random.default_rng(4)
+    n = 12
+    K = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    K[0, 1] = complex(-0.0, 0.0)
+    K[2, 3] = complex(0.0, -0.0)
+    D = rng.standard_normal((n, n)) * 1e-3 + 0j
+    rhs = rng.standard_normal((n, 2)) + 0j
+    for w in (0.0, 1.0, 37.5, 1e4):
+        A0 = O.assemble(K, None, D, 0.02, w)
+        Az = O.assemble(K, np.zeros((n, n), complex), D, 0.02, w)
+        assert np.array_equal(np.ascontiguousarray(A0).view(np.uint64), np.ascontiguousarray(Az).view(np.uint64))
+    X0, _ = O.sweep(K, None, D, 0.02, rhs, [0.0, 3.0])
+    Xz, _ = O.sweep(K, np.zeros((n, n), complex), D, 0.02, rhs, [0.0, 3.0])
+    assert np.array_equal(np.ascontiguousarray(X0).view(np.uint64), np.ascontiguousarray(Xz).view(np.uint64))
