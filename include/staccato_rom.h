@@ -201,6 +201,23 @@ SROM_API int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *ro
                                double *const *R);
 
 /*
+ * Complex projection R_m = Z^H A_m V (Z = V when Z is NULL), the complex form of generateROM
+ * (KrylovROMSubstructure.cpp:709-765: mkl_sparse_z_mm for y = A V, cblas_zgemm ConjTrans for
+ * Z^H y, with Z the left basis of non-symmetric MIMO systems).  A_m: complex values (nnz each,
+ * host array of n_mats device pointers) on one CSR pattern as in srom_project_real; upper != 0
+ * stores the upper triangle of a complex-symmetric matrix (A_ji = A_ij, the reference's
+ * SPARSE_MATRIX_TYPE_SYMMETRIC).  V, Z: n_rows x k complex column-major (ldv, ldz), k <= 64.
+ * R: host array of n_mats device pointers, each k x k complex column-major.  Runs on the real
+ * kernels: the basis is split into [Re V | Im V] rows, A's real and imaginary parts are applied
+ * as two value arrays of the same pattern, and the four real blocks of [Re Z | Im Z]^T
+ * [Re Y | Im Y] combine into Z^H Y.  Summation order is fixed (deterministic results).
+ */
+SROM_API int srom_project_complex(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t *rowptr,
+                                  const int *colind, int base, int upper, const srom_complex *const *vals, int n_mats,
+                                  const srom_complex *V, int k, int64_t ldv, const srom_complex *Z, int64_t ldz,
+                                  srom_complex *const *R);
+
+/*
  * FP64 block Gram-Schmidt orthonormalisation of V (n_rows x k, column-major, ldv) in place,
  * the reference's block scheme with re-orthogonalisation (KrylovROMSubstructure.cpp:433-475,
  * :513-534): the columns are taken in panels of 32; each pass projects the panel out of the

@@ -32,7 +32,8 @@ SROM_INFO_NOT_CONVERGED = -1
 EXPORTS = [
     "srom_create", "srom_destroy", "srom_set_stream", "srom_status_string", "srom_last_error",
     "srom_version", "srom_sweep", "srom_sweep_host", "srom_profile_enable", "srom_profile_read",
-    "srom_sweep_fp64_noalloc", "srom_project_real", "srom_orthonormalize", "srom_sweep_backward",
+    "srom_sweep_fp64_noalloc", "srom_project_real", "srom_project_complex", "srom_orthonormalize",
+    "srom_sweep_backward",
     "srom_graph_create", "srom_graph_launch", "srom_graph_destroy", "srom_tune",
     "srom_mtx_read_dense", "srom_mtx_write_dense", "srom_write_solution",
 ]
@@ -108,6 +109,9 @@ def lib() -> C.CDLL:
         L.srom_project_real.argtypes = [vp, C.c_int64, vp, vp, i, i, C.POINTER(C.c_void_p), i, vp, i,
                                         C.c_int64, C.POINTER(C.c_void_p)]
         L.srom_project_real.restype = i
+        L.srom_project_complex.argtypes = [vp, C.c_int64, C.c_int64, vp, vp, i, i, C.POINTER(C.c_void_p), i, vp, i,
+                                           C.c_int64, vp, C.c_int64, C.POINTER(C.c_void_p)]
+        L.srom_project_complex.restype = i
         L.srom_orthonormalize.argtypes = [vp, vp, C.c_int64, i, C.c_int64, i]
         L.srom_orthonormalize.restype = i
         L.srom_graph_create.argtypes = [vp, C.POINTER(RomDesc), i, C.POINTER(SweepOpts), pp]

@@ -679,6 +679,77 @@ int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *rowptr, con
     return SROM_OK;
 }
 
+int srom_project_complex(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind,
+                         int base, int upper, const srom_complex *const *vals, int n_mats, const srom_complex *V, int k,
+                         int64_t ldv, const srom_complex *Z, int64_t ldz, srom_complex *const *R) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    if (n_rows < 0 || k < 0 || nnz < 0) return set_err(h, SROM_ERR_INVALID, "negative size");
+    if (n_mats < 1 || n_mats > 3) return set_err(h, SROM_ERR_INVALID, "n_mats must be 1..3");
+    if (k > 64) return set_err(h, SROM_ERR_UNSUPPORTED, "k = %d exceeds 64 (complex form)", k);
+    if (base != 0 && base != 1) return set_err(h, SROM_ERR_INVALID, "base must be 0 or 1");
+    if (!vals || !R) return set_err(h, SROM_ERR_INVALID, "vals and R must be non-null");
+    for (int m = 0; m < n_mats; ++m)
+        if (!vals[m] || !R[m]) return set_err(h, SROM_ERR_INVALID, "vals[%d] / R[%d] is null", m, m);
+    if (n_rows == 0 || k == 0) return SROM_OK;
+    if (!rowptr || !colind || !V) return set_err(h, SROM_ERR_INVALID, "rowptr, colind and V must be non-null");
+    if (ldv < n_rows || (Z && ldz < n_rows)) return set_err(h, SROM_ERR_INVALID, "ldv / ldz < n_rows");
+    DeviceGuard g(h->device);
+    const int k2 = 2 * k, kp = (k2 + 7) & ~7;
+    const int nblk = h->sm_count;
+    const size_t w_b = align_up(sizeof(double) * (size_t)n_rows * k2, 256);
+    const size_t v_b = align_up(sizeof(double) * (size_t)nnz, 256);
+    const size_t p_b = align_up(sizeof(double) * (size_t)nblk * kp * kp, 256);
+    const size_t g_b = align_up(sizeof(double) * (size_t)k2 * k2, 256);
+    // Vt2 [Re V | Im V], Zt2 (when Z is given), Ar, Ai, P_r, P_i, partials, G
+    const size_t need = w_b * (Z ? 4 : 3) + 2 * v_b + p_b + g_b;
+    int s = ensure_device_buffer(h, &h->d_proj, &h->d_proj_bytes, need);
+    if (s) return s;
+    char *bp = static_cast<char *>(h->d_proj);
+    double *Vt2 = reinterpret_cast<double *>(bp);
+    bp += w_b;
+    double *Zt2 = Vt2;
+    if (Z) {
+        Zt2 = reinterpret_cast<double *>(bp);
+        bp += w_b;
+    }
+    double *Pr = reinterpret_cast<double *>(bp);
+    bp += w_b;
+    double *Pi = reinterpret_cast<double *>(bp);
+    bp += w_b;
+    double *Ar = reinterpret_cast<double *>(bp);
+    bp += v_b;
+    double *Ai = reinterpret_cast<double *>(bp);
+    bp += v_b;
+    double *part = reinterpret_cast<double *>(bp);
+    bp += p_b;
+    double *G = reinterpret_cast<double *>(bp);
+    SROM_CUDA(h, srom::launch_transpose_split(reinterpret_cast<const double2 *>(V), n_rows, k, ldv, Vt2, h->stream));
+    if (Z) SROM_CUDA(h, srom::launch_transpose_split(reinterpret_cast<const double2 *>(Z), n_rows, k, ldz, Zt2, h->stream));
+    for (int m = 0; m < n_mats; ++m) {
+        SROM_CUDA(h, srom::launch_split_values(reinterpret_cast<const double2 *>(vals[m]), nnz, Ar, Ai, h->sm_count,
+                                               h->stream));
+        srom::ProjVals pv{};
+        pv.v[0] = Ar;
+        pv.v[1] = Ai;
+        {
+            ProfScope ps(h, "spmm_complex", n_rows, 0.0, 0.0);
+            // P_r and P_i are adjacent: the SpMM writes matrix m' of pv at Pr + m' * (n_rows * 2k)
+            SROM_CUDA(h, srom::launch_spmm(n_rows, rowptr, colind, base, upper, pv, 2, Vt2, k2, Pr,
+                                           (int64_t)(Pi - Pr), h->sm_count, h->stream));
+        }
+        SROM_CUDA(h, srom::launch_combine_y(Pr, Pi, n_rows, k, h->sm_count, h->stream));
+        srom::ProjOut po{};
+        po.r[0] = G;
+        {
+            ProfScope ps(h, "vty_dmma_complex", n_rows, 2.0 * (double)n_rows * k2 * k2, 0.0);
+            SROM_CUDA(h, srom::launch_vty(n_rows, k2, Zt2, Pr, 0, 1, nblk, part, po, h->stream));
+        }
+        SROM_CUDA(h, srom::launch_combine_r(G, k, reinterpret_cast<double2 *>(R[m]), h->stream));
+    }
+    return SROM_OK;
+}
+
 int srom_sweep_backward(srom_handle *h, const srom_rom_desc *rom, const srom_complex *gbar, int ldg,
                         const srom_dparam *params, int n_params, double *dJdp, srom_complex *lambda) {
     if (!h) return SROM_ERR_INVALID;

@@ -542,6 +542,95 @@ __global__ void __launch_bounds__(256, 2) gs_update_kernel(double *__restrict__ 
         if (cb + c < b) V[r + (int64_t)(j0 + cb + c) * ldv] = o[c];
 }
 
+// ---- complex projection R = Z^H A V through the real kernels ------------------------------
+// With A = Ar + i Ai and the basis stored as the real N x 2k rows [Re V | Im V], the real SpMM
+// over the two value arrays (Ar, Ai) gives P_r = Ar [Vr | Vi] and P_i = Ai [Vr | Vi]; then
+// Y = A V has Re Y = Ar Vr - Ai Vi and Im Y = Ar Vi + Ai Vr (combined in place into P_r's rows
+// as [Re Y | Im Y]), and the real V^T Y kernel on W = [Re Z | Im Z] gives G = W^T [Re Y | Im Y],
+// whose four k x k blocks combine into Z^H Y = (Zr^T Yr + Zi^T Yi) + i (Zr^T Yi - Zi^T Yr).
+
+// V (complex, column-major, ldv) -> Wt (real, row-major N x 2k: [Re V(row) | Im V(row)])
+__global__ void transpose_split_kernel(const double2 *__restrict__ V, int64_t N, int k, int64_t ldv,
+                                       double *__restrict__ Wt) {
+    __shared__ double2 t[32][33];
+    const int64_t r0 = (int64_t)blockIdx.x * 32;
+    const int c0 = blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int64_t r = r0 + threadIdx.x;
+        const int c = c0 + y;
+        if (r < N && c < k) t[y][threadIdx.x] = V[r + (int64_t)c * ldv];
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int64_t r = r0 + y;
+        const int c = c0 + threadIdx.x;
+        if (r < N && c < k) {
+            const double2 v = t[threadIdx.x][y];
+            Wt[r * 2 * k + c] = v.x;
+            Wt[r * 2 * k + k + c] = v.y;
+        }
+    }
+}
+
+// complex values -> separate real and imaginary arrays
+__global__ void split_values_kernel(const double2 *__restrict__ a, int64_t nnz, double *__restrict__ re,
+                                    double *__restrict__ im) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = a[e];
+        re[e] = v.x;
+        im[e] = v.y;
+    }
+}
+
+// rows of P_r = [Ar Vr | Ar Vi] and P_i = [Ai Vr | Ai Vi] -> rows of P_r = [Re Y | Im Y]
+__global__ void combine_y_kernel(double *__restrict__ Pr, const double *__restrict__ Pi, int64_t N, int k) {
+    const int64_t tot = N * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / k;
+        const int c = (int)(e % k);
+        double *pr = Pr + r * 2 * k;
+        const double *pi = Pi + r * 2 * k;
+        const double yr = pr[c] - pi[k + c];
+        const double yi = pr[k + c] + pi[c];
+        pr[c] = yr;
+        pr[k + c] = yi;
+    }
+}
+
+// G (2k x 2k, column-major) -> R (k x k complex, column-major)
+__global__ void combine_r_kernel(const double *__restrict__ G, int k, double2 *__restrict__ R) {
+    const int k2 = 2 * k;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < k * k; e += gridDim.x * blockDim.x) {
+        const int a = e % k, b = e / k;
+        const double re = G[a + (int64_t)b * k2] + G[(k + a) + (int64_t)(k + b) * k2];
+        const double im = G[a + (int64_t)(k + b) * k2] - G[(k + a) + (int64_t)b * k2];
+        R[a + (int64_t)b * k] = make_double2(re, im);
+    }
+}
+
+cudaError_t launch_transpose_split(const double2 *V, int64_t N, int k, int64_t ldv, double *Wt, cudaStream_t st) {
+    dim3 grid((unsigned)((N + 31) / 32), (unsigned)((k + 31) / 32)), block(32, 8);
+    transpose_split_kernel<<<grid, block, 0, st>>>(V, N, k, ldv, Wt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_split_values(const double2 *a, int64_t nnz, double *re, double *im, int sms, cudaStream_t st) {
+    const int grid = (int)std::min<int64_t>((nnz + 255) / 256, (int64_t)sms * 8);
+    if (grid > 0) split_values_kernel<<<grid, 256, 0, st>>>(a, nnz, re, im);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_combine_y(double *Pr, const double *Pi, int64_t N, int k, int sms, cudaStream_t st) {
+    const int grid = (int)std::min<int64_t>((N * k + 255) / 256, (int64_t)sms * 8);
+    if (grid > 0) combine_y_kernel<<<grid, 256, 0, st>>>(Pr, Pi, N, k);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_combine_r(const double *G, int k, double2 *R, cudaStream_t st) {
+    combine_r_kernel<<<(k * k + 255) / 256, 256, 0, st>>>(G, k, R);
+    return cudaGetLastError();
+}
+
 // ---- host launchers -------------------------------------------------------------------------
 cudaError_t launch_transpose(const double *V, int64_t N, int k, int64_t ldv, double *Vt, cudaStream_t st) {
     dim3 grid((unsigned)((N + 31) / 32), (unsigned)((k + 31) / 32)), block(32, 8);

@@ -21,6 +21,10 @@ cudaError_t launch_spmm(int64_t N, const int64_t *rowptr, const int *colind, int
 size_t vty_smem_bytes(int k, int n_mats);
 cudaError_t launch_vty(int64_t N, int k, const double *Vt, const double *Y, int64_t y_stride, int n_mats, int nblk,
                        double *partial, ProjOut out, cudaStream_t st);
+cudaError_t launch_transpose_split(const double2 *V, int64_t N, int k, int64_t ldv, double *Wt, cudaStream_t st);
+cudaError_t launch_split_values(const double2 *a, int64_t nnz, double *re, double *im, int sms, cudaStream_t st);
+cudaError_t launch_combine_y(double *Pr, const double *Pi, int64_t N, int k, int sms, cudaStream_t st);
+cudaError_t launch_combine_r(const double *G, int k, double2 *R, cudaStream_t st);
 size_t gs_workspace_doubles(int k, int nblk);
 cudaError_t launch_gram_schmidt(double *V, int64_t N, int k, int64_t ldv, int passes, double *work, int nblk,
                                 cudaStream_t st);

@@ -55,6 +55,28 @@ def project(handle: _capi.Handle, csr: DeviceCsr, values: Sequence, V) -> List:
     return [o.t() for o in outs]
 
 
+def project_complex(handle: _capi.Handle, csr: DeviceCsr, values: Sequence, V, Z=None) -> List:
+    """R_m = Z^H A_m V (Z = V by default) for complex values sharing one CSR pattern
+    (``srom_project_complex``, k <= 64).  values: complex128 tensors (nnz each); V, Z:
+    contiguous (k, n_rows) complex128 tensors = n_rows x k column-major bases.  Returns k x k
+    complex128 tensors."""
+    import torch
+
+    k, n = int(V.shape[0]), int(V.shape[1])
+    assert n == csr.n_rows and V.is_contiguous() and V.dtype == torch.complex128
+    if Z is not None:
+        assert tuple(Z.shape) == (k, n) and Z.is_contiguous() and Z.dtype == torch.complex128
+    nnz = int(values[0].numel())
+    outs = [torch.empty((k, k), dtype=torch.complex128, device=V.device) for _ in values]
+    vals = (C.c_void_p * len(values))(*[C.c_void_p(v.data_ptr()) for v in values])
+    rs = (C.c_void_p * len(values))(*[C.c_void_p(o.data_ptr()) for o in outs])
+    check(handle.ptr, _capi.lib().srom_project_complex(
+        handle.ptr, csr.n_rows, nnz, C.c_void_p(csr.rowptr.data_ptr()), C.c_void_p(csr.colind.data_ptr()),
+        csr.base, int(csr.upper), vals, len(values), C.c_void_p(V.data_ptr()), k, n,
+        None if Z is None else C.c_void_p(Z.data_ptr()), n, rs))
+    return [o.t() for o in outs]
+
+
 def orthonormalize(handle: _capi.Handle, V, passes: int = 2) -> None:
     """In-place block Gram-Schmidt (``passes`` projection passes per 32-column panel) of an
     n x k column-major basis given as a contiguous (k, n) float64 tensor."""

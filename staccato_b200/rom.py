@@ -20,7 +20,7 @@ from typing import Optional
 import numpy as np
 
 from . import _capi
-from .project import DeviceCsr, orthonormalize, project
+from .project import DeviceCsr, orthonormalize, project, project_complex
 from .sweep import DeviceRom, sweep
 
 
@@ -42,19 +42,31 @@ class KrylovROMSubstructure:
         self.eta = float(eta)
 
     def generate_rom(self, csr: DeviceCsr, K_vals, M_vals, V, D_vals=None, B=None, C=None, eta: float = 0.0):
-        """Projection of the FE operators (real, sharing the CSR pattern) onto V.
+        """Projection of the FE operators (sharing the CSR pattern) onto V, as generateROM
+        (KrylovROMSubstructure.cpp:709-765): K_r = V^H K V, M_r = V^H M V, D_r = V^H D V,
+        B_r = V^H B, C_r = C V.
 
-        V: (k, n) float64 tensor = n x k column-major basis.  B: n x n_in, C: n_out x n."""
+        V: (k, n) tensor = n x k column-major basis, float64 (real form, k <= 128) or
+        complex128 (complex form, k <= 64; complex values are used as given, real values are
+        promoted).  B: n x n_in, C: n_out x n."""
         import torch
 
         mats = [K_vals, M_vals] + ([D_vals] if D_vals is not None else [])
-        R = project(self.handle, csr, mats, V)
-        to_c = lambda r: r.to(torch.complex128)
+        complex_form = V.dtype == torch.complex128 or any(torch.as_tensor(a).is_complex() for a in mats)
+        if complex_form:
+            Vc = V.to(torch.complex128).contiguous()
+            R = project_complex(self.handle, csr, [torch.as_tensor(a).to(torch.complex128).contiguous() for a in mats],
+                                Vc)
+            to_c = lambda r: r
+        else:
+            Vc = V
+            R = project(self.handle, csr, mats, V)
+            to_c = lambda r: r.to(torch.complex128)
         self.K_r, self.M_r = to_c(R[0]), to_c(R[1])
         self.D_r = to_c(R[2]) if D_vals is not None else None
-        Vcm = V.t()  # n x k view
-        self.B_r = None if B is None else (Vcm.t().to(torch.complex128) @ torch.as_tensor(B, device=V.device).to(torch.complex128))
-        self.C_r = None if C is None else (torch.as_tensor(C, device=V.device).to(torch.complex128) @ Vcm.to(torch.complex128))
+        Vcm = Vc.t().to(torch.complex128)  # n x k
+        self.B_r = None if B is None else (Vcm.conj().t() @ torch.as_tensor(B, device=V.device).to(torch.complex128))
+        self.C_r = None if C is None else (torch.as_tensor(C, device=V.device).to(torch.complex128) @ Vcm)
         self.eta = float(eta)
         return R
 
