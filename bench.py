@@ -297,6 +297,47 @@ def adjoint_leg(torch, dev, h):
             "grad_p0": float(gh[0]), "fd_p0": float(fd0), "rel_diff_p0": float(abs(gh[0] - fd0) / abs(fd0))}
 
 
+def workloads_leg(torch, dev, h, reps=3):
+    """Both forms on the single-ROM workloads beside the batching one: plain (n = 64, 500
+    frequencies, r = 1) and precision (n = 256, 4096 frequencies, 60 % within 0.1 % of an
+    eigenfrequency, r = 8, damping D).  Device time per sweep (median of reps), freq-solves/s,
+    and for the mixed form the error against the oracle's refined x_ref on every 16th
+    frequency."""
+    from oracle import oracle as O
+    from staccato_b200 import _capi, workloads as W
+    from staccato_b200.sweep import DeviceRom, sweep
+
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for name, rom in (("plain_n64", W.plain_rom()), ("precision_n256", W.precision_rom())):
+        d = DeviceRom.from_host(rom.K, rom.M, rom.D, rom.rhs, rom.omega, device=dev)
+        res = {"n": rom.n, "F": rom.F, "r": int(rom.rhs.shape[1])}
+        for form, prec, flags in (("fp64", _capi.SROM_FP64, 0),
+                                  ("mixed", _capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)):
+            sweep(h, [d], precision=prec, flags=flags)
+            ts = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                sweep(h, [d], precision=prec, flags=flags)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                ts.append(e0.elapsed_time(e1))
+            ms = float(np.median(ts))
+            res[form] = {"ms": ms, "freq_solves_per_s": rom.F / (ms * 1e-3)}
+            if form == "mixed":
+                sel = slice(None, None, 16)
+                X = d.solutions()[sel]
+                Xr = O.x_ref(rom.K, rom.M, rom.D, 0.0, rom.rhs, rom.omega[sel])
+                err = O.rel_err(X, Xr)
+                res[form]["max_rel_err"] = float(err.max())
+                st = d.steps.cpu().numpy()
+                res[form]["refine_steps_hist"] = {str(k): int(v) for k, v in zip(*np.unique(st, return_counts=True))}
+        res["mixed_vs_plain"] = res["mixed"]["freq_solves_per_s"] / res["fp64"]["freq_solves_per_s"]
+        out[name] = res
+    return out
+
+
 # ----------------------------------------------------------------------------- arms
 
 def run_reference(args):
@@ -486,6 +527,7 @@ def run_ours(args):
     if rank == 0 and not args.no_extras:
         extras["projection"] = projection_leg(torch, dev, h, measured_peaks())
         extras["adjoint"] = adjoint_leg(torch, dev, h)
+        extras["workloads"] = workloads_leg(torch, dev, h)
 
     cpu = acc = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -519,6 +561,7 @@ def run_ours(args):
             "gpu_launches": int(nrec),
             "projection": extras.get("projection"),
             "adjoint": extras.get("adjoint"),
+            "workloads": extras.get("workloads"),
         }
         print(json.dumps(line), flush=True)
     if pg is not None:
