@@ -60,6 +60,10 @@ typedef struct {
 /* ---- sweep flags ---------------------------------------------------------------------- */
 #define SROM_FLAG_FALLBACK_FP64 1 /* re-solve non-converged frequencies with the FP64 kernel */
 #define SROM_FLAG_KEEP_FACTORS 2  /* write LU factors + pivots into desc.LU / desc.ipiv (FP64) */
+#define SROM_FLAG_MIXED_EVERY 4   /* mixed forms: factor every system in FP32.  Without it, systems
+                                     small enough for two FP64 shared-memory factorisations per SM
+                                     (n <= ~84) are solved by the FP64 kernel outright (steps = 0),
+                                     which is faster than FP32 factors plus refinement there   */
 
 /*
  * One reduced-order model and its frequency request.  Mirrors the members the reference's
@@ -83,7 +87,8 @@ typedef struct {
     const double *omega;    /* F angular frequencies (rad/s)                         */
     srom_complex *X;        /* F blocks of n x r (ld n): x(w_f) = A(w_f)^-1 rhs      */
     int *info;              /* F ints or NULL                                        */
-    int *steps;             /* F ints or NULL: refinement steps taken (-1: FP64 fallback) */
+    int *steps;             /* F ints or NULL: refinement steps taken (0: solved in FP64
+                               outright, -1: FP64 fallback)                          */
     double *berr;           /* F doubles or NULL: estimated relative error left (mixed) */
     srom_complex *LU;       /* F blocks of n x n or NULL (SROM_FLAG_KEEP_FACTORS)    */
     int *ipiv;              /* F blocks of n ints (1-based) or NULL                  */

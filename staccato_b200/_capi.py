@@ -25,6 +25,7 @@ SROM_MIXED_TF32 = 2
 
 SROM_FLAG_FALLBACK_FP64 = 1
 SROM_FLAG_KEEP_FACTORS = 2
+SROM_FLAG_MIXED_EVERY = 4
 
 SROM_INFO_NOT_CONVERGED = -1
 

@@ -177,6 +177,20 @@ int validate_desc(srom_handle *h, const srom_rom_desc &d, int idx) {
     return SROM_OK;
 }
 
+// Device descriptors (srom_sweep, graphs, srom_sweep_backward): every array must be aligned to
+// its element's vector width.  srom_sweep_host copies into its own aligned arena instead.
+int validate_device_alignment(srom_handle *h, const srom_rom_desc &d, int idx) {
+    if (d.n == 0 || d.F == 0 || d.r == 0) return SROM_OK;
+    const void *cz[] = {d.K, d.M, d.D, d.rhs, d.X, d.LU, d.C, d.Y};
+    for (const void *p : cz)
+        if (srom::misaligned(p, 16))
+            return set_err(h, SROM_ERR_INVALID, "rom %d: complex arrays on the device must be 16-byte aligned", idx);
+    if (srom::misaligned(d.omega, 8) || srom::misaligned(d.berr, 8) || srom::misaligned(d.info, 4) ||
+        srom::misaligned(d.steps, 4) || srom::misaligned(d.ipiv, 4))
+        return set_err(h, SROM_ERR_INVALID, "rom %d: omega/berr must be 8-byte and info/steps/ipiv 4-byte aligned", idx);
+    return SROM_OK;
+}
+
 // Back-projection launch parameters of a descriptor (n_out = 0: none).
 srom::BackProj backproj_of(const srom_rom_desc &d) {
     srom::BackProj b{};
@@ -361,6 +375,17 @@ int fp64_class(const srom_handle *h, int n, int r) {
     return 0;
 }
 
+// Mixed-form class: a system the FP64 shared-memory kernel holds two or more at a time per SM
+// is solved there outright.  At those orders (n <= ~84 for r <= 4) one FP64 factorisation in
+// shared memory is faster than complex-FP32 factors in the global kernel plus refinement
+// (measured 1.5-2.2x at n = 32..80), and its result is the FP64 form's, bit for bit (steps = 0).
+// Larger systems, or any with SROM_FLAG_MIXED_EVERY, go to the mixed global kernel.
+int mixed_class(const srom_handle *h, int n, int r, int flags) {
+    if (flags & SROM_FLAG_MIXED_EVERY) return 1;
+    if (fp64_class(h, n, r) != 0) return 1;
+    return srom::fp64_smem_blocks_per_sm(srom::fp64_smem_bytes(n, r)) >= 2 ? 0 : 1;
+}
+
 int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts, SweepPlan &P) {
     if (n_roms < 0 || (n_roms > 0 && !roms)) return set_err(h, SROM_ERR_INVALID, "roms is null");
     srom_sweep_opts o = opts ? *opts : srom_sweep_opts{SROM_FP64, 5, 0.0, 0};
@@ -371,6 +396,7 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
     if (o.tol < 0.0) return set_err(h, SROM_ERR_INVALID, "tol must be >= 0");
     for (int i = 0; i < n_roms; ++i) {
         int s = validate_desc(h, roms[i], i);
+        if (!s) s = validate_device_alignment(h, roms[i], i);
         if (s) return s;
         if (mixed && roms[i].LU)
             return set_err(h, SROM_ERR_UNSUPPORTED, "rom %d: factors are kept only by the FP64 form", i);
@@ -380,7 +406,8 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
     P.mixed = mixed;
     P.o = o;
     // FP64: systems that fit shared memory use the smem kernel (unless tuned otherwise),
-    // the rest the global kernel.  Mixed: every system uses the global kernel.
+    // the rest the global kernel.  Mixed: the smallest systems use the FP64 smem kernel
+    // (mixed_class), the rest the mixed global kernel.
     const size_t smem_cap = (size_t)h->max_smem_optin;
     std::vector<RomDev> dev(n_roms);
     std::vector<int> cls(n_roms, -1);
@@ -394,7 +421,7 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
             P.backproj.push_back(backproj_of(roms[i]));
         const srom_rom_desc &d = roms[i];
         if (d.n == 0 || d.F == 0 || d.r == 0) continue;
-        cls[i] = mixed ? 1 : fp64_class(h, d.n, d.r);
+        cls[i] = mixed ? mixed_class(h, d.n, d.r, o.flags) : fp64_class(h, d.n, d.r);
         if (cls[i] == 0) {
             P.smem_max = std::max(P.smem_max, srom::fp64_smem_bytes(d.n, d.r));
         } else {
@@ -694,6 +721,10 @@ int srom_project_complex(srom_handle *h, int64_t n_rows, int64_t nnz, const int6
     if (n_rows == 0 || k == 0) return SROM_OK;
     if (!rowptr || !colind || !V) return set_err(h, SROM_ERR_INVALID, "rowptr, colind and V must be non-null");
     if (ldv < n_rows || (Z && ldz < n_rows)) return set_err(h, SROM_ERR_INVALID, "ldv / ldz < n_rows");
+    bool bad = srom::misaligned(V, 16) || srom::misaligned(Z, 16) || srom::misaligned(rowptr, 8) ||
+               srom::misaligned(colind, 4);
+    for (int m = 0; m < n_mats; ++m) bad = bad || srom::misaligned(vals[m], 16) || srom::misaligned(R[m], 16);
+    if (bad) return set_err(h, SROM_ERR_INVALID, "complex arrays must be 16-byte aligned (rowptr 8, colind 4)");
     DeviceGuard g(h->device);
     const int k2 = 2 * k, kp = (k2 + 7) & ~7;
     const int nblk = h->sm_count;
@@ -756,7 +787,10 @@ int srom_sweep_backward(srom_handle *h, const srom_rom_desc *rom, const srom_com
     h->err.clear();
     if (!rom) return set_err(h, SROM_ERR_INVALID, "rom is null");
     int s = validate_desc(h, *rom, 0);
+    if (!s) s = validate_device_alignment(h, *rom, 0);
     if (s) return s;
+    if (srom::misaligned(gbar, 16) || srom::misaligned(lambda, 16) || srom::misaligned(dJdp, 8))
+        return set_err(h, SROM_ERR_INVALID, "gbar/lambda must be 16-byte and dJdp 8-byte aligned");
     if (n_params < 0 || (n_params > 0 && (!params || !dJdp)))
         return set_err(h, SROM_ERR_INVALID, "params and dJdp must be non-null");
     if (rom->n == 0 || rom->F == 0 || rom->r == 0 || n_params == 0) {
@@ -769,6 +803,8 @@ int srom_sweep_backward(srom_handle *h, const srom_rom_desc *rom, const srom_com
     std::vector<srom::DParamTerm> terms;
     for (int j = 0; j < n_params; ++j) {
         const srom_dparam &p = params[j];
+        if (srom::misaligned(p.U, 16) || srom::misaligned(p.W, 16) || srom::misaligned(p.G, 16))
+            return set_err(h, SROM_ERR_INVALID, "param %d: U, W and G must be 16-byte aligned", j);
         srom::DParamDev &d = pd[j];
         d.kind = p.kind;
         d.rank = p.rank;

@@ -87,6 +87,15 @@ extern "C" int srom_sweep_fp64_noalloc(const srom_rom_desc *d, void *cuda_stream
         return fail(err, err_len, SROM_ERR_INVALID, "LU and ipiv must be given together");
     if (d->n_out < 0 || (d->n_out > 0 && (!d->C || !d->Y || d->ldc < d->n_out)))
         return fail(err, err_len, SROM_ERR_INVALID, "n_out > 0 needs C, Y and ldc >= n_out");
+    {
+        const void *cz[] = {d->K, d->M, d->D, d->rhs, d->X, d->LU, d->C, d->Y};
+        bool bad = srom::misaligned(d->omega, 8) || srom::misaligned(d->berr, 8) || srom::misaligned(d->info, 4) ||
+                   srom::misaligned(d->steps, 4) || srom::misaligned(d->ipiv, 4);
+        for (const void *p : cz) bad = bad || srom::misaligned(p, 16);
+        if (bad)
+            return fail(err, err_len, SROM_ERR_INVALID,
+                        "complex arrays must be 16-byte aligned (omega/berr 8, info/steps/ipiv 4)");
+    }
     if (d->n > NOALLOC_MAX_N) {
         char b[96];
         snprintf(b, sizeof b, "n = %d exceeds the limit of %d", d->n, NOALLOC_MAX_N);

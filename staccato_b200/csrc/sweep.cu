@@ -285,7 +285,7 @@ __device__ void lu_solve_strips(const T *A, int64_t lda, int n, T *B, int ldb, i
     };
     issue_f(0);
     for (int blk = 0; blk < nblk; ++blk) {
-        const int jb = blk * SW, bs = min(SW, n - jb), je = jb + bs, rows = n - jb;
+        const int jb = blk * SW, bs = min(SW, n - jb), rows = n - jb;
         if (blk + 1 < nblk) {
             issue_f(blk + 1);
             cp_async_wait<1>();

@@ -10,6 +10,11 @@ namespace srom {
 struct RomDev;
 struct Item;
 
+// The kernels read and write complex values as 16-byte vectors (double2), doubles as 8 bytes
+// and ints as 4; srom_complex itself only promises 8-byte alignment, so device pointers are
+// checked on the host before any launch (a misaligned vector access would fault the kernel).
+inline bool misaligned(const void *p, size_t a) { return p && (reinterpret_cast<uintptr_t>(p) % a) != 0; }
+
 // ---- FP64 (bit-identical to the restated zgetrf/zgetrs) ----
 size_t fp64_smem_bytes(int n, int r);
 size_t fp64_global_smem_bytes(int n_max, int r_max);

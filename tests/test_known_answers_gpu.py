@@ -11,7 +11,9 @@ from staccato_b200.sweep import DeviceRom, sweep
 
 pytestmark = pytest.mark.gpu
 
-FORMS = [(_capi.SROM_FP64, 0), (_capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)]
+# the mixed form with every system in the mixed kernel (small ones included)
+FORMS = [(_capi.SROM_FP64, 0),
+         (_capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64 | _capi.SROM_FLAG_MIXED_EVERY)]
 
 
 def _run(handle, K, M, rhs, omega, eta, form):

@@ -137,3 +137,27 @@ def test_empty_roms_in_a_batch(handle, form):
             assert _bits_equal(rom.solutions(), Xo)
         else:
             assert O.rel_err(rom.solutions(), O.x_ref(sysd[0], sysd[1], None, 0.0, sysd[3], sysd[4])).max() <= 1e-10
+
+
+@pytest.mark.parametrize("field", ["K", "M", "rhs", "X", "Y"])
+def test_misaligned_device_arrays_are_rejected(handle, field):
+    """A complex array that is 8- but not 16-byte aligned is refused on the host before any
+    launch (the kernels access complex values as 16-byte vectors)."""
+    import torch
+
+    K, M, _, rhs, omega = _system(21, 8, 2, 3)
+    Cm = np.ones((2, 8), dtype=np.complex128)
+    rom = DeviceRom.from_host(K, M, None, rhs, omega, C=Cm)
+    d = rom.desc()
+    setattr(d, field, getattr(d, field) + 8)
+    arr = (_capi.RomDesc * 1)(d)
+    for prec in (_capi.SROM_FP64, _capi.SROM_MIXED_FP32):
+        o = _capi.SweepOpts(precision=prec, max_refine=5, tol=0.0, flags=0)
+        st = _capi.lib().srom_sweep(handle.ptr, arr, 1, C.byref(o))
+        assert st == _capi.SROM_ERR_INVALID
+        assert b"aligned" in _capi.lib().srom_last_error(handle.ptr)
+    torch.cuda.synchronize()
+    sweep(handle, [rom])  # the aligned descriptor still works on the same handle
+    torch.cuda.synchronize()
+    Xo, _ = O.sweep(K, M, None, 0.0, rhs, omega)
+    assert _bits_equal(rom.solutions(), Xo)

@@ -15,6 +15,7 @@ pytestmark = pytest.mark.gpu
 
 MIXED = _capi.SROM_MIXED_FP32
 FALLBACK = _capi.SROM_FLAG_FALLBACK_FP64
+EVERY = _capi.SROM_FLAG_MIXED_EVERY  # keeps the smallest systems in the mixed kernel
 
 
 def _run(handle, rom_like, omega, precision=MIXED, flags=FALLBACK, max_refine=5):
@@ -31,7 +32,7 @@ def test_mixed_random_wellconditioned(handle, n):
     M = c((n, n)) * 0.1
     r = 3 if n < 300 else 1
     rom = W.Rom(K=K, M=M, D=c((n, n)) * 0.01, rhs=c((n, r)), omega=rng.uniform(0.1, 1.0, 4))
-    d = _run(handle, rom, rom.omega, flags=0)
+    d = _run(handle, rom, rom.omega, flags=EVERY)
     xr = O.x_ref(rom.K, rom.M, rom.D, 0.0, rom.rhs, rom.omega)
     err = O.rel_err(d.solutions(), xr)
     assert err.max() <= 1e-10, err
@@ -44,10 +45,36 @@ def test_mixed_random_wellconditioned(handle, n):
 def test_mixed_plain_workload(handle):
     rom = W.plain_rom()
     sel = rom.omega  # all 500 frequencies: the gate is on the maximum
-    d = _run(handle, rom, sel)
+    d = _run(handle, rom, sel, flags=FALLBACK | EVERY)
     xr = O.x_ref(rom.K, rom.M, rom.D, 0.0, rom.rhs, sel)
     assert O.rel_err(d.solutions(), xr).max() <= 1e-10
-    assert (d.steps.cpu().numpy() >= 0).all()  # no fallback needed on this workload
+    assert (d.steps.cpu().numpy() >= 1).all()  # refined, and no fallback needed on this workload
+
+
+@pytest.mark.parametrize("n,r,routed", [(40, 2, True), (80, 4, True), (96, 1, False), (128, 4, False)])
+def test_mixed_form_solves_small_systems_in_fp64(n, r, routed):
+    """Without SROM_FLAG_MIXED_EVERY, systems held two per SM by the FP64 shared-memory kernel
+    are solved by it outright: the FP64 form's bits, steps = 0, berr = 0.  Larger ones are
+    refined.  A fresh handle, so that no tuning table changes the kernel choice."""
+    h = _capi.Handle(0)
+    try:
+        rom = W.plain_rom(n=n, F=40)
+        rng = np.random.default_rng(n)
+        rhs = rng.standard_normal((n, r)) + 1j * rng.standard_normal((n, r))
+        d = DeviceRom.from_host(rom.K, rom.M, rom.D, rhs, rom.omega)
+        sweep(h, [d], precision=MIXED, flags=FALLBACK)
+        steps = d.steps.cpu().numpy()
+        xr = O.x_ref(rom.K, rom.M, rom.D, 0.0, rhs, rom.omega)
+        assert O.rel_err(d.solutions(), xr).max() <= 1e-10
+        if routed:
+            d64 = DeviceRom.from_host(rom.K, rom.M, rom.D, rhs, rom.omega)
+            sweep(h, [d64], precision=_capi.SROM_FP64)
+            assert np.array_equal(d.solutions().view(np.uint64), d64.solutions().view(np.uint64))
+            assert (steps == 0).all() and (d.berr.cpu().numpy() == 0.0).all()
+        else:
+            assert (steps != 0).all()
+    finally:
+        h.close()
 
 
 def test_mixed_precision_workload_near_resonance(handle):
@@ -85,10 +112,10 @@ def test_mixed_nonconvergence_and_fallback(handle):
     M = np.zeros((n, n), dtype=np.complex128)
     rhs = rng.standard_normal((n, 1)) + 0j
     rom = W.Rom(K=K, M=M, D=None, rhs=rhs, omega=np.array([0.0, 0.0]))
-    d0 = _run(handle, rom, rom.omega, flags=0, max_refine=3)
+    d0 = _run(handle, rom, rom.omega, flags=EVERY, max_refine=3)
     assert (d0.info.cpu().numpy() == -1).all()
     assert (d0.steps.cpu().numpy() == 3).all()
-    d1 = _run(handle, rom, rom.omega, flags=FALLBACK, max_refine=3)
+    d1 = _run(handle, rom, rom.omega, flags=FALLBACK | EVERY, max_refine=3)
     assert (d1.steps.cpu().numpy() == -1).all()
     d64 = _run(handle, rom, rom.omega, precision=_capi.SROM_FP64, flags=0)
     assert np.array_equal(d1.solutions().view(np.uint64), d64.solutions().view(np.uint64))
