@@ -33,6 +33,7 @@
 // Reference sequence: src/analysis/KrylovROMSubstructure.cpp:1403-1453 (host, MKL), the
 // cuBLAS batched sweep of test/krylovMidsizeTest/gpu/concurrent/batchedLU/src/main.cu:223-267
 // (no pivoting), the classical stopping rule of iterative refinement on the correction size (Wilkinson; Moler 1967).
+#include <algorithm>
 #include <climits>
 #include <type_traits>
 
@@ -133,6 +134,27 @@ __device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
+// wait_group takes an immediate: a runtime pending count (clamped to 0..15) picks the case.
+__device__ __forceinline__ void cp_async_wait_dyn(int n) {
+    switch (n <= 0 ? 0 : (n > 15 ? 15 : n)) {
+        case 0: cp_async_wait<0>(); break;
+        case 1: cp_async_wait<1>(); break;
+        case 2: cp_async_wait<2>(); break;
+        case 3: cp_async_wait<3>(); break;
+        case 4: cp_async_wait<4>(); break;
+        case 5: cp_async_wait<5>(); break;
+        case 6: cp_async_wait<6>(); break;
+        case 7: cp_async_wait<7>(); break;
+        case 8: cp_async_wait<8>(); break;
+        case 9: cp_async_wait<9>(); break;
+        case 10: cp_async_wait<10>(); break;
+        case 11: cp_async_wait<11>(); break;
+        case 12: cp_async_wait<12>(); break;
+        case 13: cp_async_wait<13>(); break;
+        case 14: cp_async_wait<14>(); break;
+        default: cp_async_wait<15>(); break;
+    }
+}
 
 // One row of the blocked substitution: b[i, c] -= sum_j A[i, j] b[j, c] over the block's
 // columns j (increasing for the forward sweep, decreasing for the backward one), all
@@ -773,13 +795,14 @@ __device__ void trailing_update(T *A, int64_t lda, int n, int j0, int nbc, const
 }
 
 // Shared-memory carve-up of the global-class kernels (bytes from the dynamic base).
+// The u and panel regions come last: during the mixed form's refinement neither is in use, and
+// together with whatever dynamic shared memory lies beyond `total` they form the staging ring
+// of the correction solves (ring = [u, end of the dynamic allocation)).
 struct GlobalSmem {
-    size_t panel, u, work64, work32, perm, ptot, pos, ipiv, moved, dinv, total;
+    size_t work64, work32, perm, ptot, pos, ipiv, moved, dinv, u, panel, total;
     static __host__ __device__ size_t up(size_t b) { return (b + 255) / 256 * 256; }
     __host__ __device__ GlobalSmem(int ldp, int n_max, int r_max) {
-        panel = 0;                                         // ldp x 16 double2 == ldp x 32 float2
-        u = panel + up((size_t)ldp * 256);                 // per warp NB x CWG complex
-        work64 = u + up((size_t)NW * 2048);
+        work64 = 0;
         work32 = work64 + up((size_t)n_max * r_max * 16);
         perm = work32 + up((size_t)n_max * r_max * 8);
         ptot = perm + up((size_t)ldp * 4);
@@ -787,7 +810,9 @@ struct GlobalSmem {
         ipiv = pos + up((size_t)ldp * 4);
         moved = ipiv + up((size_t)ldp * 4);
         dinv = moved + up((size_t)2 * 2 * NB32 * 4);
-        total = dinv + up((size_t)ldp * 16);              // reciprocals of diag(U), mixed form
+        u = dinv + up((size_t)ldp * 16);                  // reciprocals of diag(U), mixed form
+        panel = u + up((size_t)NW * 2048);                // per warp NB x CWG complex
+        total = panel + up((size_t)ldp * 256);            // ldp x 16 double2 == ldp x 32 float2
     }
 };
 
@@ -947,6 +972,118 @@ __device__ void apply_correction(double2 *X, const float2 *B32, int n, int nrhs,
     __syncthreads();
 }
 
+// Correction solve of the mixed form: LU x = b with the complex-FP32 factor in global memory
+// (ld n) and b (n x nrhs, ld n, interchanges applied) in shared memory.  The factor is read
+// strip by strip (SW columns; the forward strips from the first, then the backward ones from
+// the last), each strip through one slot of a ring of ns shared-memory slots, so that up to
+// ns - 1 strips' loads are in flight while one is processed.  Each thread copies the rows it
+// will update itself; the strip's diagonal block, copied by its rows' owners, is read by the
+// triangle after a barrier.  One warp per right-hand side solves the triangle (the backward
+// one multiplies by the reciprocals of U's diagonal), then every thread updates its rows.
+template <int SW, int RPT>
+__device__ void lu_solve_ring(const float2 *A, int n, float2 *B, int nrhs, unsigned char *ring, int ring_bytes,
+                              const float2 *dinv) {
+    using C = CT<float2>;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nblk = (n + SW - 1) / SW;
+    const int slot = SW * n;  // S[j * n + r] = A[r, jb + j]
+    const int ns = min(8, ring_bytes / (slot * 8));
+    float2 *S0 = reinterpret_cast<float2 *>(ring);
+    const int total = 2 * nblk;
+    auto range = [&](int s, int &jb, int &bs) {
+        if (s < nblk) {
+            jb = s * SW;
+            bs = min(SW, n - jb);
+        } else {
+            const int jend = n - (s - nblk) * SW;
+            jb = max(jend - SW, 0);
+            bs = jend - jb;
+        }
+    };
+    auto issue = [&](int s) {
+        if (s < total) {
+            int jb, bs;
+            range(s, jb, bs);
+            const int lo = s < nblk ? jb : 0, hi = s < nblk ? n : jb + bs;
+            float2 *d = S0 + (s % ns) * slot;
+#pragma unroll
+            for (int k = 0; k < RPT; ++k) {
+                const int r = tid + k * NT;
+                if (r >= lo && r < hi)
+                    for (int j = 0; j < bs; ++j) cp_async_elem(d + j * n + r, A + r + (int64_t)(jb + j) * n);
+            }
+        }
+        cp_async_commit();
+    };
+    for (int s = 0; s < ns - 1; ++s) issue(s);
+    for (int s = 0; s < total; ++s) {
+        asm volatile("" ::: "memory");
+        issue(s + ns - 1);
+        cp_async_wait_dyn(ns - 1);
+        __syncthreads();
+        int jb, bs;
+        range(s, jb, bs);
+        const bool fwd = s < nblk;
+        const float2 *S = S0 + (s % ns) * slot;
+        for (int c = warp; c < nrhs; c += NW) {
+            float2 *b = B + (int64_t)c * n + jb;
+            float2 v = lane < bs ? b[lane] : C::zero();
+            if (fwd) {
+                for (int j = 0; j < bs; ++j) {
+                    const float2 bj = C::shfl(v, j, 32);
+                    if (lane > j && lane < bs) v = C::subm(v, S[j * n + jb + lane], bj);
+                }
+            } else {
+                for (int j = bs - 1; j >= 0; --j) {
+                    if (lane == j) v = C::mul(v, dinv[jb + j]);
+                    const float2 bj = C::shfl(v, j, 32);
+                    if (lane < j) v = C::subm(v, S[j * n + jb + lane], bj);
+                }
+            }
+            if (lane < bs) b[lane] = v;
+        }
+        __syncthreads();
+        const int lo = fwd ? jb + bs : 0, hi = fwd ? n : jb;
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+            const int r = tid + k * NT;
+            if (r >= lo && r < hi) {
+                for (int c0 = 0; c0 < nrhs; c0 += 4) {
+                    const int nc = min(4, nrhs - c0);
+                    float2 acc[4];
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) acc[cc] = cc < nc ? B[r + (int64_t)(c0 + cc) * n] : C::zero();
+#pragma unroll
+                    for (int j = 0; j < SW; ++j) {
+                        if (j < bs) {
+                            const float2 a = S[j * n + r];
+#pragma unroll
+                            for (int cc = 0; cc < 4; ++cc)
+                                if (cc < nc) acc[cc] = C::subm(acc[cc], a, B[jb + j + (int64_t)(c0 + cc) * n]);
+                        }
+                    }
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc)
+                        if (cc < nc) B[r + (int64_t)(c0 + cc) * n] = acc[cc];
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+}
+
+// Strip width of the correction solve: 16 columns when the ring holds four such strips of this
+// system, else 8 (more strips in flight for the larger orders).
+template <int RPT>
+__device__ void solve_ring(const float2 *A, int n, float2 *B, int nrhs, unsigned char *ring, int ring_bytes,
+                           const float2 *dinv) {
+    if (ring_bytes >= 4 * 16 * n * (int)sizeof(float2))
+        lu_solve_ring<16, RPT>(A, n, B, nrhs, ring, ring_bytes, dinv);
+    else
+        lu_solve_ring<8, RPT>(A, n, B, nrhs, ring, ring_bytes, dinv);
+}
+
 constexpr int RMAX_MIXED = 16;
 constexpr int SROM_INFO_NOT_CONVERGED_DEV = -1;
 
@@ -973,6 +1110,7 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
     const int tid = threadIdx.x;
     const int n_items = a.n_items_dev ? *a.n_items_dev : a.n_items;
     int *s_ipiv = reinterpret_cast<int *>(sm + L.ipiv);
+
     for (;;) {
         const int it = next_item(a.counter, &s_item);
         if (it >= n_items) break;
@@ -994,6 +1132,8 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
             factor_global<float2, NB32, RPT>(A32, n, n, a.ldp, sm, L, nullptr, 0, PL, Xx, s_pivlg);
             info = PL.info;
             float2 *s_dinv = reinterpret_cast<float2 *>(sm + L.dinv);
+            unsigned char *ring = sm + L.u;  // u, panel and the rest of the allocation
+            const int ring_bytes = a.smem_dyn - (int)L.u;
             for (int l = tid; l < n; l += NT) {
                 s_pos[s_ptot[l]] = l;
                 s_dinv[l] = CT<float2>::recip(A32[l + (int64_t)l * n]);
@@ -1011,7 +1151,7 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
             double prev = 1.0;  // relative size of the previous correction (the first is x itself)
             for (int s = 0;; ++s) {
                 if (s > 0) residual64<RPT>(R, w, X, B32, s_pos);
-                lu_solve_strips<float2, 16>(A32, n, n, B32, n, R.r, reinterpret_cast<float2 *>(sm + L.panel), s_dinv);
+                solve_ring<RPT>(A32, n, B32, R.r, ring, ring_bytes, s_dinv);
                 apply_correction(X, B32, n, R.r, s_dx);
                 if (s > 0) {
                     // error left after this correction ~ rho * ||d||, rho ~ ||d_s|| / ||d_{s-1}||
@@ -1089,10 +1229,27 @@ int fp64_smem_blocks_per_sm(size_t smem) {
     return b;
 }
 
+// The mixed kernel takes all the shared memory a CTA may have (one CTA per SM either way, by
+// registers): what lies beyond its fixed regions deepens the correction solves' staging ring.
 template <bool MIXED, int RPT>
-static cudaError_t launch_global_t(const GlobalArgs &a, int grid, cudaStream_t st) {
+static cudaError_t launch_global_t(const GlobalArgs &a0, int grid, cudaStream_t st) {
     auto k = sweep_global_kernel<MIXED, RPT>;
-    const size_t smem = global_smem_bytes(a.n_max, a.r_max);
+    GlobalArgs a = a0;
+    size_t smem = global_smem_bytes(a.n_max, a.r_max);
+    if (MIXED) {
+        int dev = 0, optin = 0;
+        cudaFuncAttributes fa{};
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k);
+        if (e != cudaSuccess) return e;
+        const size_t cap = (size_t)optin - fa.sharedSizeBytes;
+        if (cap > smem) smem = cap / 256 * 256;
+        // the correction solves' ring must hold two strips of 8 columns of the largest system
+        const size_t ring = smem - GlobalSmem(a.ldp, a.n_max, a.r_max).u;
+        if (ring < 2 * (size_t)8 * a.n_max * sizeof(float2)) return cudaErrorInvalidValue;
+    }
+    a.smem_dyn = (int)smem;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, NT, smem, st>>>(a);

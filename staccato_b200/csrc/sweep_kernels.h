@@ -41,6 +41,7 @@ struct GlobalArgs {
     Item *fb_items;  // mixed: non-converged systems are appended here (null: keep the last iterate)
     int *fb_count;
     int steps_value;  // FP64: value stored in steps (0; -1 when re-solving mixed fallbacks)
+    int smem_dyn;     // dynamic shared memory of the launch (set by launch_global)
 };
 // Global-storage kernel, FP64 (mixed = false) or complex-FP32 factors + FP64 refinement.
 cudaError_t launch_global(bool mixed, const GlobalArgs &a, int grid, cudaStream_t st);
