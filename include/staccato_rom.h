@@ -58,7 +58,9 @@ typedef struct {
                               SROM_ERR_UNSUPPORTED for it                                       */
 
 /* ---- sweep flags ---------------------------------------------------------------------- */
-#define SROM_FLAG_FALLBACK_FP64 1 /* re-solve non-converged frequencies with the FP64 kernel */
+#define SROM_FLAG_FALLBACK_FP64 1 /* re-solve non-converged frequencies in FP64 (steps = -1);
+                                     with it, refinement stops early once the measured
+                                     contraction shows tol cannot be reached in max_refine */
 #define SROM_FLAG_KEEP_FACTORS 2  /* write LU factors + pivots into desc.LU / desc.ipiv (FP64) */
 #define SROM_FLAG_MIXED_EVERY 4   /* mixed forms: factor every system in FP32.  Without it, systems
                                      small enough for two FP64 shared-memory factorisations per SM

@@ -1073,15 +1073,13 @@ __device__ void lu_solve_ring(const float2 *A, int n, float2 *B, int nrhs, unsig
     __syncthreads();
 }
 
-// Strip width of the correction solve: 16 columns when the ring holds four such strips of this
-// system, else 8 (more strips in flight for the larger orders).
+// Strips of 16 columns: the ring (at least the u and panel regions, 16 KB + 256 ldp bytes)
+// always holds two of them; with fewer, wider strips the triangles and barriers cost less than
+// narrower strips gain in depth (measured at n = 128..512).
 template <int RPT>
 __device__ void solve_ring(const float2 *A, int n, float2 *B, int nrhs, unsigned char *ring, int ring_bytes,
                            const float2 *dinv) {
-    if (ring_bytes >= 4 * 16 * n * (int)sizeof(float2))
-        lu_solve_ring<16, RPT>(A, n, B, nrhs, ring, ring_bytes, dinv);
-    else
-        lu_solve_ring<8, RPT>(A, n, B, nrhs, ring, ring_bytes, dinv);
+    lu_solve_ring<16, RPT>(A, n, B, nrhs, ring, ring_bytes, dinv);
 }
 
 constexpr int RMAX_MIXED = 16;
@@ -1147,7 +1145,7 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
             }
             __syncthreads();
             const double tol_x = a.tol > 0.0 ? a.tol : 5.820766091346741e-11;  // 2^-34
-            bool conv = false;
+            bool conv = false, hopeless = false;
             double prev = 1.0;  // relative size of the previous correction (the first is x itself)
             for (int s = 0;; ++s) {
                 if (s > 0) residual64<RPT>(R, w, X, B32, s_pos);
@@ -1158,13 +1156,22 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
                     // (the contraction of the iteration), taken twice for safety
                     double worst = 0.0;
                     for (int c = 0; c < R.r; ++c) worst = fmax(worst, s_dx[c]);
-                    const double rho = fmin(1.0, 2.0 * worst / prev);
+                    const double ratio = worst / prev;
+                    const double rho = fmin(1.0, 2.0 * ratio);
                     berr = worst * rho;
                     conv = berr <= tol_x;
                     prev = worst;
+                    // With the FP64 fallback on, stop as soon as even the measured contraction
+                    // (no safety factor) cannot reach tol in the steps left: those corrections
+                    // would be discarded by the re-solve anyway.
+                    if (!conv && a.fb_items && s >= 2 && s < a.max_refine) {
+                        double pred = worst * ratio;
+                        for (int k = s; k < a.max_refine && pred > tol_x; ++k) pred *= ratio;
+                        hopeless = ratio >= 1.0 || pred > tol_x;
+                    }
                 }
                 steps = s;
-                if (conv || s >= a.max_refine) break;
+                if (conv || hopeless || s >= a.max_refine) break;
             }
             if (!conv && a.fb_items) {
                 // re-solved by the FP64 kernel that runs after this one; it writes X and status
@@ -1245,9 +1252,9 @@ static cudaError_t launch_global_t(const GlobalArgs &a0, int grid, cudaStream_t 
         if (e != cudaSuccess) return e;
         const size_t cap = (size_t)optin - fa.sharedSizeBytes;
         if (cap > smem) smem = cap / 256 * 256;
-        // the correction solves' ring must hold two strips of 8 columns of the largest system
+        // the correction solves' ring must hold two strips of 16 columns of the largest system
         const size_t ring = smem - GlobalSmem(a.ldp, a.n_max, a.r_max).u;
-        if (ring < 2 * (size_t)8 * a.n_max * sizeof(float2)) return cudaErrorInvalidValue;
+        if (ring < 2 * (size_t)16 * a.n_max * sizeof(float2)) return cudaErrorInvalidValue;
     }
     a.smem_dyn = (int)smem;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
