@@ -120,7 +120,7 @@ class ClockSampler:
 # workload (the 64-ROM batching draw of rank 0), from a one-pass ncu capture of
 # dram__bytes_read.sum + dram__bytes_write.sum over
 # `bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-e2e --no-extras` (mean of 4 launches).
-MEASURED_TRAFFIC = {"mixed_global": 571.6e9 + 454.7e9, "fp64_global": 1742.5e9 + 1799.0e9}
+MEASURED_TRAFFIC = {"mixed_global": 574.5e9 + 460.1e9, "fp64_global": 1757.4e9 + 1803.5e9}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, one-pass capture of this "
                   "workload with the current kernels; compare with the bytes the matrices alone need "
                   "(8 n^2 B per FP32 system, 16 n^2 B per FP64 system)")
@@ -544,7 +544,7 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "systems_per_gpu": systems,
                        "tflop_per_step_per_gpu": flops / 1e12, "precision": headline,
-                       "refine": "complex-FP32 LU, FP64 residuals, <=5 corrections, stop when the predicted error rho*||d||/||x|| <= 2^-34, back substitution by reciprocals of diag(U), FP64 fallback",
+                       "refine": "complex-FP32 LU, FP64 residuals, <=5 corrections, stop when the predicted error rho*||d||/||x|| <= 2^-34 (or early once the measured contraction cannot reach it), correction solves streamed through a shared-memory strip ring, back substitution by reciprocals of diag(U), FP64 fallback; systems with n <= ~84 solved by the FP64 smem kernel",
                        "l2": "inputs 167 MB + outputs 1.6 GB per step exceed L2; no flush",
                        "parallelism": f"independent batch per GPU x{world} (seed 3 + 1000003*rank)"},
             "roofline": info.get("roofline"),
