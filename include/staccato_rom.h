@@ -237,6 +237,36 @@ SROM_API int srom_project_complex(srom_handle *h, int64_t n_rows, int64_t nnz, c
 SROM_API int srom_orthonormalize(srom_handle *h, double *V, int64_t n_rows, int k, int64_t ldv, int passes);
 
 /*
+ * Krylov basis of a substructure, KrylovROMSubstructure::addKrylovModesForExpansionPoint
+ * (src/analysis/KrylovROMSubstructure.cpp:367-569).  For every expansion point f0 (Hz,
+ * w0 = 2 pi f0): K~ = -(K - w0^2 M + i w0 D) is factored on the GPU (band LDL^T after a
+ * reverse Cuthill-McKee ordering, no pivoting: K~ must be complex symmetric and its leading
+ * blocks nonsingular), Q = K~^-1 B (then, from the second point on, re-orthogonalised against
+ * the basis so far), and krylov_order - 1 times Q = K~^-1 (M Q) re-orthogonalised; each block
+ * is reduced by a column-pivoted QR to its leading columns with |R_ii| > tol (absolute, as in
+ * the reference; tol <= 0 means its 1e-8) and appended to V.
+ *   rowptr/colind: CSR pattern shared by K, M, D (device; base 0 or 1; upper = 1 for the
+ *   upper triangle of the symmetric matrix, 0 for the full symmetric pattern).  K, M, D
+ *   (nullable): device values.  B: device n_rows x n_in, ldb.  exp_points_hz: HOST array.
+ *   V: device n_rows x max_cols (ldv); *n_cols (host) receives the number of columns written.
+ * Device memory: the band, (n_rows + 128) x (bandwidth + 129) x 16 bytes (srom_band_order
+ * reports it), plus a few n_rows x n_in blocks.  Synchronises the handle's stream.
+ */
+SROM_API int srom_krylov_basis(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind,
+                               int base, int upper, const srom_complex *K, const srom_complex *M, const srom_complex *D,
+                               const srom_complex *B, int n_in, int64_t ldb, const double *exp_points_hz, int n_points,
+                               int krylov_order, double tol, srom_complex *V, int64_t ldv, int max_cols, int *n_cols);
+
+/*
+ * Host-only: the reverse Cuthill-McKee ordering srom_krylov_basis uses for a pattern (HOST
+ * rowptr/colind, as above).  perm (n_rows ints, may be NULL): perm[k] = original row of row k;
+ * *bandwidth = max |new i - new j| over the entries; *band_bytes = device bytes of the band
+ * factor.  err (may be NULL) receives a message on failure.
+ */
+SROM_API int srom_band_order(int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind, int base, int upper,
+                             int *perm, int64_t *bandwidth, int64_t *band_bytes, char *err, int err_len);
+
+/*
  * FP64 sweep of one ROM that allocates no device memory.  No counterpart in the reference.
  * For callers that cannot let a library allocate: programs that own all device memory
  * through their own pool, or real-time loops in which cudaMalloc's implicit synchronisation

@@ -37,6 +37,7 @@ EXPORTS = [
     "srom_sweep_backward",
     "srom_graph_create", "srom_graph_launch", "srom_graph_destroy", "srom_tune",
     "srom_mtx_read_dense", "srom_mtx_write_dense", "srom_write_solution",
+    "srom_krylov_basis", "srom_band_order",
 ]
 
 SROM_DPARAM_LOWRANK = 0
@@ -113,6 +114,12 @@ def lib() -> C.CDLL:
         L.srom_project_complex.argtypes = [vp, C.c_int64, C.c_int64, vp, vp, i, i, C.POINTER(C.c_void_p), i, vp, i,
                                            C.c_int64, vp, C.c_int64, C.POINTER(C.c_void_p)]
         L.srom_project_complex.restype = i
+        L.srom_krylov_basis.argtypes = [vp, C.c_int64, C.c_int64, vp, vp, i, i, vp, vp, vp, vp, i, C.c_int64, vp, i, i,
+                                        C.c_double, vp, C.c_int64, i, C.POINTER(i)]
+        L.srom_krylov_basis.restype = i
+        L.srom_band_order.argtypes = [C.c_int64, C.c_int64, vp, vp, i, i, vp, C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_int64), C.c_char_p, i]
+        L.srom_band_order.restype = i
         L.srom_orthonormalize.argtypes = [vp, vp, C.c_int64, i, C.c_int64, i]
         L.srom_orthonormalize.restype = i
         L.srom_graph_create.argtypes = [vp, C.POINTER(RomDesc), i, C.POINTER(SweepOpts), pp]

@@ -4,6 +4,7 @@
 // cost-sorted list of (ROM, frequency) systems, staging that list to the device, sizing
 // scratch memory and launching the persistent kernels on the handle's stream.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -14,6 +15,7 @@
 #include "../../include/staccato_rom.h"
 #include "srom_device.cuh"
 #include "adjoint_kernels.h"
+#include "krylov_kernels.h"
 #include "project_kernels.h"
 #include "sweep_kernels.h"
 
@@ -869,6 +871,83 @@ int srom_sweep_backward(srom_handle *h, const srom_rom_desc *rom, const srom_com
     const double n3 = (double)rom->n * rom->n;
     ProfScope ps(h, "adjoint", rom->F, (8.0 * n3 * rom->r) * rom->F, 0.0);
     SROM_CUDA(h, srom::launch_adjoint(a, rom->n, rom->r, rom->F, grid, dJdp, h->stream));
+    return SROM_OK;
+}
+
+int srom_krylov_basis(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind, int base,
+                      int upper, const srom_complex *K, const srom_complex *M, const srom_complex *D,
+                      const srom_complex *B, int n_in, int64_t ldb, const double *exp_points_hz, int n_points,
+                      int krylov_order, double tol, srom_complex *V, int64_t ldv, int max_cols, int *n_cols) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    if (!n_cols) return set_err(h, SROM_ERR_INVALID, "n_cols is null");
+    *n_cols = 0;
+    if (n_rows < 0 || nnz < 0 || n_in < 0 || n_points < 0 || max_cols < 0)
+        return set_err(h, SROM_ERR_INVALID, "negative size");
+    if (n_rows > INT32_MAX - 1) return set_err(h, SROM_ERR_UNSUPPORTED, "n_rows above 2^31 - 2");
+    if (base != 0 && base != 1) return set_err(h, SROM_ERR_INVALID, "base must be 0 or 1");
+    if (krylov_order < 1) return set_err(h, SROM_ERR_INVALID, "krylov_order must be >= 1");
+    if (n_rows == 0 || n_in == 0 || n_points == 0) return SROM_OK;
+    if (!rowptr || !colind || !K || !M || !B || !V || !exp_points_hz)
+        return set_err(h, SROM_ERR_INVALID, "rowptr, colind, K, M, B, V and exp_points_hz must be non-null");
+    if (ldb < n_rows || ldv < n_rows) return set_err(h, SROM_ERR_INVALID, "ldb and ldv must be >= n_rows");
+    if (n_rows * (int64_t)n_in > INT32_MAX) return set_err(h, SROM_ERR_UNSUPPORTED, "n_rows * n_in above 2^31 - 1");
+    if (srom::misaligned(K, 16) || srom::misaligned(M, 16) || srom::misaligned(D, 16) || srom::misaligned(B, 16) ||
+        srom::misaligned(V, 16) || srom::misaligned(rowptr, 8) || srom::misaligned(colind, 4))
+        return set_err(h, SROM_ERR_INVALID, "complex arrays must be 16-byte aligned (rowptr 8, colind 4)");
+    for (int i = 0; i < n_points; ++i)
+        if (!std::isfinite(exp_points_hz[i])) return set_err(h, SROM_ERR_INVALID, "expansion point %d is not finite", i);
+    DeviceGuard g(h->device);
+    srom::kry::KrylovArgs a{};
+    a.stream = h->stream;
+    a.n_rows = n_rows;
+    a.nnz = nnz;
+    a.rowptr = rowptr;
+    a.colind = colind;
+    a.base = base;
+    a.upper = upper ? 1 : 0;
+    a.K = K;
+    a.M = M;
+    a.D = D;
+    a.B = B;
+    a.n_in = n_in;
+    a.ldb = ldb;
+    a.exp_points_hz = exp_points_hz;
+    a.n_points = n_points;
+    a.order = krylov_order;
+    a.tol = tol > 0.0 ? tol : 1e-8;
+    a.V = V;
+    a.ldv = ldv;
+    a.max_cols = max_cols;
+    std::string msg;
+    ProfScope ps(h, "krylov_basis", n_points, 0.0, 0.0);
+    const int s = srom::kry::krylov_basis(a, &msg, n_cols, nullptr);
+    if (s) return set_err(h, s, "%s", msg.c_str());
+    return SROM_OK;
+}
+
+int srom_band_order(int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind, int base, int upper,
+                    int *perm, int64_t *bandwidth, int64_t *band_bytes_out, char *err, int err_len) {
+    auto fail = [&](int code, const std::string &m) {
+        if (err && err_len > 0) snprintf(err, (size_t)err_len, "%s", m.c_str());
+        return code;
+    };
+    if (err && err_len > 0) err[0] = 0;
+    if (n_rows < 0 || nnz < 0) return fail(SROM_ERR_INVALID, "negative size");
+    if (n_rows > INT32_MAX - 1) return fail(SROM_ERR_UNSUPPORTED, "n_rows above 2^31 - 2");
+    if (base != 0 && base != 1) return fail(SROM_ERR_INVALID, "base must be 0 or 1");
+    if (n_rows > 0 && (!rowptr || (nnz > 0 && !colind))) return fail(SROM_ERR_INVALID, "rowptr and colind must be non-null");
+    if (n_rows > 0 && (rowptr[0] != base || rowptr[n_rows] - base != nnz))
+        return fail(SROM_ERR_INVALID, "rowptr does not start at base or does not end at base + nnz");
+    std::vector<int64_t> frp, fmap;
+    std::vector<int> fci, p;
+    std::string m;
+    int s = srom::kry::full_pattern(n_rows, nnz, rowptr, colind, base, upper, frp, fci, fmap, &m);
+    if (s) return fail(s, m);
+    const int64_t bw = srom::kry::rcm_order(n_rows, frp, fci, p);
+    if (perm) std::copy(p.begin(), p.end(), perm);
+    if (bandwidth) *bandwidth = bw;
+    if (band_bytes_out) *band_bytes_out = srom::kry::band_bytes(n_rows, bw);
     return SROM_OK;
 }
 

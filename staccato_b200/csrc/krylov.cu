@@ -1,0 +1,848 @@
+// Krylov basis generation on the GPU: the block Arnoldi process with block Gram-Schmidt
+// re-orthogonalisation and rank-revealing deflation of
+// KrylovROMSubstructure::addKrylovModesForExpansionPoint (src/analysis/KrylovROMSubstructure.cpp:367-569).
+//
+// Per expansion point f0 (w0 = 2 pi f0) the reference factors K~ = -(K - w0^2 M + i w0 D) with
+// PARDISO (:387-406, :571-707).  Here K~ is factored directly on the GPU as a band matrix:
+//
+//  * ordering  -- reverse Cuthill-McKee on the host (once per pattern) to shrink the bandwidth bw;
+//  * storage   -- the lower band, column j holding rows j-NB .. j+bw+NB at band[j*ldab + i-j+NB]
+//                 (NB rows of headroom above the diagonal), so that every dense sub-block of the
+//                 band is a column-major matrix with leading dimension ldab-1;
+//  * factor    -- blocked LDL^T without pivoting (K~ is complex symmetric), NB columns a step:
+//                 the NB x NB diagonal block in one CTA, the panel L21 = A21 L11^-T D^-1 by one
+//                 warp a row, and the trailing update A22 -= (L21 D) L21^T as one strided-batched
+//                 ZGEMM (cuBLAS) over the column blocks of the window;
+//  * solves    -- blocked forward / diagonal / backward substitution for all right-hand sides.
+//
+// The rest of the process runs on the GPU as in the reference: M Q by a complex CSR SpMM, the
+// re-orthogonalisation Q <- Q - V (V^H Q) with ZGEMMs until the norm ratio exceeds 1/sqrt(2),
+// and the column-pivoted Householder QR (the steps of zgeqp3 with exact partial column norms)
+// whose leading |R_ii| > tol decide the rank, Q formed from the reflectors (zungqr).
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/staccato_rom.h"
+#include "krylov_kernels.h"
+
+namespace srom {
+namespace kry {
+
+constexpr int NB = 64;   // columns per elimination step (and rows of band headroom)
+constexpr int KT = 256;  // threads per CTA
+constexpr int SLD = NB + 1;
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// c - a b
+__device__ __forceinline__ double2 cfms(double2 c, double2 a, double2 b) {
+    return make_double2(fma(-a.x, b.x, fma(a.y, b.y, c.x)), fma(-a.x, b.y, fma(-a.y, b.x, c.y)));
+}
+// a / b by Smith's method
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+    if (fabs(b.x) >= fabs(b.y)) {
+        const double r = b.y / b.x, den = b.x + b.y * r;
+        return make_double2((a.x + a.y * r) / den, (a.y - a.x * r) / den);
+    }
+    const double r = b.x / b.y, den = b.y + b.x * r;
+    return make_double2((a.x * r + a.y) / den, (a.y * r - a.x) / den);
+}
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+    return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// ---- K~ into band storage -----------------------------------------------------------------
+// Full symmetric pattern (0-based, rows of the original numbering); vmap[e] indexes the caller's
+// value arrays.  Entry (i, j) lands at (pi, pj) = (iperm[i], iperm[j]) when pi >= pj, so every
+// unordered pair is written once.  Value -(K - w^2 M + i w D).  One warp per row.
+__global__ void scatter_band_kernel(int64_t n, const int64_t *__restrict__ rp, const int *__restrict__ ci,
+                                    const int64_t *__restrict__ vmap, const double2 *__restrict__ K,
+                                    const double2 *__restrict__ M, const double2 *__restrict__ D, double w,
+                                    const int *__restrict__ iperm, double2 *__restrict__ band, int64_t ldab) {
+    const int lane = threadIdx.x & 31;
+    const double w2 = w * w;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n;
+         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int pi = iperm[i];
+        for (int64_t e = rp[i] + lane; e < rp[i + 1]; e += 32) {
+            const int pj = iperm[ci[e]];
+            if (pi < pj) continue;
+            const int64_t v = vmap[e];
+            const double2 k = K[v], m = M[v];
+            double re = k.x - w2 * m.x, im = k.y - w2 * m.y;
+            if (D) {
+                const double2 d = D[v];
+                re -= w * d.y;
+                im += w * d.x;
+            }
+            band[(int64_t)pj * ldab + (pi - pj + NB)] = make_double2(-re, -im);
+        }
+    }
+}
+
+// ---- blocked LDL^T ------------------------------------------------------------------------
+// The nb x nb diagonal block at column j0: A11 = L11 D L11^T (unit L11, no pivoting), in place
+// (D on the diagonal).  The first exactly-zero pivot is recorded 1-based in *info.
+__global__ void __launch_bounds__(KT) ldlt_diag_kernel(double2 *__restrict__ band, int64_t ldab, int64_t j0, int nb,
+                                                       int *__restrict__ info) {
+    extern __shared__ double2 S[];  // S[i * SLD + j], i >= j
+    const int t = threadIdx.x;
+    for (int e = t; e < nb * nb; e += KT) {
+        const int i = e % nb, j = e / nb;
+        if (i >= j) S[i * SLD + j] = band[(j0 + j) * ldab + (i - j + NB)];
+    }
+    __syncthreads();
+    for (int k = 0; k < nb; ++k) {
+        const double2 d = S[k * SLD + k];
+        if (t == 0 && d.x == 0.0 && d.y == 0.0) atomicCAS(info, 0, (int)(j0 + k + 1));
+        for (int i = k + 1 + t; i < nb; i += KT) S[i * SLD + k] = cdiv(S[i * SLD + k], d);
+        __syncthreads();
+        const int m = nb - k - 1;
+        for (int e = t; e < m * m; e += KT) {
+            const int i = k + 1 + e % m, j = k + 1 + e / m;
+            if (i >= j) S[i * SLD + j] = cfms(S[i * SLD + j], cmul(S[i * SLD + k], d), S[j * SLD + k]);
+        }
+        __syncthreads();
+    }
+    for (int e = t; e < nb * nb; e += KT) {
+        const int i = e % nb, j = e / nb;
+        if (i >= j) band[(j0 + j) * ldab + (i - j + NB)] = S[i * SLD + j];
+    }
+}
+
+// Loads the factored diagonal block (L11 below, D on the diagonal) into shared memory.
+__device__ __forceinline__ void load_l11(const double2 *band, int64_t ldab, int64_t j0, int nb, double2 *S) {
+    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+        const int i = e % nb, j = e / nb;
+        if (i >= j) S[i * SLD + j] = band[(j0 + j) * ldab + (i - j + NB)];
+    }
+    __syncthreads();
+}
+
+// Panel rows t in [0, rows) (matrix rows j0+nb+t): x L11^T = a, L21 = x D^-1; x goes to W
+// (= L21 D) and L21 to Lp and to the band.  Rows [rows, zero_to) of W and Lp are zeroed (the
+// strided-batched update reads up to NB * (batches - 1) + rows rows).  One warp a row, lane l
+// holding columns l and l + 32.
+__global__ void __launch_bounds__(KT) ldlt_panel_kernel(double2 *__restrict__ band, int64_t ldab, int64_t j0, int nb,
+                                                        int rows, int zero_to, double2 *__restrict__ W,
+                                                        double2 *__restrict__ Lp, int ldw) {
+    extern __shared__ double2 S[];
+    load_l11(band, ldab, j0, nb, S);
+    const int lane = threadIdx.x & 31;
+    const int t = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    if (t >= zero_to) return;
+    if (t >= rows) {
+        for (int k = lane; k < NB; k += 32) {
+            W[t + (int64_t)k * ldw] = make_double2(0.0, 0.0);
+            Lp[t + (int64_t)k * ldw] = make_double2(0.0, 0.0);
+        }
+        return;
+    }
+    const int64_t r = j0 + nb + t;
+    double2 x[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int k = lane + 32 * h;
+        x[h] = k < nb ? band[(j0 + k) * ldab + (r - (j0 + k) + NB)] : make_double2(0.0, 0.0);
+    }
+    for (int m = 0; m < nb; ++m) {
+        const double2 xm = m < 32 ? shfl2(x[0], m) : shfl2(x[1], m - 32);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int k = lane + 32 * h;
+            if (k > m && k < nb) x[h] = cfms(x[h], S[k * SLD + m], xm);
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int k = lane + 32 * h;
+        if (k < NB) {
+            double2 l = make_double2(0.0, 0.0), wv = make_double2(0.0, 0.0);
+            if (k < nb) {
+                wv = x[h];
+                l = cdiv(x[h], S[k * SLD + k]);
+                band[(j0 + k) * ldab + (r - (j0 + k) + NB)] = l;
+            }
+            W[t + (int64_t)k * ldw] = wv;
+            Lp[t + (int64_t)k * ldw] = l;
+        }
+    }
+}
+
+// Triangular solves with the unit L11 of block j0 for all right-hand sides (X rows j0..j0+nb):
+// forward (trans = 0) L11 y = x, backward (trans = 1) L11^T y = x.  One warp a right-hand side.
+__global__ void __launch_bounds__(KT) trsv_block_kernel(const double2 *__restrict__ band, int64_t ldab, int64_t j0,
+                                                        int nb, double2 *__restrict__ X, int64_t ldx, int nrhs,
+                                                        int trans) {
+    extern __shared__ double2 S[];
+    load_l11(band, ldab, j0, nb, S);
+    const int lane = threadIdx.x & 31;
+    for (int c = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5); c < nrhs;
+         c += (int)(((int64_t)gridDim.x * blockDim.x) >> 5)) {
+        double2 *x = X + (int64_t)c * ldx + j0;
+        double2 v[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int k = lane + 32 * h;
+            v[h] = k < nb ? x[k] : make_double2(0.0, 0.0);
+        }
+        if (!trans) {
+            for (int m = 0; m < nb; ++m) {
+                const double2 vm = m < 32 ? shfl2(v[0], m) : shfl2(v[1], m - 32);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = lane + 32 * h;
+                    if (k > m && k < nb) v[h] = cfms(v[h], S[k * SLD + m], vm);
+                }
+            }
+        } else {
+            for (int m = nb - 1; m >= 0; --m) {
+                const double2 vm = m < 32 ? shfl2(v[0], m) : shfl2(v[1], m - 32);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = lane + 32 * h;
+                    if (k < m) v[h] = cfms(v[h], S[m * SLD + k], vm);
+                }
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int k = lane + 32 * h;
+            if (k < nb) x[k] = v[h];
+        }
+    }
+}
+
+// X[i, c] /= D_i (the diagonal of the factored band).
+__global__ void diag_scale_kernel(const double2 *__restrict__ band, int64_t ldab, int64_t n, double2 *__restrict__ X,
+                                  int64_t ldx, int nrhs) {
+    const int64_t total = n * nrhs;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, c = e / n;
+        X[i + c * ldx] = cdiv(X[i + c * ldx], band[i * ldab + NB]);
+    }
+}
+
+// dst[iperm[i], c] = src[i, c] (to = 1) or dst[i, c] = src[iperm[i], c] (to = 0).
+__global__ void permute_kernel(int64_t n, int nrhs, const int *__restrict__ iperm, const double2 *__restrict__ src,
+                               int64_t lds, double2 *__restrict__ dst, int64_t ldd, int to) {
+    const int64_t total = n * nrhs;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, c = e / n;
+        if (to)
+            dst[iperm[i] + c * ldd] = src[i + c * lds];
+        else
+            dst[i + c * ldd] = src[iperm[i] + c * lds];
+    }
+}
+
+// Y = A Q for the full pattern with values A[vmap[e]]; one warp a row, lanes over its entries.
+__global__ void csr_spmm_complex_kernel(int64_t n, const int64_t *__restrict__ rp, const int *__restrict__ ci,
+                                        const int64_t *__restrict__ vmap, const double2 *__restrict__ A,
+                                        const double2 *__restrict__ Q, int64_t ldq, int k, double2 *__restrict__ Y,
+                                        int64_t ldy) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n;
+         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        for (int c = 0; c < k; ++c) {
+            double2 acc = make_double2(0.0, 0.0);
+            for (int64_t e = rp[i] + lane; e < rp[i + 1]; e += 32) {
+                const double2 a = A[vmap[e]], q = Q[ci[e] + (int64_t)c * ldq];
+                acc.x = fma(a.x, q.x, fma(-a.y, q.y, acc.x));
+                acc.y = fma(a.x, q.y, fma(a.y, q.x, acc.y));
+            }
+#pragma unroll
+            for (int off = 16; off; off >>= 1) {
+                acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+                acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+            }
+            if (lane == 0) Y[i + (int64_t)c * ldy] = acc;
+        }
+    }
+}
+
+// ---- column-pivoted Householder QR pieces (one CTA a column) -------------------------------
+__device__ __forceinline__ double block_sum(double v, double *red) {
+    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    v = threadIdx.x < (KT >> 5) ? red[threadIdx.x] : 0.0;
+    if (w == 0)
+        for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// out[j - j0] = sum_{i >= r0} |A[i, j]|^2 for j in [j0, j0 + count)
+__global__ void __launch_bounds__(KT) col_norm2_kernel(const double2 *__restrict__ A, int64_t lda, int64_t n, int64_t r0,
+                                                       int j0, double *__restrict__ out) {
+    __shared__ double red[KT / 32];
+    const int j = j0 + blockIdx.x;
+    double s = 0.0;
+    for (int64_t i = r0 + threadIdx.x; i < n; i += KT) {
+        const double2 a = A[i + (int64_t)j * lda];
+        s = fma(a.x, a.x, fma(a.y, a.y, s));
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+__global__ void swap_cols_kernel(double2 *__restrict__ A, int64_t lda, int64_t n, int a, int b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 t = A[i + (int64_t)a * lda];
+        A[i + (int64_t)a * lda] = A[i + (int64_t)b * lda];
+        A[i + (int64_t)b * lda] = t;
+    }
+}
+
+// Column k of A becomes the Householder vector (v_k = 1 implicit, A[k, k] = beta): rows > k
+// scaled by s.
+__global__ void householder_scale_kernel(double2 *__restrict__ A, int64_t lda, int64_t n, int k, double2 s,
+                                         double beta) {
+    double2 *a = A + (int64_t)k * lda;
+    for (int64_t i = k + 1 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = cmul(a[i], s);
+    if (blockIdx.x == 0 && threadIdx.x == 0) a[k] = make_double2(beta, 0.0);
+}
+
+// w[j - j0] = v^H T[k:, j] with v = (1, V[k+1:, vk]) for j in [j0, j0 + count)
+__global__ void __launch_bounds__(KT) reflector_dots_kernel(const double2 *__restrict__ Vr, int64_t ldv, int vk,
+                                                            const double2 *__restrict__ T, int64_t ldt, int64_t n,
+                                                            int64_t k, int j0, double2 *__restrict__ w) {
+    __shared__ double red[KT / 32];
+    const int j = j0 + blockIdx.x;
+    const double2 *v = Vr + (int64_t)vk * ldv;
+    const double2 *t = T + (int64_t)j * ldt;
+    double sr = 0.0, si = 0.0;
+    for (int64_t i = k + threadIdx.x; i < n; i += KT) {
+        const double2 vi = i == k ? make_double2(1.0, 0.0) : v[i];
+        const double2 ti = t[i];
+        sr = fma(vi.x, ti.x, fma(vi.y, ti.y, sr));  // conj(v) t
+        si = fma(vi.x, ti.y, fma(-vi.y, ti.x, si));
+    }
+    sr = block_sum(sr, red);
+    si = block_sum(si, red);
+    if (threadIdx.x == 0) w[blockIdx.x] = make_double2(sr, si);
+}
+
+// T[i, j] -= tau v_i w_j for i >= k, j in [j0, j0 + count)
+__global__ void reflector_apply_kernel(const double2 *__restrict__ Vr, int64_t ldv, int vk, double2 *__restrict__ T,
+                                       int64_t ldt, int64_t n, int64_t k, int j0, int count,
+                                       const double2 *__restrict__ w, double2 tau) {
+    const double2 *v = Vr + (int64_t)vk * ldv;
+    const int64_t rows = n - k, total = rows * count;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = k + e % rows;
+        const int j = j0 + (int)(e / rows);
+        const double2 vi = i == k ? make_double2(1.0, 0.0) : v[i];
+        T[i + (int64_t)j * ldt] = cfms(T[i + (int64_t)j * ldt], cmul(tau, vi), w[j - j0]);
+    }
+}
+
+// Column i of Q from reflector i (zung2r): Q[r, i] = -tau v_r (r > i), 1 - tau (r = i), 0 (r < i).
+__global__ void reflector_column_kernel(const double2 *__restrict__ Vr, int64_t ldv, int vi, double2 *__restrict__ Q,
+                                        int64_t ldq, int64_t n, int i, double2 tau) {
+    const double2 *v = Vr + (int64_t)vi * ldv;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        double2 q;
+        if (r < i)
+            q = make_double2(0.0, 0.0);
+        else if (r == i)
+            q = make_double2(1.0 - tau.x, -tau.y);
+        else
+            q = make_double2(-(tau.x * v[r].x - tau.y * v[r].y), -(tau.x * v[r].y + tau.y * v[r].x));
+        Q[r + (int64_t)i * ldq] = q;
+    }
+}
+
+// ==================================================================================================
+// host side
+// ==================================================================================================
+namespace {
+
+struct Err {
+    int code = SROM_OK;
+    std::string msg;
+    int set(int c, const std::string &m) {
+        if (code == SROM_OK) {
+            code = c;
+            msg = m;
+        }
+        return c;
+    }
+};
+
+#define KCU(call)                                                                           \
+    do {                                                                                    \
+        cudaError_t _e = (call);                                                            \
+        if (_e != cudaSuccess) return E.set(SROM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+#define KBL(call)                                                                               \
+    do {                                                                                        \
+        cublasStatus_t _s = (call);                                                             \
+        if (_s != CUBLAS_STATUS_SUCCESS) return E.set(SROM_ERR_CUDA, std::string(#call) + " failed (cuBLAS status " + std::to_string((int)_s) + ")"); \
+    } while (0)
+
+// Device buffers freed at scope exit (after the stream has drained).
+struct Bufs {
+    cudaStream_t st = nullptr;
+    std::vector<void *> ptrs;
+    ~Bufs() {
+        if (st) cudaStreamSynchronize(st);
+        for (void *p : ptrs) cudaFree(p);
+    }
+    template <typename T>
+    cudaError_t alloc(T **p, size_t count) {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) ptrs.push_back(q);
+        *p = static_cast<T *>(q);
+        return e;
+    }
+};
+
+int grid_for(int64_t work, int threads) {
+    const int64_t b = (work + threads - 1) / threads;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
+}
+
+}  // namespace
+
+// Full symmetric pattern of a CSR matrix given in full or upper storage (base 0 or 1), with the
+// index of each entry's value in the caller's arrays.
+int full_pattern(int64_t n, int64_t nnz, const int64_t *rp, const int *ci, int base, int upper, std::vector<int64_t> &frp,
+                 std::vector<int> &fci, std::vector<int64_t> &fmap, std::string *err) {
+    frp.assign(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) {
+        for (int64_t e = rp[i] - base; e < rp[i + 1] - base; ++e) {
+            const int64_t j = (int64_t)ci[e] - base;
+            if (j < 0 || j >= n) {
+                if (err) *err = "column index out of range in row " + std::to_string(i);
+                return SROM_ERR_INVALID;
+            }
+            if (upper && j < i) {
+                if (err) *err = "upper storage holds an entry below the diagonal in row " + std::to_string(i);
+                return SROM_ERR_INVALID;
+            }
+            frp[i + 1]++;
+            if (upper && j != i) frp[j + 1]++;
+        }
+    }
+    for (int64_t i = 0; i < n; ++i) frp[i + 1] += frp[i];
+    fci.assign(frp[n], 0);
+    fmap.assign(frp[n], 0);
+    std::vector<int64_t> pos(frp.begin(), frp.end() - 1);
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t e = rp[i] - base; e < rp[i + 1] - base; ++e) {
+            const int64_t j = (int64_t)ci[e] - base;
+            fci[pos[i]] = (int)j;
+            fmap[pos[i]++] = e;
+            if (upper && j != i) {
+                fci[pos[j]] = (int)i;
+                fmap[pos[j]++] = e;
+            }
+        }
+    (void)nnz;
+    return SROM_OK;
+}
+
+// Reverse Cuthill-McKee on the full pattern: perm[k] = old index of new row k; each connected
+// component starts from a pseudo-peripheral node (George & Liu), neighbours visited by increasing
+// degree.  Returns the bandwidth max |iperm[i] - iperm[j]| over the entries.
+int64_t rcm_order(int64_t n, const std::vector<int64_t> &frp, const std::vector<int> &fci, std::vector<int> &perm) {
+    std::vector<int> deg(n), level(n, -1), order;
+    order.reserve(n);
+    for (int64_t i = 0; i < n; ++i) deg[i] = (int)(frp[i + 1] - frp[i]);
+    std::vector<char> done(n, 0);
+    std::vector<int> queue(n), nbr;
+    auto bfs_levels = [&](int s, int &last_level, std::vector<int> &touched) {
+        // breadth-first levels from s among nodes not yet ordered; returns nodes visited
+        touched.clear();
+        int head = 0, tail = 0;
+        queue[tail++] = s;
+        level[s] = 0;
+        touched.push_back(s);
+        last_level = 0;
+        while (head < tail) {
+            const int u = queue[head++];
+            last_level = std::max(last_level, level[u]);
+            for (int64_t e = frp[u]; e < frp[u + 1]; ++e) {
+                const int v = fci[e];
+                if (!done[v] && level[v] < 0) {
+                    level[v] = level[u] + 1;
+                    queue[tail++] = v;
+                    touched.push_back(v);
+                }
+            }
+        }
+    };
+    std::vector<int> touched;
+    std::vector<int64_t> by_degree(n);
+    for (int64_t i = 0; i < n; ++i) by_degree[i] = i;
+    std::stable_sort(by_degree.begin(), by_degree.end(), [&](int64_t a, int64_t b) { return deg[a] < deg[b]; });
+    for (int64_t idx = 0; idx < n; ++idx) {
+        int s = (int)by_degree[idx];
+        if (done[s]) continue;
+        // pseudo-peripheral start node
+        int ecc = -1;
+        for (int it = 0; it < 16; ++it) {
+            int last = 0;
+            bfs_levels(s, last, touched);
+            int best = -1;
+            for (int v : touched)
+                if (level[v] == last && (best < 0 || deg[v] < deg[best])) best = v;
+            for (int v : touched) level[v] = -1;
+            if (last <= ecc || best < 0) break;
+            ecc = last;
+            s = best;
+        }
+        // Cuthill-McKee from s
+        int head = (int)order.size();
+        order.push_back(s);
+        done[s] = 1;
+        while (head < (int)order.size()) {
+            const int u = order[head++];
+            nbr.clear();
+            for (int64_t e = frp[u]; e < frp[u + 1]; ++e) {
+                const int v = fci[e];
+                if (!done[v]) {
+                    done[v] = 1;
+                    nbr.push_back(v);
+                }
+            }
+            std::stable_sort(nbr.begin(), nbr.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+            order.insert(order.end(), nbr.begin(), nbr.end());
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    perm = order;
+    std::vector<int> iperm(n);
+    for (int64_t k = 0; k < n; ++k) iperm[perm[k]] = (int)k;
+    int64_t bw = 0;
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t e = frp[i]; e < frp[i + 1]; ++e) bw = std::max<int64_t>(bw, std::llabs((int64_t)iperm[i] - iperm[fci[e]]));
+    return bw;
+}
+
+int64_t band_bytes(int64_t n, int64_t bw) { return (n + 2 * NB) * (bw + 2 * NB + 1) * (int64_t)sizeof(double2); }
+
+namespace {
+
+// One factorisation K~ = L D L^T in band storage and its solves.
+struct BandLDLT {
+    int64_t n = 0, bw = 0, ldab = 0;
+    int ldw = 0;
+    double2 *band = nullptr, *W = nullptr, *Lp = nullptr;
+    int *d_info = nullptr;
+    cudaStream_t st = nullptr;
+    cublasHandle_t cb = nullptr;
+
+    int factor(Err &E) {
+        const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0), one = make_cuDoubleComplex(1.0, 0.0);
+        const size_t smem = sizeof(double2) * NB * SLD;
+        KCU(cudaMemsetAsync(d_info, 0, sizeof(int), st));
+        int prev_rows = ldw;
+        for (int64_t j0 = 0; j0 < n; j0 += NB) {
+            const int nb = (int)std::min<int64_t>(NB, n - j0);
+            ldlt_diag_kernel<<<1, KT, smem, st>>>(band, ldab, j0, nb, d_info);
+            const int rows = (int)std::min<int64_t>(bw, n - j0 - nb);
+            if (rows <= 0) continue;
+            const int zero_to = std::max(rows, prev_rows);
+            prev_rows = rows;
+            ldlt_panel_kernel<<<(zero_to + KT / 32 - 1) / (KT / 32), KT, smem, st>>>(band, ldab, j0, nb, rows, zero_to, W,
+                                                                                     Lp, ldw);
+            const int batches = (rows + NB - 1) / NB;
+            double2 *C0 = band + (j0 + nb) * ldab + NB;
+            KBL(cublasZgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_T, rows, NB, nb, &mone,
+                                          reinterpret_cast<const cuDoubleComplex *>(W), ldw, NB,
+                                          reinterpret_cast<const cuDoubleComplex *>(Lp), ldw, NB, &one,
+                                          reinterpret_cast<cuDoubleComplex *>(C0), (int)(ldab - 1), (long long)NB * ldab,
+                                          batches));
+        }
+        KCU(cudaGetLastError());
+        int info = 0;
+        KCU(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st));
+        KCU(cudaStreamSynchronize(st));
+        if (info != 0)
+            return E.set(SROM_ERR_INVALID, "K~ has an exactly zero pivot at (permuted) row " + std::to_string(info) +
+                                               ": the shifted matrix is singular");
+        return SROM_OK;
+    }
+
+    // X (n x nrhs, ldx, permuted order) <- K~^-1 X
+    int solve(double2 *X, int64_t ldx, int nrhs, Err &E) {
+        const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0), one = make_cuDoubleComplex(1.0, 0.0);
+        const size_t smem = sizeof(double2) * NB * SLD;
+        const int tgrid = (nrhs + KT / 32 - 1) / (KT / 32);
+        for (int64_t j0 = 0; j0 < n; j0 += NB) {
+            const int nb = (int)std::min<int64_t>(NB, n - j0);
+            trsv_block_kernel<<<tgrid, KT, smem, st>>>(band, ldab, j0, nb, X, ldx, nrhs, 0);
+            const int rows = (int)std::min<int64_t>(bw, n - j0 - nb);
+            if (rows <= 0) continue;
+            KBL(cublasZgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, rows, nrhs, nb, &mone,
+                            reinterpret_cast<const cuDoubleComplex *>(band + j0 * ldab + NB + nb), (int)(ldab - 1),
+                            reinterpret_cast<const cuDoubleComplex *>(X + j0), (int)ldx, &one,
+                            reinterpret_cast<cuDoubleComplex *>(X + j0 + nb), (int)ldx));
+        }
+        diag_scale_kernel<<<grid_for(n * nrhs, KT), KT, 0, st>>>(band, ldab, n, X, ldx, nrhs);
+        const int64_t last = ((n - 1) / NB) * NB;
+        for (int64_t j0 = last; j0 >= 0; j0 -= NB) {
+            const int nb = (int)std::min<int64_t>(NB, n - j0);
+            const int rows = (int)std::min<int64_t>(bw, n - j0 - nb);
+            if (rows > 0)
+                KBL(cublasZgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nb, nrhs, rows, &mone,
+                                reinterpret_cast<const cuDoubleComplex *>(band + j0 * ldab + NB + nb), (int)(ldab - 1),
+                                reinterpret_cast<const cuDoubleComplex *>(X + j0 + nb), (int)ldx, &one,
+                                reinterpret_cast<cuDoubleComplex *>(X + j0), (int)ldx));
+            trsv_block_kernel<<<tgrid, KT, smem, st>>>(band, ldab, j0, nb, X, ldx, nrhs, 1);
+        }
+        KCU(cudaGetLastError());
+        return SROM_OK;
+    }
+};
+
+// Q (n x m, ld n) <- Q - V (V^H Q) repeated until ||Q_new||_F / ||Q_old||_F > 1/sqrt(2).
+int reorthogonalize(cublasHandle_t cb, cudaStream_t st, const double2 *V, int64_t ldv, int kv, double2 *&Q,
+                    double2 *&U, int64_t n, int m, double2 *S, Err &E) {
+    if (kv == 0 || m == 0) return SROM_OK;
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0),
+                          mone = make_cuDoubleComplex(-1.0, 0.0);
+    const double eta = 1.0 / std::sqrt(2.0);
+    for (int it = 0; it < 64; ++it) {
+        KBL(cublasZgemm(cb, CUBLAS_OP_C, CUBLAS_OP_N, kv, m, (int)n, &one, reinterpret_cast<const cuDoubleComplex *>(V),
+                        (int)ldv, reinterpret_cast<const cuDoubleComplex *>(Q), (int)n, &zero,
+                        reinterpret_cast<cuDoubleComplex *>(S), kv));
+        KCU(cudaMemcpyAsync(U, Q, sizeof(double2) * n * m, cudaMemcpyDeviceToDevice, st));
+        KBL(cublasZgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, m, kv, &mone, reinterpret_cast<const cuDoubleComplex *>(V),
+                        (int)ldv, reinterpret_cast<const cuDoubleComplex *>(S), kv, &one,
+                        reinterpret_cast<cuDoubleComplex *>(U), (int)n));
+        double nu = 0.0, nq = 0.0;
+        KBL(cublasDznrm2(cb, (int)(n * m), reinterpret_cast<const cuDoubleComplex *>(U), 1, &nu));
+        KBL(cublasDznrm2(cb, (int)(n * m), reinterpret_cast<const cuDoubleComplex *>(Q), 1, &nq));
+        std::swap(Q, U);
+        if (!(nu / nq <= eta)) return SROM_OK;  // also leaves on NaN
+    }
+    return SROM_OK;
+}
+
+// Column-pivoted Householder QR of A (n x m, ld n) in place (zgeqp3's steps, partial norms
+// recomputed exactly each step); |R_ii| in order go to rdiag; then Qo (n x rr, ld n) = the first
+// rr columns of the orthonormal factor (zungqr), rr = leading |R_ii| > tol.
+int pivoted_qr(cudaStream_t st, double2 *A, int64_t n, int m, double tol, double2 *Qo, double *d_norms, double2 *d_w,
+               std::vector<double> &rdiag, int &rr, Err &E) {
+    std::vector<double2> taus(m);
+    std::vector<double> norms(m);
+    const int kmax = (int)std::min<int64_t>(n, m);
+    rdiag.assign(kmax, 0.0);
+    for (int k = 0; k < kmax; ++k) {
+        const int cnt = m - k;
+        col_norm2_kernel<<<cnt, KT, 0, st>>>(A, n, n, k, k, d_norms);
+        KCU(cudaMemcpyAsync(norms.data(), d_norms, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st));
+        KCU(cudaStreamSynchronize(st));
+        int p = 0;
+        for (int j = 1; j < cnt; ++j)
+            if (norms[j] > norms[p]) p = j;
+        if (p != 0) swap_cols_kernel<<<grid_for(n, KT), KT, 0, st>>>(A, n, n, k, k + p);
+        double2 alpha;
+        KCU(cudaMemcpyAsync(&alpha, A + k + (int64_t)k * n, sizeof(double2), cudaMemcpyDeviceToHost, st));
+        KCU(cudaStreamSynchronize(st));
+        const double xnorm2 = std::max(0.0, norms[p] - (alpha.x * alpha.x + alpha.y * alpha.y));
+        double2 tau = make_double2(0.0, 0.0);
+        double beta = alpha.x;
+        if (!(xnorm2 == 0.0 && alpha.y == 0.0)) {
+            const double nrm = std::sqrt(norms[p]);
+            beta = alpha.x >= 0.0 ? -nrm : nrm;
+            tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+            // s = 1 / (alpha - beta)
+            const double ar = alpha.x - beta, ai = alpha.y, den = ar * ar + ai * ai;
+            householder_scale_kernel<<<grid_for(n, KT), KT, 0, st>>>(A, n, n, k, make_double2(ar / den, -ai / den), beta);
+        }
+        taus[k] = tau;
+        rdiag[k] = std::fabs(beta) > 0.0 ? std::fabs(beta) : std::hypot(alpha.x, alpha.y);
+        if (k + 1 < m && (tau.x != 0.0 || tau.y != 0.0)) {
+            reflector_dots_kernel<<<m - k - 1, KT, 0, st>>>(A, n, k, A, n, n, k, k + 1, d_w);
+            reflector_apply_kernel<<<grid_for((n - k) * (m - k - 1), KT), KT, 0, st>>>(
+                A, n, k, A, n, n, k, k + 1, m - k - 1, d_w, make_double2(tau.x, -tau.y));
+        }
+    }
+    KCU(cudaGetLastError());
+    rr = 0;
+    while (rr < kmax && rdiag[rr] > tol) ++rr;
+    // Q = H_0 H_1 ... H_{rr-1} applied to the first rr unit columns, last reflector first
+    for (int i = rr - 1; i >= 0; --i) {
+        const double2 tau = taus[i];
+        if (i + 1 < rr) {
+            reflector_dots_kernel<<<rr - i - 1, KT, 0, st>>>(A, n, i, Qo, n, n, i, i + 1, d_w);
+            reflector_apply_kernel<<<grid_for((n - i) * (rr - i - 1), KT), KT, 0, st>>>(A, n, i, Qo, n, n, i, i + 1,
+                                                                                      rr - i - 1, d_w, tau);
+        }
+        reflector_column_kernel<<<grid_for(n, KT), KT, 0, st>>>(A, n, i, Qo, n, n, i, tau);
+    }
+    KCU(cudaGetLastError());
+    return SROM_OK;
+}
+
+}  // namespace
+
+int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *log) {
+    Err E;
+    cudaStream_t st = a.stream;
+    const int64_t n = a.n_rows;
+    *n_cols = 0;
+    if (log) log->blocks.clear();
+    if (n == 0 || a.n_in == 0 || a.n_points == 0) return SROM_OK;
+    // host copies of the pattern: full symmetric pattern and RCM order
+    std::vector<int64_t> rp(n + 1);
+    std::vector<int> ci(a.nnz);
+    {
+        cudaError_t e = cudaMemcpyAsync(rp.data(), a.rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && a.nnz > 0)
+            e = cudaMemcpyAsync(ci.data(), a.colind, sizeof(int) * a.nnz, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            *msg = std::string("copying the pattern to the host: ") + cudaGetErrorString(e);
+            return SROM_ERR_CUDA;
+        }
+    }
+    if (rp[0] != a.base || rp[n] - a.base != a.nnz) {
+        *msg = "rowptr does not start at base or does not end at base + nnz";
+        return SROM_ERR_INVALID;
+    }
+    std::vector<int64_t> frp, fmap;
+    std::vector<int> fci, perm;
+    {
+        std::string err;
+        int s = full_pattern(n, a.nnz, rp.data(), ci.data(), a.base, a.upper, frp, fci, fmap, &err);
+        if (s) {
+            *msg = err;
+            return s;
+        }
+    }
+    const int64_t bw = rcm_order(n, frp, fci, perm);
+    std::vector<int> iperm(n);
+    for (int64_t k = 0; k < n; ++k) iperm[perm[k]] = (int)k;
+    if (log) log->bandwidth = bw;
+
+    Bufs B;
+    B.st = st;
+    BandLDLT F;
+    F.n = n;
+    F.bw = bw;
+    F.ldab = bw + 2 * NB + 1;
+    F.ldw = (int)(2 * bw + NB);
+    F.st = st;
+    int64_t *d_frp = nullptr, *d_fmap = nullptr;
+    int *d_fci = nullptr, *d_iperm = nullptr;
+    const int mmax = std::max(a.n_in, 1);
+    double2 *Q = nullptr, *U = nullptr, *Qo = nullptr, *S = nullptr, *d_w = nullptr;
+    double *d_norms = nullptr;
+    auto need = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess) E.set(e == cudaErrorMemoryAllocation ? SROM_ERR_ALLOC : SROM_ERR_CUDA,
+                                    std::string("allocating ") + what + ": " + cudaGetErrorString(e));
+        return e == cudaSuccess;
+    };
+    if (!need(B.alloc(&F.band, (size_t)(n + 2 * NB) * F.ldab), "the band factor") ||
+        !need(B.alloc(&F.W, (size_t)F.ldw * NB), "the panel") || !need(B.alloc(&F.Lp, (size_t)F.ldw * NB), "the panel") ||
+        !need(B.alloc(&F.d_info, 1), "info") || !need(B.alloc(&d_frp, n + 1), "the pattern") ||
+        !need(B.alloc(&d_fci, frp[n]), "the pattern") || !need(B.alloc(&d_fmap, frp[n]), "the pattern") ||
+        !need(B.alloc(&d_iperm, n), "the ordering") || !need(B.alloc(&Q, (size_t)n * mmax), "the block") ||
+        !need(B.alloc(&U, (size_t)n * mmax), "the block") || !need(B.alloc(&Qo, (size_t)n * mmax), "the block") ||
+        !need(B.alloc(&S, (size_t)std::max(a.max_cols, 1) * mmax), "the block") ||
+        !need(B.alloc(&d_w, mmax), "the block") || !need(B.alloc(&d_norms, mmax), "the block")) {
+        *msg = E.msg;
+        return E.code;
+    }
+    cublasHandle_t cb = nullptr;
+    if (cublasCreate(&cb) != CUBLAS_STATUS_SUCCESS) {
+        *msg = "cublasCreate failed";
+        return SROM_ERR_CUDA;
+    }
+    struct CbGuard {
+        cublasHandle_t h;
+        cudaStream_t st;
+        ~CbGuard() {
+            cudaStreamSynchronize(st);  // nothing queued may still use the handle's workspace
+            cublasDestroy(h);
+        }
+    } cbg{cb, st};
+    F.cb = cb;
+    auto run = [&]() -> int {
+        KBL(cublasSetStream(cb, st));
+        KBL(cublasSetPointerMode(cb, CUBLAS_POINTER_MODE_HOST));
+        const size_t smem = sizeof(double2) * NB * SLD;
+        KCU(cudaFuncSetAttribute(ldlt_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        KCU(cudaFuncSetAttribute(ldlt_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        KCU(cudaFuncSetAttribute(trsv_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        KCU(cudaMemcpyAsync(d_frp, frp.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
+        KCU(cudaMemcpyAsync(d_fci, fci.data(), sizeof(int) * frp[n], cudaMemcpyHostToDevice, st));
+        KCU(cudaMemcpyAsync(d_fmap, fmap.data(), sizeof(int64_t) * frp[n], cudaMemcpyHostToDevice, st));
+        KCU(cudaMemcpyAsync(d_iperm, iperm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+        KCU(cudaMemsetAsync(F.W, 0, sizeof(double2) * F.ldw * NB, st));
+        KCU(cudaMemsetAsync(F.Lp, 0, sizeof(double2) * F.ldw * NB, st));
+        int kv = 0;  // columns of V so far
+        std::vector<double> rdiag;
+        for (int ip = 0; ip < a.n_points; ++ip) {
+            const double w = 2.0 * 3.141592653589793 * a.exp_points_hz[ip];
+            KCU(cudaMemsetAsync(F.band, 0, sizeof(double2) * (size_t)(n + 2 * NB) * F.ldab, st));
+            scatter_band_kernel<<<grid_for(n * 32, KT), KT, 0, st>>>(
+                n, d_frp, d_fci, d_fmap, reinterpret_cast<const double2 *>(a.K), reinterpret_cast<const double2 *>(a.M),
+                reinterpret_cast<const double2 *>(a.D), w, d_iperm, F.band, F.ldab);
+            KCU(cudaGetLastError());
+            int s = F.factor(E);
+            if (s) return s;
+            // Q = K~^-1 B
+            int m = a.n_in;
+            permute_kernel<<<grid_for(n * m, KT), KT, 0, st>>>(n, m, d_iperm, reinterpret_cast<const double2 *>(a.B),
+                                                               a.ldb, U, n, 1);
+            s = F.solve(U, n, m, E);
+            if (s) return s;
+            permute_kernel<<<grid_for(n * m, KT), KT, 0, st>>>(n, m, d_iperm, U, n, Q, n, 0);
+            for (int order = 1; order <= a.order; ++order) {
+                if (order > 1) {
+                    // Q = K~^-1 (M Q)
+                    csr_spmm_complex_kernel<<<grid_for(n * 32, KT), KT, 0, st>>>(
+                        n, d_frp, d_fci, d_fmap, reinterpret_cast<const double2 *>(a.M), Qo, n, m, Q, n);
+                    permute_kernel<<<grid_for(n * m, KT), KT, 0, st>>>(n, m, d_iperm, Q, n, U, n, 1);
+                    s = F.solve(U, n, m, E);
+                    if (s) return s;
+                    permute_kernel<<<grid_for(n * m, KT), KT, 0, st>>>(n, m, d_iperm, U, n, Q, n, 0);
+                }
+                if (ip > 0 || order > 1) {
+                    s = reorthogonalize(cb, st, reinterpret_cast<const double2 *>(a.V), a.ldv, kv, Q, U, n, m, S, E);
+                    if (s) return s;
+                }
+                int rr = 0;
+                s = pivoted_qr(st, Q, n, m, a.tol, Qo, d_norms, d_w, rdiag, rr, E);
+                if (s) return s;
+                if (log) log->blocks.push_back({a.exp_points_hz[ip], order, rr, rdiag});
+                if (rr == 0) break;
+                if (kv + rr > a.max_cols)
+                    return E.set(SROM_ERR_INVALID, "the basis needs more than max_cols = " + std::to_string(a.max_cols) +
+                                                       " columns");
+                KCU(cudaMemcpy2DAsync(reinterpret_cast<double2 *>(a.V) + (int64_t)kv * a.ldv, sizeof(double2) * a.ldv, Qo,
+                                      sizeof(double2) * n, sizeof(double2) * n, rr, cudaMemcpyDeviceToDevice, st));
+                kv += rr;
+                *n_cols = kv;
+                m = rr;
+            }
+        }
+        KCU(cudaStreamSynchronize(st));
+        return SROM_OK;
+    };
+    const int s = run();
+    if (s) *msg = E.msg;
+    return s;
+}
+
+}  // namespace kry
+}  // namespace srom

@@ -1,0 +1,51 @@
+// Host-side entry of the Krylov basis generation (krylov.cu), used by the C ABI in capi.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace srom {
+namespace kry {
+
+struct KrylovArgs {
+    cudaStream_t stream;
+    int64_t n_rows, nnz;
+    const int64_t *rowptr;  // device, CSR (base 0 or 1), full symmetric or upper storage
+    const int *colind;
+    int base, upper;
+    const void *K, *M, *D;  // device srom_complex values on the pattern; D may be null
+    const void *B;          // device n_rows x n_in inputs, leading dimension ldb
+    int n_in;
+    int64_t ldb;
+    const double *exp_points_hz;  // host
+    int n_points, order;
+    double tol;
+    void *V;  // device n_rows x max_cols output, leading dimension ldv
+    int64_t ldv;
+    int max_cols;
+};
+
+struct KrylovBlock {
+    double point_hz;
+    int order, rank;
+    std::vector<double> rdiag;  // |R_ii| of the block's pivoted QR
+};
+
+struct KrylovLog {
+    int64_t bandwidth = 0;
+    std::vector<KrylovBlock> blocks;
+};
+
+int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *log);
+
+// host helpers (also behind srom_band_order)
+int full_pattern(int64_t n, int64_t nnz, const int64_t *rp, const int *ci, int base, int upper, std::vector<int64_t> &frp,
+                 std::vector<int> &fci, std::vector<int64_t> &fmap, std::string *err);
+int64_t rcm_order(int64_t n, const std::vector<int64_t> &frp, const std::vector<int> &fci, std::vector<int> &perm);
+int64_t band_bytes(int64_t n, int64_t bw);
+
+}  // namespace kry
+}  // namespace srom

@@ -1,0 +1,161 @@
+"""Krylov basis generation on the GPU (srom_krylov_basis) against the oracle's restatement of
+addKrylovModesForExpansionPoint (oracle/krylov.py: SuperLU solves, LAPACK pivoted QR).
+
+Gate: the same rank for every block (so the same number of columns), the GPU basis spanning
+the oracle's to 1e-8 and vice versa, orthonormal to 1e-12; and the reduced model built on it
+reproducing the full-order response near the expansion points."""
+import math
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from oracle import krylov as KR
+from staccato_b200 import _capi
+from staccato_b200 import fe_tet10 as T
+from staccato_b200.krylov import krylov_basis
+from staccato_b200.project import DeviceCsr, project_complex
+
+pytestmark = pytest.mark.gpu
+
+
+def _block(dims=(4, 4, 8), keep_clamped=False):
+    """Tet10 block, clamped DOFs removed, K and M scaled to unit maximum (so that the absolute
+    deflation tolerance of the reference, 1e-8, separates rank)."""
+    m = T.clamped_block(*dims)
+    K = sp.csr_matrix((m.K, m.indices, m.indptr), shape=(m.n_dof, m.n_dof))
+    M = sp.csr_matrix((m.M, m.indices, m.indptr), shape=(m.n_dof, m.n_dof))
+    if not keep_clamped:
+        keep = ~m.clamped
+        K, M = K[keep][:, keep].tocsr(), M[keep][:, keep].tocsr()
+    K = K / abs(K).max()
+    M = M / abs(M).max()
+    K.sort_indices()
+    M.sort_indices()
+    assert np.array_equal(M.indptr, K.indptr) and np.array_equal(M.indices, K.indices)
+    return K, M
+
+
+def _first_f(K, M):
+    return math.sqrt(spla.eigsh(K, k=1, M=M, sigma=0, which="LM")[0][0]) / (2 * math.pi)
+
+
+def _dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.complex128)).cuda()
+
+
+def _inputs(N, seed=0):
+    rng = np.random.default_rng(seed)
+    B = np.zeros((N, 3), dtype=np.complex128)
+    idx = rng.choice(N, 3, replace=False)
+    B[idx, [0, 1, 2]] = 1.0
+    B[:, 2] = B[:, 0]  # a dependent input: deflated by the rank test
+    return B
+
+
+def _upper(K, *mats):
+    """Upper-triangle storage of matrices sharing K's (sorted) CSR pattern: one mask for all."""
+    rows = np.repeat(np.arange(K.shape[0]), np.diff(K.indptr))
+    keep = K.indices >= rows
+    indptr = np.concatenate([[0], np.cumsum(np.bincount(rows[keep], minlength=K.shape[0]))])
+    return indptr, K.indices[keep], [m.data[keep] for m in (K,) + mats]
+
+
+def _run(handle, K, M, D, B, pts, order, upper=False, base=0):
+    import torch
+
+    mats = (M,) if D is None else (M, D)
+    if upper:
+        indptr, indices, data = _upper(K, *mats)
+    else:
+        indptr, indices, data = K.indptr, K.indices, [K.data] + [m.data for m in mats]
+    csr = DeviceCsr.from_host(indptr + base, indices + base, base=base, upper=upper)
+    vals = [_dev(torch, data[0]), _dev(torch, data[1])]
+    dv = None if D is None else _dev(torch, data[2])
+    Bt = _dev(torch, B.T)  # (n_in, N) row-major == N x n_in column-major
+    V = krylov_basis(handle, csr, vals[0], vals[1], dv, Bt, pts, order)
+    torch.cuda.synchronize()
+    return V.cpu().numpy().T  # N x k
+
+
+@pytest.fixture(scope="module")
+def problem():
+    K, M = _block()
+    f1 = _first_f(K, M)
+    D = sp.csr_matrix((0.01 * K.data + 0.001 * M.data, K.indices, K.indptr), shape=K.shape)
+    return K, M, D, f1
+
+
+def test_basis_matches_oracle(handle, problem):
+    K, M, D, f1 = problem
+    B = _inputs(K.shape[0])
+    pts = [0.5 * f1, 3.0 * f1]
+    Vo, log = KR.krylov_basis(K, M, D, B, pts, 4, 1e-8, return_log=True)
+    V = _run(handle, K, M, D, B, pts, 4)
+    assert V.shape == Vo.shape, (V.shape, Vo.shape, [l[2] for l in log])
+    assert np.abs(V.conj().T @ V - np.eye(V.shape[1])).max() <= 1e-12
+    assert KR.subspace_gap(V, Vo) <= 1e-8
+    assert KR.subspace_gap(Vo, V) <= 1e-8
+
+
+def test_without_damping_and_single_point(handle, problem):
+    K, M, _, f1 = problem
+    B = _inputs(K.shape[0], seed=3)[:, :2]
+    Vo = KR.krylov_basis(K, M, None, B, [0.3 * f1], 3, 1e-8)
+    V = _run(handle, K, M, None, B, [0.3 * f1], 3)
+    assert V.shape == Vo.shape
+    assert KR.subspace_gap(V, Vo) <= 1e-8 and KR.subspace_gap(Vo, V) <= 1e-8
+
+
+def test_upper_storage_and_base_one(handle, problem):
+    K, M, D, f1 = problem
+    B = _inputs(K.shape[0], seed=5)
+    pts = [0.5 * f1, 2.0 * f1]
+    V0 = _run(handle, K, M, D, B, pts, 2)
+    V1 = _run(handle, K, M, D, B, pts, 2, upper=True, base=1)
+    assert V0.shape == V1.shape
+    assert np.abs(V0 - V1).max() <= 1e-12
+
+
+def test_reduced_model_reproduces_the_full_order_response(handle, problem):
+    """Project K, M, D on the basis and solve the reduced model at frequencies around the
+    expansion points: the reduced transfer function matches the full-order solve."""
+    import torch
+
+    K, M, D, f1 = problem
+    N = K.shape[0]
+    B = _inputs(N, seed=7)[:, :2]
+    pts = [0.5 * f1, 2.5 * f1]
+    V = _run(handle, K, M, D, B, pts, 4)
+    csr = DeviceCsr.from_host(K.indptr, K.indices)
+    Vt = torch.from_numpy(np.ascontiguousarray(V.T)).cuda()
+    Kr, Mr, Dr = [r.cpu().numpy() for r in project_complex(
+        handle, csr, [_dev(torch, K.data), _dev(torch, M.data), _dev(torch, D.data)], Vt)]
+    Br = V.conj().T @ B
+    for f in (0.45 * f1, 0.55 * f1, 2.4 * f1, 2.6 * f1):
+        w = 2 * math.pi * f
+        x_full = spla.spsolve((K - w * w * M + 1j * w * D).tocsc(), B)
+        x_red = V @ np.linalg.solve(Kr - w * w * Mr + 1j * w * Dr, Br)
+        err = np.linalg.norm(x_red - x_full) / np.linalg.norm(x_full)
+        assert err <= 1e-6, (f / f1, err)
+
+
+def test_singular_shift_and_column_limit(handle):
+    import torch
+
+    K, M = _block(keep_clamped=True)  # clamped DOFs left in: empty rows, K~ singular
+    B = _inputs(K.shape[0])
+    with pytest.raises(_capi.SromError) as e:
+        _run(handle, K, M, None, B, [1e-4], 2)
+    assert e.value.status == _capi.SROM_ERR_INVALID and "pivot" in str(e.value)
+    K, M = _block()
+    csr = DeviceCsr.from_host(K.indptr, K.indices)
+    with pytest.raises(_capi.SromError) as e:
+        krylov_basis(handle, csr, _dev(torch, K.data), _dev(torch, M.data), None,
+                     _dev(torch, _inputs(K.shape[0]).T), [1e-4], 3, max_cols=2)
+    assert e.value.status == _capi.SROM_ERR_INVALID and "max_cols" in str(e.value)
+    # the handle still works after both errors
+    V = krylov_basis(handle, csr, _dev(torch, K.data), _dev(torch, M.data), None,
+                     _dev(torch, _inputs(K.shape[0]).T), [1e-4], 1)
+    assert V.shape[0] == 2
