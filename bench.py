@@ -338,6 +338,45 @@ def workloads_leg(torch, dev, h, reps=3):
     return out
 
 
+def krylov_leg(torch, dev, h):
+    """Krylov basis generation (srom_krylov_basis) on the Tet10 block of the projection leg
+    (10 x 10 x 40 hexes, z = 0 face clamped and removed, N = 105,840): D = 1e-5 K + 2 M, four
+    unit-scaled point loads, one expansion point of order 1 and two points (100, 800 Hz) of
+    order 4.  Wall time of the call (it synchronises: host ordering, band factorisation of K~
+    per point, solves, re-orthogonalisation, pivoted QR) and the band factor's size."""
+    import scipy.sparse as sp
+
+    from staccato_b200 import fe_tet10
+    from staccato_b200.krylov import band_order, krylov_basis
+    from staccato_b200.project import DeviceCsr
+
+    m = fe_tet10.clamped_block(10, 10, 40)
+    keep = ~m.clamped
+    K = sp.csr_matrix((m.K, m.indices, m.indptr), shape=(m.n_dof, m.n_dof))[keep][:, keep].tocsr()
+    M = sp.csr_matrix((m.M, m.indices, m.indptr), shape=(m.n_dof, m.n_dof))[keep][:, keep].tocsr()
+    K.sort_indices()
+    M.sort_indices()
+    n = K.shape[0]
+    _, bw, band_b = band_order(K.indptr, K.indices)
+    rng = np.random.default_rng(0)
+    B = np.zeros((n, 4), dtype=np.complex128)
+    B[rng.choice(n, 4, replace=False), np.arange(4)] = 1e9
+    c = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.complex128)).to(dev)
+    csr = DeviceCsr.from_host(K.indptr, K.indices, device=dev)
+    Kd, Md, Dd, Bd = c(K.data), c(M.data), c(1e-5 * K.data + 2.0 * M.data), c(B.T)
+    out = {"workload": "Tet10 block 10x10x40, N=%d, nnz=%d, 4 inputs" % (n, K.nnz), "bandwidth": bw,
+           "band_gb": band_b / 1e9, "solver": "band LDL^T (RCM order), cuBLAS ZGEMM trailing updates"}
+    for name, pts, order in (("one_point_order1", [100.0], 1), ("two_points_order4", [100.0, 800.0], 4)):
+        krylov_basis(h, csr, Kd, Md, Dd, Bd, pts, order)  # warm-up
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        V = krylov_basis(h, csr, Kd, Md, Dd, Bd, pts, order)
+        torch.cuda.synchronize(dev)
+        out[name] = {"s": time.perf_counter() - t0, "columns": int(V.shape[0])}
+    out["factor_tflop"] = 8.0 * n * bw * bw / 1e12
+    return out
+
+
 # ----------------------------------------------------------------------------- arms
 
 def run_reference(args):
@@ -528,6 +567,7 @@ def run_ours(args):
         extras["projection"] = projection_leg(torch, dev, h, measured_peaks())
         extras["adjoint"] = adjoint_leg(torch, dev, h)
         extras["workloads"] = workloads_leg(torch, dev, h)
+        extras["krylov"] = krylov_leg(torch, dev, h)
 
     cpu = acc = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

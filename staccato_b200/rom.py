@@ -1,8 +1,11 @@
 """``KrylovROMSubstructure``: the reference's ROM interface on the B200 kernels.
 
-Mirrors the two members of STACCATO's ``KrylovROMSubstructure`` that form the hot path
-(src/analysis/KrylovROMSubstructure.h:156, .cpp:709-765 and :1393-1460):
+Mirrors the members of STACCATO's ``KrylovROMSubstructure`` that form the hot path
+(src/analysis/KrylovROMSubstructure.h:156, .cpp:709-765 and :1393-1460) and the basis
+generation before it (.cpp:367-569):
 
+* ``add_krylov_modes_for_expansion_point(...)`` -- the Krylov basis V for the given expansion
+  points and order (block Arnoldi with deflation; the shifted FE matrix factored on the GPU);
 * ``generate_rom(K, M, V, D=None, B=None, C=None)`` -- project the sparse FE operators onto
   the basis: K_r = V^T K V, M_r = V^T M V (D_r = V^T D V), B_r = V^T B, C_r = C V;
 * ``back_transform_kmor(freq_hz, input_load)`` -- for every frequency assemble
@@ -29,6 +32,7 @@ class KrylovROMSubstructure:
         self.handle = handle or _capi.Handle(device)
         self.device = device
         self.K_r = self.M_r = self.D_r = self.B_r = self.C_r = None
+        self.V = None
         self.eta = 0.0
 
     # --------------------------------------------------------------- reduced operators
@@ -40,6 +44,21 @@ class KrylovROMSubstructure:
         c = lambda a: None if a is None else torch.as_tensor(a, dtype=torch.complex128, device=dev)
         self.K_r, self.M_r, self.D_r, self.B_r, self.C_r = c(K_r), c(M_r), c(D_r), c(B_r), c(C_r)
         self.eta = float(eta)
+
+    def add_krylov_modes_for_expansion_point(self, csr: DeviceCsr, K_vals, M_vals, B, exp_points_hz, krylov_order: int,
+                                             D_vals=None, tol: float = 1e-8):
+        """The basis of addKrylovModesForExpansionPoint (KrylovROMSubstructure.cpp:367-569) on the
+        GPU (``srom_krylov_basis``), kept as ``self.V`` ((k, n) complex128 = n x k column-major,
+        ready for ``generate_rom``).  B: n x n_in (numpy or torch)."""
+        import torch
+
+        from .krylov import krylov_basis
+
+        dev = torch.device("cuda", self.device)
+        c = lambda a: None if a is None else torch.as_tensor(a, dtype=torch.complex128, device=dev).contiguous()
+        Bt = torch.as_tensor(B, dtype=torch.complex128, device=dev).t().contiguous()
+        self.V = krylov_basis(self.handle, csr, c(K_vals), c(M_vals), c(D_vals), Bt, exp_points_hz, krylov_order, tol)
+        return self.V
 
     def generate_rom(self, csr: DeviceCsr, K_vals, M_vals, V, D_vals=None, B=None, C=None, eta: float = 0.0):
         """Projection of the FE operators (sharing the CSR pattern) onto V, as generateROM

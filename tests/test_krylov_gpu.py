@@ -159,3 +159,28 @@ def test_singular_shift_and_column_limit(handle):
     V = krylov_basis(handle, csr, _dev(torch, K.data), _dev(torch, M.data), None,
                      _dev(torch, _inputs(K.shape[0]).T), [1e-4], 1)
     assert V.shape[0] == 2
+
+
+def test_rom_interface_generates_basis_then_rom(handle, problem):
+    """KrylovROMSubstructure mirror: basis, projection and sweep in a row; the sweep's output
+    matches the full-order solve at an expansion point."""
+    import torch
+
+    from staccato_b200.rom import KrylovROMSubstructure
+
+    K, M, D, f1 = problem
+    N = K.shape[0]
+    B = _inputs(N, seed=11)[:, :2]
+    C = np.zeros((3, N))
+    C[np.arange(3), np.random.default_rng(12).choice(N, 3, replace=False)] = 1.0
+    sub = KrylovROMSubstructure(handle=handle)
+    csr = DeviceCsr.from_host(K.indptr, K.indices)
+    V = sub.add_krylov_modes_for_expansion_point(csr, K.data, M.data, B, [0.5 * f1], 4, D_vals=D.data)
+    sub.generate_rom(csr, _dev(torch, K.data), _dev(torch, M.data), V, D_vals=_dev(torch, D.data), B=B, C=C)
+    f = 0.5 * f1
+    Y, info = sub.back_transform_kmor([f], np.eye(2))
+    y = Y[0].cpu().numpy()
+    assert (info.cpu().numpy() == 0).all()
+    w = 2 * math.pi * f
+    y_full = C @ spla.spsolve((K - w * w * M + 1j * w * D).tocsc(), B)
+    assert np.linalg.norm(y - y_full) <= 1e-8 * np.linalg.norm(y_full)
