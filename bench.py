@@ -374,6 +374,15 @@ def krylov_leg(torch, dev, h):
         torch.cuda.synchronize(dev)
         out[name] = {"s": time.perf_counter() - t0, "columns": int(V.shape[0])}
     out["factor_tflop"] = 8.0 * n * bw * bw / 1e12
+    # full-order direct sweep (performSolveFOM) at two frequencies, the four loads at once
+    from staccato_b200.krylov import fom_sweep
+
+    fom_sweep(h, csr, Kd, Md, Dd, Bd, [500.0])  # warm-up
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    fom_sweep(h, csr, Kd, Md, Dd, Bd, [300.0, 900.0])
+    torch.cuda.synchronize(dev)
+    out["fom_sweep_s_per_freq"] = (time.perf_counter() - t0) / 2
     return out
 
 

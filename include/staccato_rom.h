@@ -258,6 +258,20 @@ SROM_API int srom_krylov_basis(srom_handle *h, int64_t n_rows, int64_t nnz, cons
                                int krylov_order, double tol, srom_complex *V, int64_t ldv, int max_cols, int *n_cols);
 
 /*
+ * Full-order frequency sweep, KrylovROMSubstructure::performSolveFOM
+ * (src/analysis/KrylovROMSubstructure.cpp:1355-1391): for every frequency f (Hz, w = 2 pi f)
+ * solve (K - w^2 M + i w D) X_f = F directly on the GPU, with the band LDL^T of
+ * srom_krylov_basis (same pattern arguments and memory; the matrix must be complex symmetric).
+ *   F: device n_rows x r loads (ldf).  freq_hz: HOST array.  X: device, n_freq blocks of
+ *   n_rows x r (leading dimension ldx, block f at X + f * ldx * r), stacked per frequency like
+ *   the reference's results vector.  Synchronises the handle's stream.
+ */
+SROM_API int srom_fom_sweep(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind,
+                            int base, int upper, const srom_complex *K, const srom_complex *M, const srom_complex *D,
+                            const srom_complex *F, int r, int64_t ldf, const double *freq_hz, int n_freq,
+                            srom_complex *X, int64_t ldx);
+
+/*
  * Host-only: the reverse Cuthill-McKee ordering srom_krylov_basis uses for a pattern (HOST
  * rowptr/colind, as above).  perm (n_rows ints, may be NULL): perm[k] = original row of row k;
  * *bandwidth = max |new i - new j| over the entries; *band_bytes = device bytes of the band

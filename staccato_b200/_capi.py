@@ -37,7 +37,7 @@ EXPORTS = [
     "srom_sweep_backward",
     "srom_graph_create", "srom_graph_launch", "srom_graph_destroy", "srom_tune",
     "srom_mtx_read_dense", "srom_mtx_write_dense", "srom_write_solution",
-    "srom_krylov_basis", "srom_band_order",
+    "srom_krylov_basis", "srom_band_order", "srom_fom_sweep",
 ]
 
 SROM_DPARAM_LOWRANK = 0
@@ -117,6 +117,9 @@ def lib() -> C.CDLL:
         L.srom_krylov_basis.argtypes = [vp, C.c_int64, C.c_int64, vp, vp, i, i, vp, vp, vp, vp, i, C.c_int64, vp, i, i,
                                         C.c_double, vp, C.c_int64, i, C.POINTER(i)]
         L.srom_krylov_basis.restype = i
+        L.srom_fom_sweep.argtypes = [vp, C.c_int64, C.c_int64, vp, vp, i, i, vp, vp, vp, vp, i, C.c_int64, vp, i, vp,
+                                     C.c_int64]
+        L.srom_fom_sweep.restype = i
         L.srom_band_order.argtypes = [C.c_int64, C.c_int64, vp, vp, i, i, vp, C.POINTER(C.c_int64),
                                       C.POINTER(C.c_int64), C.c_char_p, i]
         L.srom_band_order.restype = i

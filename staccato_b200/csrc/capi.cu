@@ -926,6 +926,50 @@ int srom_krylov_basis(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t
     return SROM_OK;
 }
 
+int srom_fom_sweep(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind, int base,
+                   int upper, const srom_complex *K, const srom_complex *M, const srom_complex *D, const srom_complex *F,
+                   int r, int64_t ldf, const double *freq_hz, int n_freq, srom_complex *X, int64_t ldx) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    if (n_rows < 0 || nnz < 0 || r < 0 || n_freq < 0) return set_err(h, SROM_ERR_INVALID, "negative size");
+    if (n_rows > INT32_MAX - 1) return set_err(h, SROM_ERR_UNSUPPORTED, "n_rows above 2^31 - 2");
+    if (base != 0 && base != 1) return set_err(h, SROM_ERR_INVALID, "base must be 0 or 1");
+    if (n_rows == 0 || r == 0 || n_freq == 0) return SROM_OK;
+    if (!rowptr || !colind || !K || !M || !F || !X || !freq_hz)
+        return set_err(h, SROM_ERR_INVALID, "rowptr, colind, K, M, F, X and freq_hz must be non-null");
+    if (ldf < n_rows || ldx < n_rows) return set_err(h, SROM_ERR_INVALID, "ldf and ldx must be >= n_rows");
+    if (n_rows * (int64_t)r > INT32_MAX) return set_err(h, SROM_ERR_UNSUPPORTED, "n_rows * r above 2^31 - 1");
+    if (srom::misaligned(K, 16) || srom::misaligned(M, 16) || srom::misaligned(D, 16) || srom::misaligned(F, 16) ||
+        srom::misaligned(X, 16) || srom::misaligned(rowptr, 8) || srom::misaligned(colind, 4))
+        return set_err(h, SROM_ERR_INVALID, "complex arrays must be 16-byte aligned (rowptr 8, colind 4)");
+    for (int i = 0; i < n_freq; ++i)
+        if (!std::isfinite(freq_hz[i])) return set_err(h, SROM_ERR_INVALID, "frequency %d is not finite", i);
+    DeviceGuard g(h->device);
+    srom::kry::FomArgs a{};
+    a.stream = h->stream;
+    a.n_rows = n_rows;
+    a.nnz = nnz;
+    a.rowptr = rowptr;
+    a.colind = colind;
+    a.base = base;
+    a.upper = upper ? 1 : 0;
+    a.K = K;
+    a.M = M;
+    a.D = D;
+    a.F = F;
+    a.r = r;
+    a.ldf = ldf;
+    a.freq_hz = freq_hz;
+    a.n_freq = n_freq;
+    a.X = X;
+    a.ldx = ldx;
+    std::string msg;
+    ProfScope ps(h, "fom_sweep", n_freq, 0.0, 0.0);
+    const int s = srom::kry::fom_sweep(a, &msg);
+    if (s) return set_err(h, s, "%s", msg.c_str());
+    return SROM_OK;
+}
+
 int srom_band_order(int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind, int base, int upper,
                     int *perm, int64_t *bandwidth, int64_t *band_bytes_out, char *err, int err_len) {
     auto fail = [&](int code, const std::string &m) {

@@ -63,11 +63,13 @@ __device__ __forceinline__ double2 shfl2(double2 v, int src) {
 // ---- K~ into band storage -----------------------------------------------------------------
 // Full symmetric pattern (0-based, rows of the original numbering); vmap[e] indexes the caller's
 // value arrays.  Entry (i, j) lands at (pi, pj) = (iperm[i], iperm[j]) when pi >= pj, so every
-// unordered pair is written once.  Value -(K - w^2 M + i w D).  One warp per row.
+// unordered pair is written once.  Value sign * (K - w^2 M + i w D): sign = -1 gives the Krylov
+// process's K~, +1 the full-order dynamic stiffness.  One warp per row.
 __global__ void scatter_band_kernel(int64_t n, const int64_t *__restrict__ rp, const int *__restrict__ ci,
                                     const int64_t *__restrict__ vmap, const double2 *__restrict__ K,
                                     const double2 *__restrict__ M, const double2 *__restrict__ D, double w,
-                                    const int *__restrict__ iperm, double2 *__restrict__ band, int64_t ldab) {
+                                    double sign, const int *__restrict__ iperm, double2 *__restrict__ band,
+                                    int64_t ldab) {
     const int lane = threadIdx.x & 31;
     const double w2 = w * w;
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n;
@@ -84,7 +86,7 @@ __global__ void scatter_band_kernel(int64_t n, const int64_t *__restrict__ rp, c
                 re -= w * d.y;
                 im += w * d.x;
             }
-            band[(int64_t)pj * ldab + (pi - pj + NB)] = make_double2(-re, -im);
+            band[(int64_t)pj * ldab + (pi - pj + NB)] = make_double2(sign * re, sign * im);
         }
     }
 }
@@ -694,91 +696,73 @@ int pivoted_qr(cudaStream_t st, double2 *A, int64_t n, int m, double tol, double
 
 }  // namespace
 
-int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *log) {
-    Err E;
-    cudaStream_t st = a.stream;
-    const int64_t n = a.n_rows;
-    *n_cols = 0;
-    if (log) log->blocks.clear();
-    if (n == 0 || a.n_in == 0 || a.n_points == 0) return SROM_OK;
-    // host copies of the pattern: full symmetric pattern and RCM order
-    std::vector<int64_t> rp(n + 1);
-    std::vector<int> ci(a.nnz);
-    {
-        cudaError_t e = cudaMemcpyAsync(rp.data(), a.rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess && a.nnz > 0)
-            e = cudaMemcpyAsync(ci.data(), a.colind, sizeof(int) * a.nnz, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) {
-            *msg = std::string("copying the pattern to the host: ") + cudaGetErrorString(e);
-            return SROM_ERR_CUDA;
-        }
-    }
-    if (rp[0] != a.base || rp[n] - a.base != a.nnz) {
-        *msg = "rowptr does not start at base or does not end at base + nnz";
-        return SROM_ERR_INVALID;
-    }
-    std::vector<int64_t> frp, fmap;
-    std::vector<int> fci, perm;
-    {
-        std::string err;
-        int s = full_pattern(n, a.nnz, rp.data(), ci.data(), a.base, a.upper, frp, fci, fmap, &err);
-        if (s) {
-            *msg = err;
-            return s;
-        }
-    }
-    const int64_t bw = rcm_order(n, frp, fci, perm);
-    std::vector<int> iperm(n);
-    for (int64_t k = 0; k < n; ++k) iperm[perm[k]] = (int)k;
-    if (log) log->bandwidth = bw;
+namespace {
 
+// The factorisation context shared by the Krylov basis and the full-order sweep: the pattern
+// (full symmetric, on host and device), its RCM order, the band factor and its panels, and a
+// cuBLAS handle on the caller's stream.  Members are released in reverse order: the cuBLAS
+// handle (after the stream drains), then the device buffers.
+struct BandContext {
     Bufs B;
-    B.st = st;
-    BandLDLT F;
-    F.n = n;
-    F.bw = bw;
-    F.ldab = bw + 2 * NB + 1;
-    F.ldw = (int)(2 * bw + NB);
-    F.st = st;
+    struct CbGuard {
+        cublasHandle_t h = nullptr;
+        cudaStream_t st = nullptr;
+        ~CbGuard() {
+            if (h) {
+                cudaStreamSynchronize(st);  // nothing queued may still use the handle's workspace
+                cublasDestroy(h);
+            }
+        }
+    } cbg;
+    cudaStream_t st = nullptr;
+    int64_t n = 0;
+    std::vector<int64_t> frp, fmap;
+    std::vector<int> fci, perm, iperm;
     int64_t *d_frp = nullptr, *d_fmap = nullptr;
     int *d_fci = nullptr, *d_iperm = nullptr;
-    const int mmax = std::max(a.n_in, 1);
-    double2 *Q = nullptr, *U = nullptr, *Qo = nullptr, *S = nullptr, *d_w = nullptr;
-    double *d_norms = nullptr;
-    auto need = [&](cudaError_t e, const char *what) {
-        if (e != cudaSuccess) E.set(e == cudaErrorMemoryAllocation ? SROM_ERR_ALLOC : SROM_ERR_CUDA,
-                                    std::string("allocating ") + what + ": " + cudaGetErrorString(e));
-        return e == cudaSuccess;
-    };
-    if (!need(B.alloc(&F.band, (size_t)(n + 2 * NB) * F.ldab), "the band factor") ||
-        !need(B.alloc(&F.W, (size_t)F.ldw * NB), "the panel") || !need(B.alloc(&F.Lp, (size_t)F.ldw * NB), "the panel") ||
-        !need(B.alloc(&F.d_info, 1), "info") || !need(B.alloc(&d_frp, n + 1), "the pattern") ||
-        !need(B.alloc(&d_fci, frp[n]), "the pattern") || !need(B.alloc(&d_fmap, frp[n]), "the pattern") ||
-        !need(B.alloc(&d_iperm, n), "the ordering") || !need(B.alloc(&Q, (size_t)n * mmax), "the block") ||
-        !need(B.alloc(&U, (size_t)n * mmax), "the block") || !need(B.alloc(&Qo, (size_t)n * mmax), "the block") ||
-        !need(B.alloc(&S, (size_t)std::max(a.max_cols, 1) * mmax), "the block") ||
-        !need(B.alloc(&d_w, mmax), "the block") || !need(B.alloc(&d_norms, mmax), "the block")) {
-        *msg = E.msg;
-        return E.code;
-    }
-    cublasHandle_t cb = nullptr;
-    if (cublasCreate(&cb) != CUBLAS_STATUS_SUCCESS) {
-        *msg = "cublasCreate failed";
-        return SROM_ERR_CUDA;
-    }
-    struct CbGuard {
-        cublasHandle_t h;
-        cudaStream_t st;
-        ~CbGuard() {
-            cudaStreamSynchronize(st);  // nothing queued may still use the handle's workspace
-            cublasDestroy(h);
-        }
-    } cbg{cb, st};
-    F.cb = cb;
-    auto run = [&]() -> int {
-        KBL(cublasSetStream(cb, st));
-        KBL(cublasSetPointerMode(cb, CUBLAS_POINTER_MODE_HOST));
+    BandLDLT F;
+
+    int init(cudaStream_t stream, int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind, int base,
+             int upper, Err &E) {
+        st = stream;
+        n = n_rows;
+        B.st = st;
+        std::vector<int64_t> rp(n + 1);
+        std::vector<int> ci(nnz);
+        KCU(cudaMemcpyAsync(rp.data(), rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+        if (nnz > 0) KCU(cudaMemcpyAsync(ci.data(), colind, sizeof(int) * nnz, cudaMemcpyDeviceToHost, st));
+        KCU(cudaStreamSynchronize(st));
+        if (rp[0] != base || rp[n] - base != nnz)
+            return E.set(SROM_ERR_INVALID, "rowptr does not start at base or does not end at base + nnz");
+        std::string err;
+        int s = full_pattern(n, nnz, rp.data(), ci.data(), base, upper, frp, fci, fmap, &err);
+        if (s) return E.set(s, err);
+        const int64_t bw = rcm_order(n, frp, fci, perm);
+        iperm.assign(n, 0);
+        for (int64_t k = 0; k < n; ++k) iperm[perm[k]] = (int)k;
+        F.n = n;
+        F.bw = bw;
+        F.ldab = bw + 2 * NB + 1;
+        F.ldw = (int)(2 * bw + NB);
+        F.st = st;
+        auto need = [&](cudaError_t e, const char *what) {
+            if (e != cudaSuccess)
+                E.set(e == cudaErrorMemoryAllocation ? SROM_ERR_ALLOC : SROM_ERR_CUDA,
+                      std::string("allocating ") + what + " (" + std::to_string(band_bytes(n, bw)) +
+                          " bytes for the band): " + cudaGetErrorString(e));
+            return e == cudaSuccess;
+        };
+        if (!need(B.alloc(&F.band, (size_t)(n + 2 * NB) * F.ldab), "the band factor") ||
+            !need(B.alloc(&F.W, (size_t)F.ldw * NB), "the panel") ||
+            !need(B.alloc(&F.Lp, (size_t)F.ldw * NB), "the panel") || !need(B.alloc(&F.d_info, 1), "info") ||
+            !need(B.alloc(&d_frp, n + 1), "the pattern") || !need(B.alloc(&d_fci, frp[n]), "the pattern") ||
+            !need(B.alloc(&d_fmap, frp[n]), "the pattern") || !need(B.alloc(&d_iperm, n), "the ordering"))
+            return E.code;
+        if (cublasCreate(&cbg.h) != CUBLAS_STATUS_SUCCESS) return E.set(SROM_ERR_CUDA, "cublasCreate failed");
+        cbg.st = st;
+        F.cb = cbg.h;
+        KBL(cublasSetStream(cbg.h, st));
+        KBL(cublasSetPointerMode(cbg.h, CUBLAS_POINTER_MODE_HOST));
         const size_t smem = sizeof(double2) * NB * SLD;
         KCU(cudaFuncSetAttribute(ldlt_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         KCU(cudaFuncSetAttribute(ldlt_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -789,33 +773,74 @@ int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *
         KCU(cudaMemcpyAsync(d_iperm, iperm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
         KCU(cudaMemsetAsync(F.W, 0, sizeof(double2) * F.ldw * NB, st));
         KCU(cudaMemsetAsync(F.Lp, 0, sizeof(double2) * F.ldw * NB, st));
+        return SROM_OK;
+    }
+
+    // sign * (K - w^2 M + i w D) into the band, then L D L^T
+    int assemble_factor(const void *K, const void *M, const void *D, double w, double sign, Err &E) {
+        KCU(cudaMemsetAsync(F.band, 0, sizeof(double2) * (size_t)(n + 2 * NB) * F.ldab, st));
+        scatter_band_kernel<<<grid_for(n * 32, KT), KT, 0, st>>>(
+            n, d_frp, d_fci, d_fmap, reinterpret_cast<const double2 *>(K), reinterpret_cast<const double2 *>(M),
+            reinterpret_cast<const double2 *>(D), w, sign, d_iperm, F.band, F.ldab);
+        KCU(cudaGetLastError());
+        return F.factor(E);
+    }
+
+    // Y (n x m, ldy) = A^-1 X (n x m, ldx) with the current factor; work: n x m scratch
+    int solve(const double2 *X, int64_t ldx, double2 *Y, int64_t ldy, int m, double2 *work, Err &E) {
+        permute_kernel<<<grid_for(n * m, KT), KT, 0, st>>>(n, m, d_iperm, X, ldx, work, n, 1);
+        int s = F.solve(work, n, m, E);
+        if (s) return s;
+        permute_kernel<<<grid_for(n * m, KT), KT, 0, st>>>(n, m, d_iperm, work, n, Y, ldy, 0);
+        KCU(cudaGetLastError());
+        return SROM_OK;
+    }
+};
+
+}  // namespace
+
+int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *log) {
+    Err E;
+    *n_cols = 0;
+    if (log) log->blocks.clear();
+    if (a.n_rows == 0 || a.n_in == 0 || a.n_points == 0) return SROM_OK;
+    BandContext X;
+    if (X.init(a.stream, a.n_rows, a.nnz, a.rowptr, a.colind, a.base, a.upper, E)) {
+        *msg = E.msg;
+        return E.code;
+    }
+    if (log) log->bandwidth = X.F.bw;
+    cudaStream_t st = a.stream;
+    const int64_t n = a.n_rows;
+    const int mmax = std::max(a.n_in, 1);
+    double2 *Q = nullptr, *U = nullptr, *Qo = nullptr, *S = nullptr, *d_w = nullptr, *work = nullptr;
+    double *d_norms = nullptr;
+    for (auto e : {X.B.alloc(&Q, (size_t)n * mmax), X.B.alloc(&U, (size_t)n * mmax), X.B.alloc(&Qo, (size_t)n * mmax),
+                   X.B.alloc(&work, (size_t)n * mmax), X.B.alloc(&S, (size_t)std::max(a.max_cols, 1) * mmax),
+                   X.B.alloc(&d_w, mmax), X.B.alloc(&d_norms, mmax)})
+        if (e != cudaSuccess) {
+            *msg = std::string("allocating the Krylov blocks: ") + cudaGetErrorString(e);
+            return e == cudaErrorMemoryAllocation ? SROM_ERR_ALLOC : SROM_ERR_CUDA;
+        }
+    cublasHandle_t cb = X.cbg.h;
+    auto run = [&]() -> int {
         int kv = 0;  // columns of V so far
         std::vector<double> rdiag;
         for (int ip = 0; ip < a.n_points; ++ip) {
             const double w = 2.0 * 3.141592653589793 * a.exp_points_hz[ip];
-            KCU(cudaMemsetAsync(F.band, 0, sizeof(double2) * (size_t)(n + 2 * NB) * F.ldab, st));
-            scatter_band_kernel<<<grid_for(n * 32, KT), KT, 0, st>>>(
-                n, d_frp, d_fci, d_fmap, reinterpret_cast<const double2 *>(a.K), reinterpret_cast<const double2 *>(a.M),
-                reinterpret_cast<const double2 *>(a.D), w, d_iperm, F.band, F.ldab);
-            KCU(cudaGetLastError());
-            int s = F.factor(E);
+            // K~ = -(K - w^2 M + i w D)
+            int s = X.assemble_factor(a.K, a.M, a.D, w, -1.0, E);
             if (s) return s;
-            // Q = K~^-1 B
             int m = a.n_in;
-            permute_kernel<<<grid_for(n * m, KT), KT, 0, st>>>(n, m, d_iperm, reinterpret_cast<const double2 *>(a.B),
-                                                               a.ldb, U, n, 1);
-            s = F.solve(U, n, m, E);
+            s = X.solve(reinterpret_cast<const double2 *>(a.B), a.ldb, Q, n, m, work, E);  // Q = K~^-1 B
             if (s) return s;
-            permute_kernel<<<grid_for(n * m, KT), KT, 0, st>>>(n, m, d_iperm, U, n, Q, n, 0);
             for (int order = 1; order <= a.order; ++order) {
                 if (order > 1) {
                     // Q = K~^-1 (M Q)
                     csr_spmm_complex_kernel<<<grid_for(n * 32, KT), KT, 0, st>>>(
-                        n, d_frp, d_fci, d_fmap, reinterpret_cast<const double2 *>(a.M), Qo, n, m, Q, n);
-                    permute_kernel<<<grid_for(n * m, KT), KT, 0, st>>>(n, m, d_iperm, Q, n, U, n, 1);
-                    s = F.solve(U, n, m, E);
+                        n, X.d_frp, X.d_fci, X.d_fmap, reinterpret_cast<const double2 *>(a.M), Qo, n, m, U, n);
+                    s = X.solve(U, n, Q, n, m, work, E);
                     if (s) return s;
-                    permute_kernel<<<grid_for(n * m, KT), KT, 0, st>>>(n, m, d_iperm, U, n, Q, n, 0);
                 }
                 if (ip > 0 || order > 1) {
                     s = reorthogonalize(cb, st, reinterpret_cast<const double2 *>(a.V), a.ldv, kv, Q, U, n, m, S, E);
@@ -837,6 +862,37 @@ int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *
             }
         }
         KCU(cudaStreamSynchronize(st));
+        return SROM_OK;
+    };
+    const int s = run();
+    if (s) *msg = E.msg;
+    return s;
+}
+
+int fom_sweep(const FomArgs &a, std::string *msg) {
+    Err E;
+    if (a.n_rows == 0 || a.r == 0 || a.n_freq == 0) return SROM_OK;
+    BandContext X;
+    if (X.init(a.stream, a.n_rows, a.nnz, a.rowptr, a.colind, a.base, a.upper, E)) {
+        *msg = E.msg;
+        return E.code;
+    }
+    double2 *work = nullptr;
+    cudaError_t e = X.B.alloc(&work, (size_t)a.n_rows * a.r);
+    if (e != cudaSuccess) {
+        *msg = std::string("allocating the solve block: ") + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? SROM_ERR_ALLOC : SROM_ERR_CUDA;
+    }
+    auto run = [&]() -> int {
+        for (int f = 0; f < a.n_freq; ++f) {
+            const double w = 2.0 * 3.141592653589793 * a.freq_hz[f];
+            int s = X.assemble_factor(a.K, a.M, a.D, w, 1.0, E);  // K - w^2 M + i w D
+            if (s) return E.set(s, "frequency " + std::to_string(f) + ": " + E.msg);
+            double2 *Xf = reinterpret_cast<double2 *>(a.X) + (int64_t)f * a.ldx * a.r;
+            s = X.solve(reinterpret_cast<const double2 *>(a.F), a.ldf, Xf, a.ldx, a.r, work, E);
+            if (s) return s;
+        }
+        KCU(cudaStreamSynchronize(a.stream));
         return SROM_OK;
     };
     const int s = run();

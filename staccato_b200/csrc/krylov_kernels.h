@@ -41,6 +41,25 @@ struct KrylovLog {
 
 int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *log);
 
+struct FomArgs {
+    cudaStream_t stream;
+    int64_t n_rows, nnz;
+    const int64_t *rowptr;  // device CSR as in KrylovArgs
+    const int *colind;
+    int base, upper;
+    const void *K, *M, *D;  // device values; D may be null
+    const void *F;          // device n_rows x r loads, leading dimension ldf
+    int r;
+    int64_t ldf;
+    const double *freq_hz;  // host
+    int n_freq;
+    void *X;  // device: n_freq blocks of n_rows x r (leading dimension ldx, block stride ldx * r)
+    int64_t ldx;
+};
+
+// (K - w^2 M + i w D) X_f = F for every frequency: band LDL^T per frequency.
+int fom_sweep(const FomArgs &a, std::string *msg);
+
 // host helpers (also behind srom_band_order)
 int full_pattern(int64_t n, int64_t nnz, const int64_t *rp, const int *ci, int base, int upper, std::vector<int64_t> &frp,
                  std::vector<int> &fci, std::vector<int64_t> &fmap, std::string *err);

@@ -48,6 +48,25 @@ def krylov_basis(handle: _capi.Handle, csr: DeviceCsr, K, M, D, B, exp_points_hz
     return V[: ncols.value].contiguous()
 
 
+def fom_sweep(handle: _capi.Handle, csr: DeviceCsr, K, M, D, F, freq_hz: Sequence[float]):
+    """Full-order responses (performSolveFOM, KrylovROMSubstructure.cpp:1355-1391): X_f solving
+    (K - w^2 M + i w D) X_f = F per frequency, as a (n_freq, r, n_rows) complex128 tensor (each
+    [f] is n_rows x r column-major).  F: contiguous (r, n_rows) complex128 device tensor."""
+    import torch
+
+    n = csr.n_rows
+    r = int(F.shape[0])
+    assert int(F.shape[1]) == n and F.is_contiguous() and F.dtype == torch.complex128
+    f = np.ascontiguousarray(freq_hz, dtype=np.float64)
+    X = torch.empty((len(f), r, n), dtype=torch.complex128, device=F.device)
+    check(handle.ptr, _capi.lib().srom_fom_sweep(
+        handle.ptr, n, int(K.numel()), C.c_void_p(csr.rowptr.data_ptr()), C.c_void_p(csr.colind.data_ptr()),
+        csr.base, int(csr.upper), C.c_void_p(K.data_ptr()), C.c_void_p(M.data_ptr()),
+        None if D is None else C.c_void_p(D.data_ptr()), C.c_void_p(F.data_ptr()), r, n,
+        f.ctypes.data_as(C.c_void_p), len(f), C.c_void_p(X.data_ptr()), n))
+    return X
+
+
 def band_order(indptr, indices, base: int = 0, upper: bool = False):
     """(perm, bandwidth, band_bytes) of the reverse Cuthill-McKee ordering of a host CSR pattern:
     perm[k] = original row of row k."""

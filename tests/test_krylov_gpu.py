@@ -184,3 +184,33 @@ def test_rom_interface_generates_basis_then_rom(handle, problem):
     w = 2 * math.pi * f
     y_full = C @ spla.spsolve((K - w * w * M + 1j * w * D).tocsc(), B)
     assert np.linalg.norm(y - y_full) <= 1e-8 * np.linalg.norm(y_full)
+
+
+def test_fom_sweep_matches_sparse_direct_solve(handle, problem):
+    """srom_fom_sweep (performSolveFOM): each frequency's full-order solve against SuperLU,
+    near resonance included, full and upper storage, with and without damping."""
+    import torch
+
+    from staccato_b200.krylov import fom_sweep
+
+    K, M, D, f1 = problem
+    N = K.shape[0]
+    rng = np.random.default_rng(21)
+    F = rng.standard_normal((N, 2)) + 1j * rng.standard_normal((N, 2))
+    freqs = [0.0, 0.3 * f1, 0.999 * f1, 1.7 * f1, 4.0 * f1]
+    for Dm, upper in ((D, False), (D, True), (None, False)):
+        mats = (M,) if Dm is None else (M, Dm)
+        if upper:
+            indptr, indices, data = _upper(K, *mats)
+        else:
+            indptr, indices, data = K.indptr, K.indices, [K.data] + [m.data for m in mats]
+        csr = DeviceCsr.from_host(indptr, indices, upper=upper)
+        X = fom_sweep(handle, csr, _dev(torch, data[0]), _dev(torch, data[1]),
+                      None if Dm is None else _dev(torch, data[2]), _dev(torch, F.T), freqs)
+        X = X.cpu().numpy()
+        for i, f in enumerate(freqs):
+            w = 2 * math.pi * f
+            A = K - w * w * M + (0 if Dm is None else 1j * w * Dm)
+            ref = spla.spsolve(sp.csc_matrix(A), F)
+            err = np.linalg.norm(X[i].T - ref) / np.linalg.norm(ref)
+            assert err <= 1e-9, (f / f1, upper, Dm is None, err)
