@@ -611,6 +611,7 @@ def run_ours(args):
             "projection": extras.get("projection"),
             "adjoint": extras.get("adjoint"),
             "workloads": extras.get("workloads"),
+            "krylov": extras.get("krylov"),
         }
         print(json.dumps(line), flush=True)
     if pg is not None:
