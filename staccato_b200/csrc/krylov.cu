@@ -93,31 +93,39 @@ __global__ void scatter_band_kernel(int64_t n, const int64_t *__restrict__ rp, c
 
 // ---- blocked LDL^T ------------------------------------------------------------------------
 // The nb x nb diagonal block at column j0: A11 = L11 D L11^T (unit L11, no pivoting), in place
-// (D on the diagonal).  The first exactly-zero pivot is recorded 1-based in *info.
+// (D on the diagonal).  The block is held whole (both triangles) in shared memory; step k
+// updates a_ij -= a_ik (a_kj / d_k) for i, j > k, each thread owning one column j (its row
+// entries are contiguous across the warp) and every fourth row, so a step needs one barrier.
+// The columns are scaled by 1/d_k once at the end.  The first exactly-zero pivot is recorded
+// 1-based in *info.
 __global__ void __launch_bounds__(KT) ldlt_diag_kernel(double2 *__restrict__ band, int64_t ldab, int64_t j0, int nb,
                                                        int *__restrict__ info) {
-    extern __shared__ double2 S[];  // S[i * SLD + j], i >= j
+    extern __shared__ double2 S[];  // S[i * SLD + j], full symmetric block
+    constexpr int RS = KT / NB;     // row stride of a thread
     const int t = threadIdx.x;
     for (int e = t; e < nb * nb; e += KT) {
-        const int i = e % nb, j = e / nb;
-        if (i >= j) S[i * SLD + j] = band[(j0 + j) * ldab + (i - j + NB)];
+        const int i = e / nb, j = e % nb;
+        const int r = max(i, j), c = min(i, j);
+        S[i * SLD + j] = band[(j0 + c) * ldab + (r - c + NB)];
     }
     __syncthreads();
+    const int j = t % NB, ir = t / NB;
     for (int k = 0; k < nb; ++k) {
         const double2 d = S[k * SLD + k];
         if (t == 0 && d.x == 0.0 && d.y == 0.0) atomicCAS(info, 0, (int)(j0 + k + 1));
-        for (int i = k + 1 + t; i < nb; i += KT) S[i * SLD + k] = cdiv(S[i * SLD + k], d);
-        __syncthreads();
-        const int m = nb - k - 1;
-        for (int e = t; e < m * m; e += KT) {
-            const int i = k + 1 + e % m, j = k + 1 + e / m;
-            if (i >= j) S[i * SLD + j] = cfms(S[i * SLD + j], cmul(S[i * SLD + k], d), S[j * SLD + k]);
+        if (j > k && j < nb) {
+            const double2 cj = cdiv(S[k * SLD + j], d);
+            for (int i = k + 1 + ((ir - (k + 1)) % RS + RS) % RS; i < nb; i += RS)
+                S[i * SLD + j] = cfms(S[i * SLD + j], S[i * SLD + k], cj);
         }
         __syncthreads();
     }
     for (int e = t; e < nb * nb; e += KT) {
-        const int i = e % nb, j = e / nb;
-        if (i >= j) band[(j0 + j) * ldab + (i - j + NB)] = S[i * SLD + j];
+        const int i = e % nb, c = e / nb;
+        if (i > c)
+            band[(j0 + c) * ldab + (i - c + NB)] = cdiv(S[i * SLD + c], S[c * SLD + c]);
+        else if (i == c)
+            band[(j0 + c) * ldab + NB] = S[c * SLD + c];
     }
 }
 
