@@ -56,6 +56,11 @@ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
     const double r = b.x / b.y, den = b.y + b.x * r;
     return make_double2((a.x * r + a.y) / den, (a.y * r - a.x) / den);
 }
+// 1 / b = conj(b) / |b|^2 (one division; this solver carries no bit-exactness contract)
+__device__ __forceinline__ double2 crecip(double2 b) {
+    const double s = 1.0 / fma(b.x, b.x, b.y * b.y);
+    return make_double2(b.x * s, -b.y * s);
+}
 __device__ __forceinline__ double2 shfl2(double2 v, int src) {
     return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
@@ -114,7 +119,7 @@ __global__ void __launch_bounds__(KT) ldlt_diag_kernel(double2 *__restrict__ ban
         const double2 d = S[k * SLD + k];
         if (t == 0 && d.x == 0.0 && d.y == 0.0) atomicCAS(info, 0, (int)(j0 + k + 1));
         if (j > k && j < nb) {
-            const double2 cj = cdiv(S[k * SLD + j], d);
+            const double2 cj = cmul(S[k * SLD + j], crecip(d));
             for (int i = k + 1 + ((ir - (k + 1)) % RS + RS) % RS; i < nb; i += RS)
                 S[i * SLD + j] = cfms(S[i * SLD + j], S[i * SLD + k], cj);
         }
@@ -123,7 +128,7 @@ __global__ void __launch_bounds__(KT) ldlt_diag_kernel(double2 *__restrict__ ban
     for (int e = t; e < nb * nb; e += KT) {
         const int i = e % nb, c = e / nb;
         if (i > c)
-            band[(j0 + c) * ldab + (i - c + NB)] = cdiv(S[i * SLD + c], S[c * SLD + c]);
+            band[(j0 + c) * ldab + (i - c + NB)] = cmul(S[i * SLD + c], crecip(S[c * SLD + c]));
         else if (i == c)
             band[(j0 + c) * ldab + NB] = S[c * SLD + c];
     }
@@ -145,8 +150,11 @@ __device__ __forceinline__ void load_l11(const double2 *band, int64_t ldab, int6
 __global__ void __launch_bounds__(KT) ldlt_panel_kernel(double2 *__restrict__ band, int64_t ldab, int64_t j0, int nb,
                                                         int rows, int zero_to, double2 *__restrict__ W,
                                                         double2 *__restrict__ Lp, int ldw) {
-    extern __shared__ double2 S[];
+    extern __shared__ double2 S[];  // L11 (NB x SLD) then 1/d (NB)
+    double2 *Dinv = S + NB * SLD;
     load_l11(band, ldab, j0, nb, S);
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) Dinv[k] = crecip(S[k * SLD + k]);
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int t = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     if (t >= zero_to) return;
@@ -179,7 +187,7 @@ __global__ void __launch_bounds__(KT) ldlt_panel_kernel(double2 *__restrict__ ba
             double2 l = make_double2(0.0, 0.0), wv = make_double2(0.0, 0.0);
             if (k < nb) {
                 wv = x[h];
-                l = cdiv(x[h], S[k * SLD + k]);
+                l = cmul(x[h], Dinv[k]);
                 band[(j0 + k) * ldab + (r - (j0 + k) + NB)] = l;
             }
             W[t + (int64_t)k * ldw] = wv;
@@ -569,8 +577,8 @@ struct BandLDLT {
             if (rows <= 0) continue;
             const int zero_to = std::max(rows, prev_rows);
             prev_rows = rows;
-            ldlt_panel_kernel<<<(zero_to + KT / 32 - 1) / (KT / 32), KT, smem, st>>>(band, ldab, j0, nb, rows, zero_to, W,
-                                                                                     Lp, ldw);
+            ldlt_panel_kernel<<<(zero_to + KT / 32 - 1) / (KT / 32), KT, smem + sizeof(double2) * NB, st>>>(
+                band, ldab, j0, nb, rows, zero_to, W, Lp, ldw);
             const int batches = (rows + NB - 1) / NB;
             double2 *C0 = band + (j0 + nb) * ldab + NB;
             KBL(cublasZgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_T, rows, NB, nb, &mone,
@@ -773,7 +781,8 @@ struct BandContext {
         KBL(cublasSetPointerMode(cbg.h, CUBLAS_POINTER_MODE_HOST));
         const size_t smem = sizeof(double2) * NB * SLD;
         KCU(cudaFuncSetAttribute(ldlt_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        KCU(cudaFuncSetAttribute(ldlt_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        KCU(cudaFuncSetAttribute(ldlt_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(smem + sizeof(double2) * NB)));
         KCU(cudaFuncSetAttribute(trsv_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         KCU(cudaMemcpyAsync(d_frp, frp.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
         KCU(cudaMemcpyAsync(d_fci, fci.data(), sizeof(int) * frp[n], cudaMemcpyHostToDevice, st));
