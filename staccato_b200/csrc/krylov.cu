@@ -441,6 +441,11 @@ int grid_for(int64_t work, int threads) {
 int full_pattern(int64_t n, int64_t nnz, const int64_t *rp, const int *ci, int base, int upper, std::vector<int64_t> &frp,
                  std::vector<int> &fci, std::vector<int64_t> &fmap, std::string *err) {
     frp.assign(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i)
+        if (rp[i + 1] < rp[i] || rp[i + 1] - base > nnz) {
+            if (err) *err = "rowptr decreases or passes nnz at row " + std::to_string(i);
+            return SROM_ERR_INVALID;
+        }
     for (int64_t i = 0; i < n; ++i) {
         for (int64_t e = rp[i] - base; e < rp[i + 1] - base; ++e) {
             const int64_t j = (int64_t)ci[e] - base;
@@ -470,7 +475,6 @@ int full_pattern(int64_t n, int64_t nnz, const int64_t *rp, const int *ci, int b
                 fmap[pos[j]++] = e;
             }
         }
-    (void)nnz;
     return SROM_OK;
 }
 

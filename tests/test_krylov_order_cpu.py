@@ -66,6 +66,11 @@ def test_bad_patterns_are_rejected():
     with pytest.raises(_capi.SromError) as e:
         band_order(A.indptr, bad)
     assert e.value.status == _capi.SROM_ERR_INVALID
+    rp = A.indptr.copy()
+    rp[5], rp[6] = rp[6], rp[5]  # a row pointer that decreases (ends still right)
+    with pytest.raises(_capi.SromError) as e:
+        band_order(rp, A.indices)
+    assert "rowptr" in str(e.value)
     L = sp.tril(A).tocsr()  # lower triangle passed as upper storage
     with pytest.raises(_capi.SromError):
         band_order(L.indptr, L.indices, upper=True)
