@@ -1,7 +1,7 @@
 """CPU restatement of the Krylov basis generation -- TEST INFRASTRUCTURE ONLY.
 
-Only tests/ (and bench.py's CPU leg) import this module, to check or time the GPU basis
-generation; the product path never does.
+Only tests/ import this module, to check the GPU basis generation; the product path never
+does.
 
 It restates ``KrylovROMSubstructure::addKrylovModesForExpansionPoint``
 (src/analysis/KrylovROMSubstructure.cpp:367-569), the block Arnoldi process with block

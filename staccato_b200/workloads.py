@@ -2,7 +2,7 @@
 
 The reference ships no ROM files (its tests read ``KSM_*_r{21,189,2520}.mtx`` from
 ``/opt/software/examples/MOR/``, which are not part of the project), so every sweep input
-here is generated from a seed.  The shapes follow the five workloads the sweep is judged on:
+here is generated from a seed.  The shapes follow the five workloads the sweep is measured on:
 
 * ``plain_rom``       n=64, hysteretic damping eta=0.02, 500 frequencies 1..1000 Hz, 1 RHS.
 * ``precision_rom``   n=256, eta=0.01 + Rayleigh damping D = 1e-5 K + 2 M, 4096 frequencies of
