@@ -48,13 +48,15 @@ def reorthogonalize(V: Optional[np.ndarray], Q: np.ndarray) -> np.ndarray:
         return Q
     eta = 1.0 / math.sqrt(2.0)
     qk_ = Q
-    while True:
+    for _ in range(64):  # the GPU path's cap; a zero block (ratio NaN) also ends the loop
         sk = V.conj().T @ qk_
         uk = qk_ - V @ sk
-        lim = np.linalg.norm(uk) / np.linalg.norm(qk_)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            lim = np.linalg.norm(uk) / np.linalg.norm(qk_)
         qk_ = uk
-        if lim > eta:
+        if not lim <= eta:
             return uk
+    return qk_
 
 
 def rank_revealing_q(Q: np.ndarray, tol: float):
