@@ -97,3 +97,15 @@ def test_noalloc_rejects_misaligned_arrays_before_any_cuda_call():
     d = desc()  # aligned: gets past the check and fails only for want of a device
     st = _capi.lib().srom_sweep_fp64_noalloc(C.byref(d), None, err, 256)
     assert st == _capi.SROM_ERR_CUDA, err.value
+
+
+def test_null_handle_is_rejected_by_every_handle_call():
+    """Calls that take a handle return SROM_ERR_INVALID for a null one (no CUDA call made)."""
+    L = _capi.lib()
+    n_cols = C.c_int(-1)
+    assert L.srom_krylov_basis(None, 4, 4, None, None, 0, 0, None, None, None, None, 1, 4, None, 1, 1, 0.0,
+                               None, 4, 4, C.byref(n_cols)) == _capi.SROM_ERR_INVALID
+    assert L.srom_fom_sweep(None, 4, 4, None, None, 0, 0, None, None, None, None, 1, 4, None, 1, None,
+                            4) == _capi.SROM_ERR_INVALID
+    assert L.srom_sweep(None, None, 0, None) == _capi.SROM_ERR_INVALID
+    assert L.srom_orthonormalize(None, None, 4, 1, 4, 2) == _capi.SROM_ERR_INVALID
