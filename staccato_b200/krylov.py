@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _capi
 from ._capi import check
-from .project import DeviceCsr
+from .project import DeviceCsr, _on_device
 
 
 def krylov_basis(handle: _capi.Handle, csr: DeviceCsr, K, M, D, B, exp_points_hz: Sequence[float], order: int,
@@ -32,6 +32,7 @@ def krylov_basis(handle: _capi.Handle, csr: DeviceCsr, K, M, D, B, exp_points_hz
     assert int(B.shape[1]) == n and B.is_contiguous() and B.dtype == torch.complex128
     for v in (K, M) + ((D,) if D is not None else ()):
         assert v.dtype == torch.complex128 and v.is_contiguous()
+    _on_device(B, K, M, *((D,) if D is not None else ()), csr.rowptr, csr.colind)
     pts = np.ascontiguousarray(exp_points_hz, dtype=np.float64)
     if max_cols is None:
         max_cols = n_in * max(order, 1) * max(len(pts), 1)
@@ -57,6 +58,7 @@ def fom_sweep(handle: _capi.Handle, csr: DeviceCsr, K, M, D, F, freq_hz: Sequenc
     n = csr.n_rows
     r = int(F.shape[0])
     assert int(F.shape[1]) == n and F.is_contiguous() and F.dtype == torch.complex128
+    _on_device(F, K, M, *((D,) if D is not None else ()), csr.rowptr, csr.colind)
     f = np.ascontiguousarray(freq_hz, dtype=np.float64)
     X = torch.empty((len(f), r, n), dtype=torch.complex128, device=F.device)
     check(handle.ptr, _capi.lib().srom_fom_sweep(

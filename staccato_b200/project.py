@@ -34,6 +34,13 @@ class DeviceCsr:
         return cls(n_rows=len(indptr) - 1, rowptr=rp, colind=ci, base=base, upper=upper)
 
 
+def _on_device(*tensors) -> None:
+    """The C ABI takes device pointers: refuse host tensors before anything is launched."""
+    for t in tensors:
+        if not getattr(t, "is_cuda", False):
+            raise ValueError("expected CUDA tensors (the C ABI takes device pointers)")
+
+
 def project(handle: _capi.Handle, csr: DeviceCsr, values: Sequence, V) -> List:
     """R_m = V^T A_m V (k x k, returned as torch float64 tensors in column-major order).
 
@@ -45,6 +52,7 @@ def project(handle: _capi.Handle, csr: DeviceCsr, values: Sequence, V) -> List:
     Vt = V  # (k, n_rows) row-major == n_rows x k column-major
     k, n = int(Vt.shape[0]), int(Vt.shape[1])
     assert n == csr.n_rows and Vt.is_contiguous() and Vt.dtype == torch.float64
+    _on_device(Vt, *values)
     outs = [torch.empty((k, k), dtype=torch.float64, device=Vt.device) for _ in values]
     vals = (C.c_void_p * len(values))(*[C.c_void_p(v.data_ptr()) for v in values])
     rs = (C.c_void_p * len(values))(*[C.c_void_p(o.data_ptr()) for o in outs])
@@ -64,6 +72,7 @@ def project_complex(handle: _capi.Handle, csr: DeviceCsr, values: Sequence, V, Z
 
     k, n = int(V.shape[0]), int(V.shape[1])
     assert n == csr.n_rows and V.is_contiguous() and V.dtype == torch.complex128
+    _on_device(V, *values, *((Z,) if Z is not None else ()))
     if Z is not None:
         assert tuple(Z.shape) == (k, n) and Z.is_contiguous() and Z.dtype == torch.complex128
     nnz = int(values[0].numel())

@@ -74,12 +74,13 @@ class KrylovROMSubstructure:
         complex_form = V.dtype == torch.complex128 or any(torch.as_tensor(a).is_complex() for a in mats)
         if complex_form:
             Vc = V.to(torch.complex128).contiguous()
-            R = project_complex(self.handle, csr, [torch.as_tensor(a).to(torch.complex128).contiguous() for a in mats],
-                                Vc)
+            R = project_complex(self.handle, csr,
+                                [torch.as_tensor(a).to(device=V.device, dtype=torch.complex128).contiguous()
+                                 for a in mats], Vc)
             to_c = lambda r: r
         else:
             Vc = V
-            R = project(self.handle, csr, mats, V)
+            R = project(self.handle, csr, [torch.as_tensor(a).to(device=V.device) for a in mats], V)
             to_c = lambda r: r.to(torch.complex128)
         self.K_r, self.M_r = to_c(R[0]), to_c(R[1])
         self.D_r = to_c(R[2]) if D_vals is not None else None

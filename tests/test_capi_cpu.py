@@ -109,3 +109,23 @@ def test_null_handle_is_rejected_by_every_handle_call():
                             4) == _capi.SROM_ERR_INVALID
     assert L.srom_sweep(None, None, 0, None) == _capi.SROM_ERR_INVALID
     assert L.srom_orthonormalize(None, None, 4, 1, 4, 2) == _capi.SROM_ERR_INVALID
+
+
+def test_python_wrappers_refuse_host_tensors():
+    """The wrappers pass device pointers to the C ABI; host tensors are refused before any call."""
+    import numpy as np
+    import torch
+
+    from staccato_b200.krylov import fom_sweep, krylov_basis
+    from staccato_b200.project import DeviceCsr, project, project_complex
+
+    csr = DeviceCsr(n_rows=4, rowptr=torch.zeros(5, dtype=torch.int64), colind=torch.zeros(0, dtype=torch.int32))
+    z = torch.zeros(0, dtype=torch.complex128)
+    with pytest.raises(ValueError):
+        project_complex(None, csr, [z], torch.zeros((2, 4), dtype=torch.complex128))
+    with pytest.raises(ValueError):
+        project(None, csr, [torch.zeros(0, dtype=torch.float64)], torch.zeros((2, 4), dtype=torch.float64))
+    with pytest.raises(ValueError):
+        krylov_basis(None, csr, z, z, None, torch.zeros((1, 4), dtype=torch.complex128), [1.0], 1)
+    with pytest.raises(ValueError):
+        fom_sweep(None, csr, z, z, None, torch.zeros((1, 4), dtype=torch.complex128), np.array([1.0]))
