@@ -89,5 +89,6 @@ def project_complex(handle: _capi.Handle, csr: DeviceCsr, values: Sequence, V, Z
 def orthonormalize(handle: _capi.Handle, V, passes: int = 2) -> None:
     """In-place block Gram-Schmidt (``passes`` projection passes per 32-column panel) of an
     n x k column-major basis given as a contiguous (k, n) float64 tensor."""
+    _on_device(V)
     k, n = int(V.shape[0]), int(V.shape[1])
     check(handle.ptr, _capi.lib().srom_orthonormalize(handle.ptr, C.c_void_p(V.data_ptr()), n, k, n, passes))

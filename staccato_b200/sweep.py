@@ -84,7 +84,13 @@ class DeviceRom:
             self.Y = torch.empty(self.F * self.n_out * self.r, dtype=torch.complex128, device=device)
 
     def desc(self) -> RomDesc:
-        p = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+        def p(t):
+            if t is None:
+                return None
+            if not t.is_cuda:
+                raise ValueError("DeviceRom arrays must be CUDA tensors (the C ABI takes device pointers)")
+            return C.c_void_p(t.data_ptr())
+
         return RomDesc(n=self.n, r=self.r, F=self.F, ldk=self.n, K=p(self.K), M=p(self.M),
                        D=p(self.D), eta=self.eta, rhs=p(self.rhs), ldb=self.n,
                        omega=p(self.omega), X=p(self.X), info=p(self.info), steps=p(self.steps),
