@@ -10,7 +10,14 @@ max-over-ranks of the step time used by the benchmark.
 * ``rom_cost(n, r, F)``            the algorithmic flop count used as the cost;
 * ``rank_seed(base, rank)``        per-rank workload seed for weak scaling (each GPU sweeps its
                                     own batch of ROMs of the same distribution);
-* ``max_over_ranks(x, group)``     the step-time reduction (works on gloo and nccl).
+* ``max_over_ranks(x, group)``     the step-time reduction (works on gloo and nccl);
+* ``frequency_slice(F, world, rank)``  the contiguous block of frequencies a rank takes in a
+                                    sharded full-order sweep (``krylov.fom_sweep``: every frequency
+                                    is its own factorisation, so frequencies shard with no
+                                    collective; sizes differ by at most one).
+
+The Krylov basis process does not shard: each expansion point's blocks are re-orthogonalised
+against every column before them.
 """
 from __future__ import annotations
 
@@ -50,3 +57,13 @@ def max_over_ranks(x: float, group=None, device=None) -> float:
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return float(t.item())
+
+
+def frequency_slice(n_freq: int, world: int, rank: int):
+    """(start, stop) of rank's contiguous share of n_freq frequencies: the first n_freq % world
+    ranks take one more."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("need 0 <= rank < world")
+    q, rem = divmod(n_freq, world)
+    start = rank * q + min(rank, rem)
+    return start, start + q + (1 if rank < rem else 0)

@@ -79,3 +79,17 @@ def test_two_rank_gloo_sharded_sweep(tmp_path):
     for i, r in enumerate(roms):
         X, _ = O.sweep(r.K, r.M, r.D, 0.0, r.rhs, r.omega)
         assert np.array_equal(data[str(i)], X)
+
+
+def test_frequency_slices_cover_once_and_balance():
+    from staccato_b200.dist import frequency_slice
+
+    for n_freq in (0, 1, 7, 100, 1001):
+        for world in (1, 2, 3, 8):
+            sl = [frequency_slice(n_freq, world, r) for r in range(world)]
+            assert sl[0][0] == 0 and sl[-1][1] == n_freq
+            assert all(sl[i][1] == sl[i + 1][0] for i in range(world - 1))
+            sizes = [b - a for a, b in sl]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        frequency_slice(10, 2, 2)
