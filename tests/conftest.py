@@ -12,6 +12,16 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
 
 
+def pytest_sessionstart(session):
+    """The library is a build artefact (not in the repository): build it when a fresh checkout
+    runs the tests before the build step."""
+    import subprocess
+
+    lib = os.path.join(ROOT, "staccato_b200", "libstaccato_rom.so")
+    if not os.path.exists(lib):
+        subprocess.run([sys.executable, os.path.join(ROOT, "staccato_b200", "build.py")], check=True)
+
+
 @pytest.fixture(scope="session")
 def cuda_device():
     import torch
