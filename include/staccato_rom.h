@@ -48,14 +48,19 @@ typedef struct {
  *  k>0 U(k,k) is exactly zero (1-based column), as LAPACK zgetrf reports it
  *      (the reference ignores this value, KrylovROMSubstructure.cpp:1428);
  * -1   mixed-precision refinement did not reach the tolerance within max_refine steps
- *      and SROM_FLAG_FALLBACK_FP64 was not set (the last iterate is returned).        */
+ *      and SROM_FLAG_FALLBACK_FP64 was not set (the last iterate is returned);
+ * -2   SROM_MIXED_TC only: a bounded device-side wait of the kernel ran out and the system
+ *      was not solved (srom_sweep_host then returns SROM_ERR_TIMEOUT).                    */
 #define SROM_INFO_NOT_CONVERGED (-1)
+#define SROM_INFO_TIMEOUT (-2)
 
 /* ---- precision of the factorisation ---------------------------------------------- */
 #define SROM_FP64 0        /* all-FP64 complex LU, bit-identical to the restated zgetrf */
 #define SROM_MIXED_FP32 1  /* complex FP32 LU + FP64 residual refinement               */
-#define SROM_MIXED_TF32 2  /* reserved: 3xTF32 tensor-core LU + FP64 refinement; this build returns
-                              SROM_ERR_UNSUPPORTED for it                                       */
+#define SROM_MIXED_TC 2    /* tensor-core form: the same LU and FP64 refinement as SROM_MIXED_FP32,
+                              with every Schur update run on the tensor cores (tcgen05 MMAs on
+                              three-piece bf16 splits of the FP32 operands, FP32 accumulation);
+                              systems up to n = 512 (larger ones use the SROM_MIXED_FP32 kernel) */
 
 /* ---- sweep flags ---------------------------------------------------------------------- */
 #define SROM_FLAG_FALLBACK_FP64 1 /* re-solve non-converged frequencies in FP64 (steps = -1);
@@ -104,7 +109,7 @@ typedef struct {
 } srom_rom_desc;
 
 typedef struct {
-    int precision;   /* SROM_FP64 / SROM_MIXED_FP32 / SROM_MIXED_TF32                */
+    int precision;   /* SROM_FP64 / SROM_MIXED_FP32 / SROM_MIXED_TC                  */
     int max_refine;  /* refinement steps for the mixed forms (default 5 when <= 0)   */
     double tol;      /* stop refining when the error estimate 2 (||d_s||/||d_s-1||) ||d_s||/||x|| <= tol; 0 = 2^-34 */
     int flags;       /* SROM_FLAG_*                                                  */

@@ -61,6 +61,9 @@ struct srom_handle {
     // FP64 storage class chosen by srom_tune per (n << 16 | r): 0 smem kernel, 1 global kernel
     std::map<long long, int> tune_fp64;
     std::vector<cudaEvent_t> event_pool;
+    // error word of the last tensor-core sweep (device, inside d_meta) and its pinned host copy
+    int *tc_flag_dev = nullptr;
+    int *h_flag = nullptr;
     std::string err;
 };
 
@@ -289,6 +292,7 @@ int srom_destroy(srom_handle *h) {
     if (h->d_adj) cudaFree(h->d_adj);
     if (h->d_zero) cudaFree(h->d_zero);
     if (h->h_meta) cudaFreeHost(h->h_meta);
+    if (h->h_flag) cudaFreeHost(h->h_flag);
     if (h->meta_done) cudaEventDestroy(h->meta_done);
     for (auto &r : h->recs) {
         cudaEventDestroy(r.a);
@@ -343,6 +347,7 @@ namespace {
 // (descriptors, cost-ordered work lists, fallback list, zeroed counters) plus launch shapes.
 struct SweepPlan {
     bool mixed = false;
+    bool tc = false;  // the mixed systems of class 1 run on the tensor-core kernel
     srom_sweep_opts o{};
     std::vector<char> meta;
     size_t off_items0 = 0, off_items1 = 0, off_fb = 0, off_ctr = 0;
@@ -391,7 +396,7 @@ int mixed_class(const srom_handle *h, int n, int r, int flags) {
 int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts, SweepPlan &P) {
     if (n_roms < 0 || (n_roms > 0 && !roms)) return set_err(h, SROM_ERR_INVALID, "roms is null");
     srom_sweep_opts o = opts ? *opts : srom_sweep_opts{SROM_FP64, 5, 0.0, 0};
-    if (o.precision != SROM_FP64 && o.precision != SROM_MIXED_FP32)
+    if (o.precision != SROM_FP64 && o.precision != SROM_MIXED_FP32 && o.precision != SROM_MIXED_TC)
         return set_err(h, SROM_ERR_UNSUPPORTED, "precision %d not available in this build", o.precision);
     const bool mixed = o.precision != SROM_FP64;
     if (o.max_refine <= 0) o.max_refine = 5;
@@ -446,6 +451,10 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
     if (P.n_items[1] > 0) {
         P.grid1 = std::min<long long>(P.n_items[1], h->sm_count);
         P.slot_bytes = (int64_t)P.g_nmax * P.g_nmax * (int64_t)sizeof(double2);
+        // SROM_MIXED_TC: the tensor-core kernel takes class 1 when its limits allow (n <= 512 and
+        // the refinement's work areas fit); otherwise the CUDA-core FP32 kernel does.
+        P.tc = o.precision == SROM_MIXED_TC && srom::tc_supported(P.g_nmax, P.g_rmax, h->max_smem_optin, nullptr);
+        if (P.tc) P.slot_bytes = std::max<int64_t>(P.slot_bytes, (int64_t)srom::tc_slot_bytes(P.g_nmax));
         P.need_scratch = mixed;
         for (int i = 0; i < n_roms; ++i)
             if (cls[i] == 1 && !roms[i].LU) P.need_scratch = true;
@@ -507,7 +516,12 @@ int enqueue_plan(srom_handle *h, const SweepPlan &P, char *dm, void *scratch, cu
             a.fb_items = reinterpret_cast<Item *>(dm + P.off_fb);
             a.fb_count = d_ctr + 2;
         }
-        {
+        if (P.tc) {
+            a.err_flag = d_ctr + 4;
+            ProfScope ps(h, "mixed_tc", P.n_items[1], P.flops[1], 0.0);
+            cudaError_t e = srom::launch_tc(a, (int)P.grid1, st);
+            if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "tensor-core launch: %s", cudaGetErrorString(e));
+        } else {
             ProfScope ps(h, P.mixed ? "mixed_global" : "fp64_global", P.n_items[1], P.flops[1], 0.0);
             cudaError_t e = srom::launch_global(P.mixed, a, (int)P.grid1, st);
             if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "global launch: %s", cudaGetErrorString(e));
@@ -521,6 +535,7 @@ int enqueue_plan(srom_handle *h, const SweepPlan &P, char *dm, void *scratch, cu
             b.counter = d_ctr + 3;
             b.fb_items = nullptr;
             b.fb_count = nullptr;
+            b.err_flag = nullptr;
             b.steps_value = -1;
             ProfScope ps(h, "fp64_fallback", 0, 0.0, 0.0);
             cudaError_t e = srom::launch_global(false, b, (int)P.grid1, st);
@@ -582,6 +597,7 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
     SROM_CUDA(h, cudaMemcpyAsync(h->d_meta, h->h_meta, P.meta.size(), cudaMemcpyHostToDevice, h->stream));
     SROM_CUDA(h, cudaEventRecord(h->meta_done, h->stream));
     h->meta_pending = true;
+    h->tc_flag_dev = P.tc ? reinterpret_cast<int *>(static_cast<char *>(h->d_meta) + P.off_ctr) + 4 : nullptr;
     return enqueue_plan(h, P, static_cast<char *>(h->d_meta), scr, h->stream, false, true);
 }
 
@@ -1085,6 +1101,11 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
     }
     s = srom_sweep(h, dd.data(), n_roms, opts);
     if (s) return s;
+    int *flag_dev = h->tc_flag_dev;
+    if (flag_dev) {
+        if (!h->h_flag) SROM_CUDA(h, cudaMallocHost(reinterpret_cast<void **>(&h->h_flag), sizeof(int)));
+        SROM_CUDA(h, cudaMemcpyAsync(h->h_flag, flag_dev, sizeof(int), D2H, h->stream));
+    }
     for (int i = 0; i < n_roms; ++i) {
         const srom_rom_desc &d = roms[i];
         const srom_rom_desc &e = dd[i];
@@ -1098,6 +1119,9 @@ int srom_sweep_host(srom_handle *h, const srom_rom_desc *roms, int n_roms, const
                                          h->stream));
     }
     SROM_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (flag_dev && *h->h_flag)
+        return set_err(h, SROM_ERR_TIMEOUT, "a bounded device-side wait of the tensor-core kernel ran out "
+                                            "(systems with info = -2 were not solved)");
     return SROM_OK;
 }
 

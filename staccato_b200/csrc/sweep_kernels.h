@@ -42,12 +42,25 @@ struct GlobalArgs {
     int *fb_count;
     int steps_value;  // FP64: value stored in steps (0; -1 when re-solving mixed fallbacks)
     int smem_dyn;     // dynamic shared memory of the launch (set by launch_global)
+    int *err_flag;    // tensor-core kernel: set to 1 when a bounded device-side wait ran out
 };
 // Global-storage kernel, FP64 (mixed = false) or complex-FP32 factors + FP64 refinement.
 cudaError_t launch_global(bool mixed, const GlobalArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_fp64_global(const RomDev *roms, const Item *items, int n_items, int *counter,
                                double2 *scratch, int64_t slot_elems, int n_max, int r_max,
                                int grid, cudaStream_t st);
+
+// ---- tensor-core mixed form (sweep_tc.cu): complex-FP32 LU whose Schur updates run as
+// tcgen05 MMAs on three-piece bf16 splits, FP64 refinement as in the global kernel ----
+constexpr int TC_MAX_N = 512;
+size_t tc_slot_bytes(int n_max);                 // global scratch per CTA
+size_t tc_smem_bytes(int n_max, int r_max);      // dynamic shared memory of the launch
+// Whether the kernel handles systems up to n_max with r_max right-hand sides; why (may be
+// null) receives the reason when it does not.
+bool tc_supported(int n_max, int r_max, int smem_optin, const char **why);
+// a.slot_bytes must be at least tc_slot_bytes(a.n_max); a.fb_items / a.err_flag as for the
+// mixed global kernel.
+cudaError_t launch_tc(const GlobalArgs &a, int grid, cudaStream_t st);
 
 // Back-projection Y_f = C X_f of one ROM's solutions (F blocks of n x r -> n_out x r).
 struct BackProj {

@@ -1,0 +1,757 @@
+// Tensor-core form of the mixed-precision sweep (SROM_MIXED_TC).
+//
+// Same contract as the complex-FP32 global kernel (sweep.cu): one CTA owns one (ROM, frequency)
+// system at a time, assembles A(w) in FP64 and rounds it to complex FP32, factors it with
+// partial pivoting (LAPACK zgetrf's row order and layout, NB = 32 panels), then refines the
+// solution with FP64 residuals (mixed_refine).  What changes is the trailing (Schur) update
+// A22 -= L21 U12 of every panel step: it runs on the 5th-generation tensor cores.
+//
+// Schur update as real GEMMs.  With L21 = Lr + i Li (m x 32) and U12 = Ur + i Ui (32 x c):
+//     [Re | Im](L21 U12) = [Lr | Li] * [[Ur, Ui], [-Ui, Ur]]
+// i.e. one real GEMM with depth K = 64 whose B operand carries the 4M arrangement, so a tile of
+// 128 rows x 64 complex columns is one M = 128, N = 128, K = 64 product whose accumulator
+// columns 0..63 hold the real parts and 64..127 the imaginary parts.
+//
+// FP32 accuracy from bf16 tensor cores.  Every FP32 operand value x is split into three bf16
+// pieces x = x0 + x1 + x2 (+ a remainder below 2^-24 |x|, each piece the round-to-nearest of
+// what the previous ones left) and the product is accumulated from the six piece products
+// a_i b_j with i + j <= 2, smallest first, into FP32 accumulators in tensor memory
+// (tcgen05.mma kind::f16, 24 MMAs of 128 x 128 x 16 per tile).  The dropped terms are below
+// 2^-25 relative, so the factor is as accurate as a CUDA-core FP32 factorisation and the FP64
+// refinement converges as fast.  (The split-operand scheme for emulating a higher precision on
+// lower-precision tensor cores is the published one of Henry, Tang and Heinecke, "Leveraging
+// the bfloat16 Artificial Intelligence Datatype For Higher-Precision Computations", 2019.)
+//
+// Data flow of one panel step j0 (matrix in the CTA's global scratch slot, L2-resident):
+//   A  panel: columns j0..j0+31 staged in shared memory and factored (panel_factor_par); the
+//      factored panel is written back in logical row order; L11^-1 (unit lower, 32 x 32) is
+//      formed in shared memory; L21 is written to the CTA's A-operand buffer in global memory
+//      as ready-made tcgen05 operand tiles (three bf16 pieces, K-major core-matrix layout);
+//   B  every trailing column: the panel's row interchanges, U12 = L11^-1 (pivot rows), and the
+//      column's four 4M entries written to the B-operand buffer (same tile format);
+//   C  Schur tiles (row tiles of 128 outer, column tiles of 64 inner): operand tiles are
+//      brought into shared memory by bulk asynchronous copies (cp.async.bulk with mbarrier
+//      completion; the A tile once per row tile, the B tiles through a 3-deep ring), one thread
+//      issues the 24 MMAs of a tile into one of two TMEM accumulators, and while the tensor
+//      cores work on tile t all 8 warps subtract tile t-1's accumulator (tcgen05.ld) from the
+//      matrix in place.
+// No cluster, no multicast: every copy reads this GPU's own memory into this CTA.
+//
+// Every mbarrier wait is bounded (about 2 s of device time); a wait that runs out marks the
+// system (info = -2), sets the launch's error word, drains the copies and MMAs this CTA has in
+// flight (bounded as well), frees its tensor memory and ends the CTA.
+//
+// Reference sequence: src/analysis/KrylovROMSubstructure.cpp:1411-1430 (assembly, zgetrf,
+// zgetrs per frequency) and the batched cuBLAS sweep of
+// test/krylovMidsizeTest/gpu/concurrent/batchedLU/src/main.cu:223-267.
+#include <cuda_bf16.h>
+
+#include "sweep_common.cuh"
+
+namespace srom {
+namespace tcm {
+
+constexpr int NB = 32;                 // panel width (complex columns)
+constexpr int KP = 2 * NB;             // depth of the real Schur GEMM: [Re L | Im L]
+constexpr int TM = 128;                // rows of a tile (TMEM lanes)
+constexpr int TNC = 64;                // complex columns of a tile
+constexpr int TN = 2 * TNC;            // real accumulator columns of a tile: [Re | Im]
+constexpr int PIECES = 3;              // bf16 pieces per FP32 value
+constexpr int MMA_K = 16;              // depth of one kind::f16 MMA
+constexpr int KSTEPS = KP / MMA_K;     // MMAs per piece product
+constexpr int STAGES = 3;              // B-operand ring depth
+constexpr int PIECE_BYTES = 128 * KP * 2;           // one bf16 piece of a 128-row operand tile
+constexpr int TILE_BYTES = PIECES * PIECE_BYTES;    // 48 KB
+constexpr int OP_BYTES = (1 + STAGES) * TILE_BYTES; // A tile + B ring
+constexpr int TMEM_COLS = 2 * TN;                   // two accumulator buffers
+constexpr int LDL = 33;                             // leading dimension of L11^-1 in smem
+constexpr int CPW = 4;                              // trailing columns per warp pass (phase B)
+constexpr int INFO_TIMEOUT = -2;
+
+// Instruction descriptor: D f32, A and B bf16, both K-major, M = 128, N = 128.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                           ((uint32_t)(TM >> 4) << 24);
+
+static_assert(TN % 16 == 0 && TN >= 16 && TN <= 256, "N of an M = 128 MMA");
+static_assert(OP_BYTES >= (512 | 1) * NB * 8, "the panel of an n = 512 system fits the operand region");
+
+// Byte offset of element (row, k) in one operand piece: K-major core matrices of 8 rows x 16
+// bytes (8 bf16), the K-adjacent ones 128 bytes apart (LBO), the 8-row groups 1024 bytes apart
+// (SBO = 8 core matrices of the 64-deep row).
+__host__ __device__ constexpr int op_off(int row, int k) {
+    return (row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+
+// Shared-memory layout (offsets from a 1024-byte aligned base).  The operand region holds the
+// panel during phase A, the A tile and the B ring during phase C, and the refinement's
+// iterate, right-hand sides and staging ring after the factorisation.
+struct TcSmem {
+    size_t op, perm, ptot, pos, ipiv, moved, dinv, linv, bars, tmem, total;
+    size_t work64, work32, ring;
+    static __host__ __device__ size_t up(size_t b) { return (b + 255) / 256 * 256; }
+    __host__ __device__ TcSmem(int ldp, int n_max, int r_max) {
+        op = 0;
+        perm = op + OP_BYTES;
+        ptot = perm + up((size_t)ldp * 4);
+        pos = ptot + up((size_t)ldp * 4);
+        ipiv = pos + up((size_t)ldp * 4);
+        moved = ipiv + up((size_t)ldp * 4);
+        dinv = moved + up((size_t)2 * 2 * NB * 4);
+        linv = dinv + up((size_t)ldp * 8);
+        bars = linv + up((size_t)NB * LDL * 8);
+        tmem = bars + up((size_t)(1 + STAGES + 2) * 8);
+        total = tmem + 256;
+        work64 = op;
+        work32 = work64 + up((size_t)n_max * r_max * 16);
+        ring = work32 + up((size_t)n_max * r_max * 8);
+    }
+};
+
+// Global scratch of one CTA: the complex-FP32 matrix, then the A- and B-operand tile buffers.
+struct TcSlot {
+    size_t a32, abuf, bbuf, total;
+    __host__ __device__ TcSlot(int n_max) {
+        const int mt = n_max > NB ? n_max - NB : 1;
+        a32 = 0;
+        abuf = ((size_t)n_max * n_max * 8 + 1023) / 1024 * 1024;
+        bbuf = abuf + (size_t)((mt + TM - 1) / TM) * TILE_BYTES;
+        total = bbuf + (size_t)((mt + TNC - 1) / TNC) * TILE_BYTES;
+    }
+};
+
+// ---------------------------------------------------------------------------- PTX wrappers
+__device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for the completion of the barrier phase with the given parity, at most about 2 s of
+// device time (and a bounded number of polls).  Returns false when the wait ran out.
+__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (mbar_test(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    for (uint32_t it = 0; it < (1u << 28); ++it) {
+        if (mbar_test(bar, parity)) return true;
+        if ((it & 255u) == 255u && globaltimer() - t0 > 2000000000ull) return false;
+    }
+    return false;
+}
+
+// Bulk copy global -> this CTA's shared memory, completion counted on an mbarrier.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: no swizzle, K-major core matrices, LBO 128 B, SBO 1024 B,
+// descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// 16 consecutive 32-bit accumulator columns of this thread's TMEM lane, waited for in the same
+// statement (so no use of the registers can be scheduled before the load completes).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// x = p0 + p1 + p2 (+ below 2^-24 |x|): each piece the bf16 rounding of what is left.
+__device__ __forceinline__ void split3(float x, __nv_bfloat16 (&p)[3]) {
+    p[0] = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(p[0]);
+    p[1] = __float2bfloat16_rn(r1);
+    const float r2 = r1 - __bfloat162float(p[1]);
+    p[2] = __float2bfloat16_rn(r2);
+}
+
+__device__ __forceinline__ unsigned short bfbits(__nv_bfloat16 v) { return __bfloat16_as_ushort(v); }
+
+// u += a * b (complex FP32)
+__device__ __forceinline__ float2 cfma(float2 u, float2 a, float2 b) {
+    return make_float2(__fmaf_rn(a.x, b.x, __fmaf_rn(-a.y, b.y, u.x)), __fmaf_rn(a.x, b.y, __fmaf_rn(a.y, b.x, u.y)));
+}
+
+// ---------------------------------------------------------------------------- pipeline state
+// Barrier words: bar_a (A tile), bar_full[s] (ring slot s), bar_mma[b] (accumulator b).
+struct Bars {
+    uint32_t base;
+    __device__ uint32_t a() const { return base; }
+    __device__ uint32_t full(int s) const { return base + 8u * (uint32_t)(1 + s); }
+    __device__ uint32_t mma(int b) const { return base + 8u * (uint32_t)(1 + STAGES + b); }
+};
+
+// Counters that give every barrier wait its parity.  Tiles are numbered over the CTA's life
+// (g): tile g uses ring slot g % STAGES (its (g / STAGES)-th fill) and accumulator g & 1 (its
+// (g >> 1)-th commit).  All threads keep g; thread 0 (the issuer) also keeps the fill and A
+// counts for the drain after a timeout.
+struct TcState {
+    int g;         // tiles issued so far
+    int loaded;    // B tiles whose copies were issued (global tile numbers [0, loaded))
+    int a_loads;   // A tiles issued
+};
+
+__device__ __forceinline__ void set_abort(int *s_abort, int *err_flag) {
+    *reinterpret_cast<volatile int *>(s_abort) = 1;
+    if (err_flag) atomicExch(err_flag, 1);
+}
+
+__device__ __forceinline__ bool aborted(const int *s_abort) { return *reinterpret_cast<const volatile int *>(s_abort) != 0; }
+
+// Thread 0 after a timeout: wait (bounded) for every copy and MMA this CTA may still have in
+// flight, so that no asynchronous write lands after the CTA has freed its resources.
+__device__ void drain(const Bars &B, const TcState &S) {
+    for (int k = 1; k <= 2 && S.g - k >= 0; ++k) {
+        const int g = S.g - k;
+        mbar_wait(B.mma(g & 1), (uint32_t)(g >> 1) & 1u);
+    }
+    for (int k = 1; k <= STAGES && S.loaded - k >= 0; ++k) {
+        const int g = S.loaded - k;
+        mbar_wait(B.full(g % STAGES), (uint32_t)(g / STAGES) & 1u);
+    }
+    if (S.a_loads > 0) mbar_wait(B.a(), (uint32_t)(S.a_loads - 1) & 1u);
+}
+
+// ---------------------------------------------------------------------------- phase A helpers
+// L11^-1 of the factored panel (unit lower triangle of logical rows 0..31), column j by warp
+// j % NW: y = e_j, then y_i -= L[i][k] y_k for k = j..30, i > k.  Stored column-major (LDL).
+__device__ void build_linv(const float2 *P, int ldp, const int *s_perm, float2 *s_linv) {
+    using C = CT<float2>;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int pr = s_perm[lane];
+    for (int j = warp; j < NB; j += NW) {
+        float2 y = lane == j ? make_float2(1.f, 0.f) : C::zero();
+        for (int k = j; k < NB - 1; ++k) {
+            const float2 yk = C::shfl(y, k, 32);
+            if (lane > k) y = C::subm(y, P[pr + (int64_t)k * ldp], yk);
+        }
+        s_linv[lane + j * LDL] = lane >= j ? y : C::zero();
+    }
+}
+
+// L21 (logical rows 32..m-1 of the factored panel) as A-operand tiles: row r of tile r / 128,
+// k < 32 the real parts of panel column k, k >= 32 the imaginary parts of column k - 32; three
+// bf16 pieces per tile.  Rows past the last (to the tile's 128) are zero.  One thread per
+// (8-row group, 8-deep chunk pair): two 16-byte stores per piece, consecutive threads on
+// consecutive 16-byte rows of a core matrix.
+__device__ void build_abuf(const float2 *P, int ldp, const int *s_perm, int mt, unsigned char *abuf) {
+    const int nrt = (mt + TM - 1) / TM;
+    const int total = nrt * (TM / 8) * 32;
+    for (int e = threadIdx.x; e < total; e += NT) {
+        const int r8 = e & 7, kc = (e >> 3) & 3, g8 = e >> 5;
+        const int r = g8 * 8 + r8;  // row of L21
+        const int rt = r / TM, rr = r % TM;
+        float re[8], im[8];
+        if (r < mt) {
+            const int pr = s_perm[NB + r];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const float2 v = P[pr + (int64_t)(8 * kc + t) * ldp];
+                re[t] = v.x;
+                im[t] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < 8; ++t) re[t] = im[t] = 0.f;
+        }
+        unsigned short pr_[3][8], pi_[3][8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            __nv_bfloat16 a[3], b[3];
+            split3(re[t], a);
+            split3(im[t], b);
+#pragma unroll
+            for (int p = 0; p < 3; ++p) {
+                pr_[p][t] = bfbits(a[p]);
+                pi_[p][t] = bfbits(b[p]);
+            }
+        }
+        unsigned char *tile = abuf + (size_t)rt * TILE_BYTES;
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+            uint4 vr, vi;
+            vr.x = pr_[p][0] | ((uint32_t)pr_[p][1] << 16);
+            vr.y = pr_[p][2] | ((uint32_t)pr_[p][3] << 16);
+            vr.z = pr_[p][4] | ((uint32_t)pr_[p][5] << 16);
+            vr.w = pr_[p][6] | ((uint32_t)pr_[p][7] << 16);
+            vi.x = pi_[p][0] | ((uint32_t)pi_[p][1] << 16);
+            vi.y = pi_[p][2] | ((uint32_t)pi_[p][3] << 16);
+            vi.z = pi_[p][4] | ((uint32_t)pi_[p][5] << 16);
+            vi.w = pi_[p][6] | ((uint32_t)pi_[p][7] << 16);
+            unsigned char *piece = tile + (size_t)p * PIECE_BYTES;
+            *reinterpret_cast<uint4 *>(piece + op_off(rr, 8 * kc)) = vr;
+            *reinterpret_cast<uint4 *>(piece + op_off(rr, 32 + 8 * kc)) = vi;
+        }
+    }
+}
+
+// Row interchanges of the panel applied to the columns left of it (LAPACK's laswp on A(:, 0:j0)).
+__device__ void swap_left(float2 *A, int n, int j0, const int *s_mdst, const int *s_msrc, int nmoved) {
+    constexpr int CB = 8;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int cb = warp * CB; cb < j0; cb += NW * CB) {
+        float2 mv[2][CB];
+#pragma unroll
+        for (int t = 0; t < CB; ++t) {
+            if (cb + t < j0) {
+                const float2 *col = A + (int64_t)(cb + t) * n + j0;
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int e = lane + 32 * q;
+                    if (e < nmoved) mv[q][t] = col[s_msrc[e]];
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < CB; ++t) {
+            if (cb + t < j0) {
+                float2 *col = A + (int64_t)(cb + t) * n + j0;
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int e = lane + 32 * q;
+                    if (e < nmoved) col[s_mdst[e]] = mv[q][t];
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------- phase B
+// Trailing columns c >= j0 + 32, a warp per column, CPW columns per pass: the panel's
+// interchanges (pivot rows read into x, displaced rows moved down to the pivot rows' places),
+// U12 = L11^-1 x written to the matrix, and the column's 4M entries (Ur, Ui; -Ui, Ur) as three
+// bf16 pieces into the B-operand tiles.  After this phase rows j0+32.. of the trailing matrix
+// are in the factor's (logical) order.
+__device__ void trailing_rows(float2 *A, int n, int j0, const int *s_perm, const int *s_mdst, const int *s_msrc,
+                              int nmoved, const float2 *s_linv, unsigned char *bbuf) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c0 = j0 + NB;
+    const int ncols = n - c0;
+    const int prow = j0 + s_perm[lane];
+    int md[2], ms[2];
+    bool mvok[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int e = lane + 32 * q;
+        mvok[q] = e < nmoved && s_mdst[e] >= NB;
+        md[q] = mvok[q] ? j0 + s_mdst[e] : 0;
+        ms[q] = mvok[q] ? j0 + s_msrc[e] : 0;
+    }
+    for (int cb = warp * CPW; cb < ncols; cb += NW * CPW) {
+        float2 x[CPW], mv[CPW][2];
+#pragma unroll
+        for (int t = 0; t < CPW; ++t) {
+            if (cb + t < ncols) {
+                const float2 *col = A + (int64_t)(c0 + cb + t) * n;
+                x[t] = col[prow];
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                    if (mvok[q]) mv[t][q] = col[ms[q]];
+            } else {
+                x[t] = make_float2(0.f, 0.f);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < CPW; ++t) {
+            if (cb + t < ncols) {
+                float2 *col = A + (int64_t)(c0 + cb + t) * n;
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                    if (mvok[q]) col[md[q]] = mv[t][q];
+            }
+        }
+        // u_l = x_l + sum_{j<l} Linv[l][j] x_j
+        float2 u[CPW];
+#pragma unroll
+        for (int t = 0; t < CPW; ++t) u[t] = x[t];
+        for (int j = 0; j < NB - 1; ++j) {
+            const float2 lv = s_linv[lane + j * LDL];
+#pragma unroll
+            for (int t = 0; t < CPW; ++t) {
+                const float2 xj = CT<float2>::shfl(x[t], j, 32);
+                if (lane > j) u[t] = cfma(u[t], lv, xj);
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < CPW; ++t) {
+            if (cb + t >= ncols) continue;
+            A[(int64_t)(c0 + cb + t) * n + j0 + lane] = u[t];
+            const int cc = cb + t, ct = cc / TNC, q = cc % TNC;
+            __nv_bfloat16 pr[3], pi[3];
+            split3(u[t].x, pr);
+            split3(u[t].y, pi);
+            unsigned char *tile = bbuf + (size_t)ct * TILE_BYTES;
+#pragma unroll
+            for (int p = 0; p < 3; ++p) {
+                unsigned char *piece = tile + (size_t)p * PIECE_BYTES;
+                const unsigned short rb = bfbits(pr[p]), ib = bfbits(pi[p]);
+                *reinterpret_cast<unsigned short *>(piece + op_off(q, lane)) = rb;
+                *reinterpret_cast<unsigned short *>(piece + op_off(TNC + q, lane)) = ib;
+                *reinterpret_cast<unsigned short *>(piece + op_off(q, NB + lane)) = (unsigned short)(ib ^ 0x8000u);
+                *reinterpret_cast<unsigned short *>(piece + op_off(TNC + q, NB + lane)) = rb;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------- phase C
+// C(tile) -= accumulator: warp w reads TMEM lanes 32 (w & 3) .. +31 (its rows) and complex
+// columns 32 (w >> 2) .. +31 of the tile, 16 at a time (real parts from column c, imaginary
+// from c + 64), and updates the matrix in place (column-major: a warp's 32 rows of one column
+// are one 256-byte segment).
+__device__ void epilogue(float2 *A, int n, int r0, int c0, uint32_t tbuf, bool ok) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q4 = warp & 3, h = warp >> 2;
+    const int gr = r0 + 32 * q4 + lane;
+    const uint32_t tb = tbuf + ((uint32_t)(32 * q4) << 16);
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const int cb = 32 * h + 16 * r;
+        float re[16], im[16];
+        tmem_ld16(tb + (uint32_t)cb, re);
+        tmem_ld16(tb + (uint32_t)(TNC + cb), im);
+        if (!ok || gr >= n) continue;
+        const int gc = c0 + cb;
+        float2 cv[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            if (gc + i < n) cv[i] = A[gr + (int64_t)(gc + i) * n];
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            if (gc + i < n) A[gr + (int64_t)(gc + i) * n] = make_float2(cv[i].x - re[i], cv[i].y - im[i]);
+    }
+}
+
+// Schur update of rows and columns [j0 + 32, n) from the operand buffers (see the file header).
+__device__ void schur_tc(float2 *A, int n, int j0, unsigned char *op, const unsigned char *abuf,
+                         const unsigned char *bbuf, uint32_t tmem, const Bars &B, TcState &S, int *s_abort,
+                         int *err_flag) {
+    const int tid = threadIdx.x;
+    const int mt = n - j0 - NB;
+    const int nrt = (mt + TM - 1) / TM, nct = (mt + TNC - 1) / TNC, T = nrt * nct;
+    const uint32_t opa = su32(op);
+    auto slot = [&](int s) { return opa + (uint32_t)((1 + s) * TILE_BYTES); };
+    const int g0 = S.g;
+    if (tid == 0 && !aborted(s_abort)) {
+        mbar_expect_tx(B.a(), TILE_BYTES);
+        bulk_load(opa, abuf, TILE_BYTES, B.a());
+        S.a_loads++;
+        for (int i = 0; i < STAGES && i < T; ++i) {
+            const int g = g0 + i;
+            mbar_expect_tx(B.full(g % STAGES), TILE_BYTES);
+            bulk_load(slot(g % STAGES), bbuf + (size_t)(i % nct) * TILE_BYTES, TILE_BYTES, B.full(g % STAGES));
+            S.loaded = g + 1;
+        }
+    }
+    // piece products (A piece, B piece), smallest first
+    constexpr int PA[6] = {2, 1, 0, 1, 0, 0};
+    constexpr int PB[6] = {0, 1, 2, 0, 1, 0};
+    for (int t = 0; t <= T; ++t) {
+        const int g = g0 + t;
+        if (tid == 0 && t < T && !aborted(s_abort)) {
+            const int rt = t / nct;
+            const bool new_rt = t == 0 || rt != (t - 1) / nct;
+            bool ok = true;
+            if (t > 0 && new_rt) {
+                // the A tile is free once every MMA reading it has completed, i.e. tile t-1's
+                ok = mbar_wait(B.mma((g - 1) & 1), (uint32_t)((g - 1) >> 1) & 1u);
+                if (ok) {
+                    mbar_expect_tx(B.a(), TILE_BYTES);
+                    bulk_load(opa, abuf + (size_t)rt * TILE_BYTES, TILE_BYTES, B.a());
+                    S.a_loads++;
+                }
+            }
+            if (ok && new_rt) ok = mbar_wait(B.a(), (uint32_t)(S.a_loads - 1) & 1u);
+            if (ok) ok = mbar_wait(B.full(g % STAGES), (uint32_t)(g / STAGES) & 1u);
+            if (ok) {
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)((g & 1) * TN);
+                const uint32_t bsl = slot(g % STAGES);
+                int acc = 0;
+#pragma unroll
+                for (int p = 0; p < 6; ++p)
+#pragma unroll
+                    for (int ks = 0; ks < KSTEPS; ++ks) {
+                        const uint64_t ad = sdesc(opa + (uint32_t)(PA[p] * PIECE_BYTES + ks * 256));
+                        const uint64_t bd = sdesc(bsl + (uint32_t)(PB[p] * PIECE_BYTES + ks * 256));
+                        mma_bf16(d, ad, bd, (uint32_t)acc);
+                        acc = 1;
+                    }
+                mma_commit(B.mma(g & 1));
+                S.g = g + 1;
+            } else {
+                set_abort(s_abort, err_flag);
+            }
+        }
+        if (t > 0) {
+            // epilogue of tile t-1 (its MMAs were issued one iteration ago)
+            const int tp = t - 1, gp = g - 1;
+            bool ok = !aborted(s_abort) && mbar_wait(B.mma(gp & 1), (uint32_t)(gp >> 1) & 1u);
+            ok = __all_sync(FULL_MASK, ok);
+            if (!ok) set_abort(s_abort, err_flag);
+            tc_fence_after();
+            epilogue(A, n, j0 + NB + (tp / nct) * TM, j0 + NB + (tp % nct) * TNC, tmem + (uint32_t)((gp & 1) * TN), ok);
+        }
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0 && t > 0 && !aborted(s_abort)) {
+            // ring slot of tile t-1 is free (its MMAs completed): fill it with tile t-1+STAGES
+            const int tn = t - 1 + STAGES;
+            if (tn < T) {
+                const int gn = g0 + tn;
+                mbar_expect_tx(B.full(gn % STAGES), TILE_BYTES);
+                bulk_load(slot(gn % STAGES), bbuf + (size_t)(tn % nct) * TILE_BYTES, TILE_BYTES, B.full(gn % STAGES));
+                S.loaded = gn + 1;
+            }
+        }
+    }
+    if (tid != 0) S.g = g0 + T;  // thread 0 counted its issues (fewer after a timeout)
+}
+
+// ---------------------------------------------------------------------------- factorisation
+// Blocked LU of the complex-FP32 system in A (n x n, ld n): the same output as factor_global
+// (LAPACK layout, rows in final order, s_ptot the composite permutation, s_ipiv the pivots,
+// PL.info the first zero pivot), with the Schur updates on the tensor cores.
+template <int RPT>
+__device__ void factor_tc(float2 *A, int n, int ldp, unsigned char *sm, const TcSmem &L, unsigned char *abuf,
+                          unsigned char *bbuf, PanelLists &PL, PivotXchg<float> &X, int *s_pivlg, uint32_t tmem,
+                          const Bars &B, TcState &S, int *s_abort, int *err_flag) {
+    float2 *P = reinterpret_cast<float2 *>(sm + L.op);
+    int *s_perm = reinterpret_cast<int *>(sm + L.perm);
+    int *s_ptot = reinterpret_cast<int *>(sm + L.ptot);
+    int *s_ipiv = reinterpret_cast<int *>(sm + L.ipiv);
+    int *s_mdst = reinterpret_cast<int *>(sm + L.moved);
+    int *s_msrc = s_mdst + 2 * NB;
+    float2 *s_linv = reinterpret_cast<float2 *>(sm + L.linv);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < n; i += NT) s_ptot[i] = i;
+    if (tid == 0) PL.info = 0;
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int nbc = min(NB, n - j0);
+        const int m = n - j0;
+        const int mt = m - NB;  // trailing rows and columns (> 0 only for full panels)
+        for (int c = warp; c < nbc; c += NW)
+            for (int i = lane; i < m; i += 32) P[i + (int64_t)c * ldp] = A[(j0 + i) + (int64_t)(j0 + c) * n];
+        if (tid == 0) {
+            PL.nmoved = 0;
+            PL.grp = 0;
+        }
+        __syncthreads();
+        panel_factor_par<float2, RPT>(P, ldp, m, nbc, s_perm, s_pivlg, s_mdst, s_msrc, PL, j0, X);
+        const int nmoved = PL.nmoved;
+        for (int c = warp; c < nbc; c += NW)
+            for (int i = lane; i < m; i += 32) A[(j0 + i) + (int64_t)(j0 + c) * n] = P[s_perm[i] + (int64_t)c * ldp];
+        if (tid < nbc) s_ipiv[j0 + tid] = j0 + s_pivlg[tid] + 1;
+        if (warp == NW - 1) {
+            int v[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int e = lane + 32 * q;
+                if (e < nmoved) v[q] = s_ptot[j0 + s_msrc[e]];
+            }
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int e = lane + 32 * q;
+                if (e < nmoved) s_ptot[j0 + s_mdst[e]] = v[q];
+            }
+            __syncwarp();
+        }
+        if (mt > 0) {
+            build_linv(P, ldp, s_perm, s_linv);
+            build_abuf(P, ldp, s_perm, mt, abuf);
+        }
+        swap_left(A, n, j0, s_mdst, s_msrc, nmoved);
+        __syncthreads();
+        if (mt > 0) {
+            trailing_rows(A, n, j0, s_perm, s_mdst, s_msrc, nmoved, s_linv, bbuf);
+            fence_proxy_async();  // generic writes (operand buffers, panel smem) before async-proxy use
+            __syncthreads();
+            schur_tc(A, n, j0, sm + L.op, abuf, bbuf, tmem, B, S, s_abort, err_flag);
+            fence_proxy_async();  // async-proxy writes of the operand region before generic reuse
+            if (aborted(s_abort)) return;
+        }
+        __syncthreads();
+    }
+}
+
+template <int RPT>
+__global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
+    extern __shared__ unsigned char sm_raw[];
+    __shared__ int s_item;
+    __shared__ int s_pivlg[NB];
+    __shared__ PanelLists PL;
+    __shared__ PivotXchg<float> Xx;
+    __shared__ double s_dx[RMAX_MIXED];
+    __shared__ int s_abort;
+    unsigned char *sm = sm_raw + ((1024u - (su32(sm_raw) & 1023u)) & 1023u);
+    const TcSmem L(a.ldp, a.n_max, a.r_max);
+    const TcSlot SL(a.n_max);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(sm + L.tmem);
+    const Bars B{su32(sm + L.bars)};
+    if (tid == 0) {
+        mbar_init(B.a(), 1);
+        for (int s = 0; s < STAGES; ++s) mbar_init(B.full(s), 1);
+        for (int b = 0; b < 2; ++b) mbar_init(B.mma(b), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(s_tmem)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *s_tmem;
+    TcState S{0, 0, 0};
+    unsigned char *slotp = a.scratch + (int64_t)blockIdx.x * a.slot_bytes;
+    float2 *A32 = reinterpret_cast<float2 *>(slotp + SL.a32);
+    unsigned char *abuf = slotp + SL.abuf;
+    unsigned char *bbuf = slotp + SL.bbuf;
+
+    for (;;) {
+        const int it = next_item(a.counter, &s_item);
+        if (it >= a.n_items) break;
+        const Item wi = a.items[it];
+        const RomDev R = a.roms[wi.rom];
+        const int n = R.n;
+        const double w = R.omega[wi.f];
+        int steps = 0, info = 0;
+        double berr = 0.0;
+        bool write_status = true;
+        assemble_into<float2>(A32, n, R, w);
+        __syncthreads();
+        factor_tc<RPT>(A32, n, a.ldp, sm, L, abuf, bbuf, PL, Xx, s_pivlg, tmem, B, S, &s_abort, a.err_flag);
+        __syncthreads();
+        if (aborted(&s_abort)) {
+            if (tid == 0 && R.info) R.info[wi.f] = INFO_TIMEOUT;
+            break;
+        }
+        info = PL.info;
+        MixedWork W{reinterpret_cast<double2 *>(sm + L.work64),
+                    reinterpret_cast<float2 *>(sm + L.work32),
+                    reinterpret_cast<int *>(sm + L.pos),
+                    reinterpret_cast<int *>(sm + L.ptot),
+                    reinterpret_cast<float2 *>(sm + L.dinv),
+                    sm + L.ring,
+                    (int)(OP_BYTES - L.ring),
+                    s_dx};
+        mixed_refine<RPT>(a, R, wi, w, A32, W, info, steps, berr, write_status);
+        if (tid == 0 && write_status) {
+            if (R.info) R.info[wi.f] = info;
+            if (R.steps) R.steps[wi.f] = steps;
+            if (R.berr) R.berr[wi.f] = berr;
+        }
+        __syncthreads();
+    }
+    if (tid == 0 && aborted(&s_abort)) drain(B, S);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
+}  // namespace tcm
+
+// ---------------------------------------------------------------------------- host side
+size_t tc_slot_bytes(int n_max) { return tcm::TcSlot(n_max).total; }
+
+size_t tc_smem_bytes(int n_max, int r_max) { return tcm::TcSmem(n_max | 1, n_max, r_max).total + 1024; }
+
+bool tc_supported(int n_max, int r_max, int smem_optin, const char **why) {
+    const char *w = nullptr;
+    if (n_max > TC_MAX_N) w = "order above the tensor-core kernel's limit";
+    else if (r_max > MIXED_MAX_R) w = "too many right-hand sides";
+    else {
+        const tcm::TcSmem L(n_max | 1, n_max, r_max);
+        if (tcm::OP_BYTES < (int64_t)L.ring || tcm::OP_BYTES - (int64_t)L.ring < 2 * 16 * (int64_t)n_max * 8)
+            w = "refinement work areas exceed shared memory";
+        else if (tc_smem_bytes(n_max, r_max) + GLOBAL_STATIC_SMEM > (size_t)smem_optin)
+            w = "shared memory";
+    }
+    if (why) *why = w;
+    return w == nullptr;
+}
+
+template <int RPT>
+static cudaError_t launch_tc_t(const GlobalArgs &a0, int grid, cudaStream_t st) {
+    auto k = tcm::sweep_tc_kernel<RPT>;
+    GlobalArgs a = a0;
+    const size_t smem = tc_smem_bytes(a.n_max, a.r_max);
+    a.smem_dyn = (int)smem;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, NT, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc(const GlobalArgs &a0, int grid, cudaStream_t st) {
+    GlobalArgs a = a0;
+    a.ldp = a.n_max | 1;
+    if (a.n_max > TC_MAX_N || a.r_max > MIXED_MAX_R || a.slot_bytes < (int64_t)tc_slot_bytes(a.n_max))
+        return cudaErrorInvalidValue;
+    const int rpt = global_rpt(a.n_max);
+    if (rpt <= 1) return launch_tc_t<1>(a, grid, st);
+    if (rpt == 2) return launch_tc_t<2>(a, grid, st);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace srom
