@@ -39,8 +39,9 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
-                   help="both: headline = mixed+refine, plain FP64 measured beside it")
+    p.add_argument("--precision", choices=["both", "mixed", "mixed_fp32", "fp64"], default="both",
+                   help="both: headline = tensor-core mixed+refine, plain FP64 and the CUDA-core mixed "
+                        "form measured beside it; mixed: the tensor-core form alone")
     p.add_argument("--cpu-sample-stride", type=int, default=16,
                    help="CPU baseline sweeps every k-th frequency of every ROM")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -159,6 +160,63 @@ def gemm_peak_tflops(torch, dev, dtype) -> float:
 
 
 # ----------------------------------------------------------------------------- CPU legs
+
+def all_systems_error(torch, drom, x64):
+    """Relative 2-norm difference (all right-hand sides of a system together) of every system's
+    solution from the FP64 form's solution of the same system, computed on the device.  The FP64
+    kernel is bit-identical to the oracle's zgetrf/zgetrs, so this compares the mixed form with
+    the FP64 oracle on all systems of the step.  Returns the summary and the per-system errors."""
+    errs = []
+    for d, x in zip(drom, x64):
+        a = d.X.view(d.F, d.r * d.n)
+        b = x.view(d.F, d.r * d.n)
+        errs.append(torch.linalg.vector_norm(a - b, dim=1) / torch.linalg.vector_norm(b, dim=1))
+    e = torch.cat(errs)
+    summary = {"systems": int(e.numel()), "max": float(e.max()), "median": float(e.median()),
+               "above_1e-10": int((e > 1e-10).sum())}
+    return {"summary": summary, "per_system": e.double().cpu().numpy()}
+
+
+def _xref_group(task):
+    """Worker: the oracle's long-double-refined solutions of one ROM at the given frequencies."""
+    from oracle import oracle as O
+
+    K, M, D, rhs, omega = task
+    return O.x_ref(K, M, D, 0.0, rhs, omega)
+
+
+def xref_worst(roms, drom, per_system, k_worst=32, seed=0):
+    """The oracle's x_ref (FP64 LU + long-double residual refinement) for the k_worst systems that
+    deviate most from the FP64 solution plus one random frequency of every ROM; returns the max
+    and median relative error of the mixed form's solutions there.  Runs in a spawn pool over
+    the host cores (the oracle is single-threaded)."""
+    import multiprocessing as mp
+
+    offs = np.cumsum([0] + [r.F for r in roms])
+    worst = np.argsort(per_system)[::-1][:k_worst]
+    rng = np.random.default_rng(seed)
+    picks = {}
+    for g in worst:
+        i = int(np.searchsorted(offs, g, side="right") - 1)
+        picks.setdefault(i, set()).add(int(g - offs[i]))
+    for i, r in enumerate(roms):
+        picks.setdefault(i, set()).add(int(rng.integers(r.F)))
+    groups = sorted((i, sorted(fs)) for i, fs in picks.items())
+    tasks = [(roms[i].K, roms[i].M, roms[i].D, roms[i].rhs, roms[i].omega[fs]) for i, fs in groups]
+    procs = max(1, min(len(tasks), os.cpu_count() or 1))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        refs = pool.map(_xref_group, tasks, chunksize=1)
+    from oracle import oracle as O
+
+    errs = []
+    for (i, fs), xr in zip(groups, refs):
+        X = drom[i].solutions()[fs]
+        errs.append(O.rel_err(X, xr))
+    e = np.concatenate(errs)
+    return {"systems": int(e.size), "max": float(e.max()), "median": float(np.median(e)),
+            "selection": f"the {k_worst} systems farthest from the FP64 solution and one random frequency per ROM",
+            "gate_1e-10": bool(e.max() <= 1e-10)}
+
 
 def cpu_sample(roms, stride):
     """Every stride-th frequency of every ROM (same n / r mix as the full workload)."""
@@ -298,7 +356,7 @@ def adjoint_leg(torch, dev, h):
 
 
 def workloads_leg(torch, dev, h, reps=3):
-    """Both forms on the single-ROM workloads beside the batching one: plain (n = 64, 500
+    """All three forms on the single-ROM workloads beside the batching one: plain (n = 64, 500
     frequencies, r = 1) and precision (n = 256, 4096 frequencies, 60 % within 0.1 % of an
     eigenfrequency, r = 8, damping D).  Device time per sweep (median of reps), freq-solves/s,
     and for the mixed form the error against the oracle's refined x_ref on every 16th
@@ -313,7 +371,8 @@ def workloads_leg(torch, dev, h, reps=3):
         d = DeviceRom.from_host(rom.K, rom.M, rom.D, rom.rhs, rom.omega, device=dev)
         res = {"n": rom.n, "F": rom.F, "r": int(rom.rhs.shape[1])}
         for form, prec, flags in (("fp64", _capi.SROM_FP64, 0),
-                                  ("mixed", _capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)):
+                                  ("mixed_fp32", _capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64),
+                                  ("mixed", _capi.SROM_MIXED_TC, _capi.SROM_FLAG_FALLBACK_FP64)):
             sweep(h, [d], precision=prec, flags=flags)
             ts = []
             for _ in range(reps):
@@ -325,7 +384,7 @@ def workloads_leg(torch, dev, h, reps=3):
                 ts.append(e0.elapsed_time(e1))
             ms = float(np.median(ts))
             res[form] = {"ms": ms, "freq_solves_per_s": rom.F / (ms * 1e-3)}
-            if form == "mixed":
+            if form != "fp64":
                 sel = slice(None, None, 16)
                 X = d.solutions()[sel]
                 Xr = O.x_ref(rom.K, rom.M, rom.D, 0.0, rom.rhs, rom.omega[sel])
@@ -334,6 +393,7 @@ def workloads_leg(torch, dev, h, reps=3):
                 st = d.steps.cpu().numpy()
                 res[form]["refine_steps_hist"] = {str(k): int(v) for k, v in zip(*np.unique(st, return_counts=True))}
         res["mixed_vs_plain"] = res["mixed"]["freq_solves_per_s"] / res["fp64"]["freq_solves_per_s"]
+        res["mixed_fp32_vs_plain"] = res["mixed_fp32"]["freq_solves_per_s"] / res["fp64"]["freq_solves_per_s"]
         out[name] = res
     return out
 
@@ -452,9 +512,12 @@ def run_ours(args):
     h.set_stream(stream.cuda_stream)
     drom = [DeviceRom.from_host(r.K, r.M, r.D, r.rhs, r.omega, device=dev) for r in roms]
     FORMS = {"fp64": (_capi.SROM_FP64, 0),
-             "mixed": (_capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)}
-    forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+             "mixed_fp32": (_capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64),
+             "mixed": (_capi.SROM_MIXED_TC, _capi.SROM_FLAG_FALLBACK_FP64)}
+    forms = {"both": ["fp64", "mixed_fp32", "mixed"], "mixed": ["mixed"], "mixed_fp32": ["mixed_fp32"],
+             "fp64": ["fp64"]}[args.precision]
     headline = forms[-1]
+    x64 = None  # FP64 solutions of every system (device), the comparator of the mixed forms
 
     def barrier():
         if pg is not None:
@@ -497,10 +560,16 @@ def run_ours(args):
             a[2] += kfl
             a[3] += 1
         steps_hist = None
-        if form == "mixed":
+        acc_all = None
+        if form == "fp64":
+            x64 = [d.X.clone() for d in drom]
+        else:
             st = np.concatenate([d.steps.cpu().numpy() for d in drom])
             steps_hist = {str(k): int(v) for k, v in zip(*np.unique(st, return_counts=True))}
-        results[form] = {"ms": ms, "value": systems * world / (ms * 1e-3), "per": per, "steps": steps_hist}
+            if x64 is not None:
+                acc_all = all_systems_error(torch, drom, x64)
+        results[form] = {"ms": ms, "value": systems * world / (ms * 1e-3), "per": per, "steps": steps_hist,
+                         "accuracy_all": acc_all}
         if form == headline:
             clk = c
 
@@ -529,28 +598,34 @@ def run_ours(args):
             p64 = gemm_peak_tflops(torch, dev, torch.float64)
             info["roofline_fp64"] = roofline("fp64", p64, "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)")
         if "mixed" in results:
-            p32 = gemm_peak_tflops(torch, dev, torch.float32)
-            mp = measured_peaks()
-            bf16 = mp.get("bf16_tflops_sustained")
+            # Headline kernel: the tensor-core mixed form (Schur updates as tcgen05 MMAs), against
+            # the GPU's dense tensor ceiling (the sustained bf16 rate: the launch lasts ~1 s).
+            # achieved counts algorithmic flops (8/3 n^3 + 8 n^2 r); the tensor pipe executes eight
+            # bf16 piece products per FP32 multiply-add of the Schur updates on top of that.
+            bf16 = measured_peaks().get("bf16_tflops_sustained")
             if bf16:
-                # The compute ceiling of this GPU is its tensor cores (the sustained dense bf16
-                # rate: the mixed launch lasts over a second); the kernel runs its FP32
-                # arithmetic on the CUDA cores, so its fraction of that ceiling is small.  The
-                # fraction of the CUDA-core FP32 rate (SGEMM measured in this run) is kept beside.
-                rm = roofline("mixed", float(bf16),
-                              "MEASURED_PEAKS.json bf16_tflops_sustained (dense bf16 tensor rate under the power cap)")
-                rm["bound"] = "tensor"
+                rm = roofline("mixed", float(bf16), "MEASURED_PEAKS.json bf16_tflops_sustained "
+                                                    "(dense bf16 tensor rate under the power cap)")
             else:
-                rm = roofline("mixed", p32, "fallback: cuBLAS SGEMM 8192^3, TF32 off, measured in this run "
-                                            "(no MEASURED_PEAKS.json)")
-                rm["bound"] = "tensor"
-            rm["peak_fp32_cuda_cores"] = p32
-            rm["frac_of_fp32_cuda_cores"] = rm["achieved"] / p32
-            rm["peak_fp32_cuda_cores_source"] = "cuBLAS SGEMM 8192^3, TF32 off, measured in this run"
+                rm = roofline("mixed", 1400.0, "fallback: 1.4 PFLOP/s sustained dense bf16 (no MEASURED_PEAKS.json)")
+            rm["tensor_work_note"] = ("Schur updates run as eight bf16 piece products per FP32 multiply-add "
+                                      "(three-piece splits); panels, solves and FP64 refinement on CUDA cores")
             info["roofline_mixed"] = rm
+        if "mixed_fp32" in results:
+            p32 = gemm_peak_tflops(torch, dev, torch.float32)
+            rf = roofline("mixed_fp32", p32, "cuBLAS SGEMM 8192^3, TF32 off, measured in this run "
+                                             "(the CUDA-core FP32 rate this kernel computes at)")
+            rf["bound"] = "fp32_cuda_cores"
+            info["roofline_mixed_fp32"] = rf
         info["roofline"] = info.get("roofline_mixed") or info.get("roofline_fp64")
     precision = FORMS[headline][0]
     pflags = FORMS[headline][1]
+
+    # the oracle's x_ref on the systems farthest from the FP64 solution (and one per ROM)
+    xref = None
+    acc_all = results.get(headline, {}).get("accuracy_all")
+    if rank == 0 and acc_all is not None and not args.no_cpu_baseline:
+        xref = xref_worst(roms, drom, acc_all["per_system"])
 
     # end to end through the host-buffer C ABI call (pinned host memory)
     e2e = None
@@ -606,11 +681,12 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": "freq-solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64 LU + c128 refinement" if headline == "mixed" else "c128",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("c64 LU (tensor-core Schur updates on bf16 piece splits) + c128 refinement"
+                      if headline == "mixed" else "c64 LU + c128 refinement" if headline == "mixed_fp32" else "c128"),
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "systems_per_gpu": systems,
                        "tflop_per_step_per_gpu": flops / 1e12, "precision": headline,
-                       "refine": "complex-FP32 LU, FP64 residuals, <=5 corrections, stop when the predicted error rho*||d||/||x|| <= 2^-34 (or early once the measured contraction cannot reach it), correction solves streamed through a shared-memory strip ring, back substitution by reciprocals of diag(U), FP64 fallback; systems with n <= ~84 solved by the FP64 smem kernel",
+                       "refine": "complex-FP32 LU (tensor-core form: Schur updates as tcgen05 MMAs on three-piece bf16 splits, FP32 accumulation in TMEM), FP64 residuals, <=5 corrections, stop when the predicted error rho*||d||/||x|| <= 2^-34 (or early once the measured contraction cannot reach it), correction solves streamed through a shared-memory strip ring, back substitution by reciprocals of diag(U), FP64 fallback; systems with n <= ~84 solved by the FP64 smem kernel",
                        "l2": "inputs 167 MB + outputs 1.6 GB per step exceed L2; no flush",
                        "parallelism": f"independent batch per GPU x{world} (seed 3 + 1000003*rank)"},
             "roofline": info.get("roofline"),
@@ -620,8 +696,18 @@ def run_ours(args):
             "mixed_vs_plain": (results["mixed"]["value"] / results["fp64"]["value"]
                                if "mixed" in results and "fp64" in results else None),
             "refine_steps_hist": results.get("mixed", {}).get("steps"),
+            "mixed_fp32": ({"value": results["mixed_fp32"]["value"], "unit": "freq-solves/s",
+                            "ms_per_step": results["mixed_fp32"]["ms"],
+                            "vs_plain": (results["mixed_fp32"]["value"] / results["fp64"]["value"]
+                                         if "fp64" in results else None),
+                            "refine_steps_hist": results["mixed_fp32"]["steps"],
+                            "accuracy_vs_fp64_all_systems": (results["mixed_fp32"]["accuracy_all"] or {}).get("summary"),
+                            "roofline": info.get("roofline_mixed_fp32")}
+                           if "mixed_fp32" in results else None),
             "cpu_baseline": cpu,
             "accuracy": acc,
+            "accuracy_vs_fp64_all_systems": (acc_all or {}).get("summary"),
+            "accuracy_vs_xref": xref,
             "e2e": e2e,
             "clocks": clk.summary(),
             "gpu_launches": int(nrec),

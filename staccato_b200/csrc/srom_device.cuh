@@ -37,6 +37,21 @@ struct Item {
     int f;
 };
 
+// L2 policy for the ROM operators K, M, D: every frequency of a ROM (hence every CTA sweeping it)
+// reads them, while each CTA's own scratch matrix streams through L2 once per panel step; marked
+// evict-last they stay resident instead of being re-read from HBM by every CTA.
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ double2 ld_keep(const double2 *ptr, uint64_t pol) {
+    double2 v;
+    asm("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(ptr), "l"(pol));
+    return v;
+}
+
 __device__ __forceinline__ double2 csubmul(double2 c, double2 a, double2 b) {
     double2 o;
     o.x = __fma_rn(-a.x, b.x, __fma_rn(a.y, b.y, c.x));

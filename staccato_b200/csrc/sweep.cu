@@ -679,8 +679,9 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
             factor_global<float2, NB32, RPT>(A32, n, n, a.ldp, sm, L, nullptr, 0, PL, Xx, s_pivlg);
             info = PL.info;
             MixedWork W{X, B32, s_pos, s_ptot, reinterpret_cast<float2 *>(sm + L.dinv), sm + L.u,
-                        a.smem_dyn - (int)L.u, s_dx};  // ring: u, panel and the rest of the allocation
-            mixed_refine<RPT>(a, R, wi, w, A32, W, info, steps, berr, write_status);
+                        a.smem_dyn - (int)L.u, s_dx, n};  // ring: u, panel and the rest of the allocation
+            const RingSolve<RPT> solve{A32, n, W.ring, W.ring_bytes, W.s_dinv};
+            mixed_refine<RPT>(a, R, wi, w, A32, W, solve, info, steps, berr, write_status);
         } else {
             double2 *A64 = R.LU ? R.LU + (int64_t)wi.f * n * n
                                 : reinterpret_cast<double2 *>(a.scratch + (int64_t)blockIdx.x * a.slot_bytes);

@@ -73,10 +73,11 @@ template <typename T>
 __device__ void assemble_into(T *A, int64_t lda, const RomDev &R, double w) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double s = -__dmul_rn(w, w);
+    const uint64_t pol = l2_keep_policy();
     for (int j = warp; j < R.n; j += NW)
         for (int i = lane; i < R.n; i += 32) {
             const int64_t e = i + (int64_t)j * R.ldk;
-            A[i + j * lda] = to_store<T>(assemble_entry(R.K[e], R.M[e], R.D, e, R.eta, s, w));
+            A[i + j * lda] = to_store<T>(assemble_entry(ld_keep(R.K + e, pol), ld_keep(R.M + e, pol), R.D, e, R.eta, s, w));
         }
 }
 
@@ -251,6 +252,7 @@ __device__ void residual64(const RomDev &R, double w, const double2 *X64, float2
     const int tid = threadIdx.x;
     const int n = R.n;
     const double s = -__dmul_rn(w, w);
+    const uint64_t pol = l2_keep_policy();
     for (int c0 = 0; c0 < R.r; c0 += 4) {
         const int nc = min(4, R.r - c0);
         double2 acc[RPT][4];
@@ -270,9 +272,9 @@ __device__ void residual64(const RomDev &R, double w, const double2 *X64, float2
                 for (int jj = 0; jj < JB; ++jj) {
                     if (i < n && j0 + jj < n) {
                         const int64_t e = i + (int64_t)(j0 + jj) * R.ldk;
-                        kv[k][jj] = R.K[e];
-                        mv[k][jj] = R.M[e];
-                        dv[k][jj] = R.D ? R.D[e] : make_double2(0.0, 0.0);
+                        kv[k][jj] = ld_keep(R.K + e, pol);
+                        mv[k][jj] = ld_keep(R.M + e, pol);
+                        dv[k][jj] = R.D ? ld_keep(R.D + e, pol) : make_double2(0.0, 0.0);
                     }
                 }
             }
@@ -476,22 +478,36 @@ struct MixedWork {
     unsigned char *ring;   // staging ring of the correction solves
     int ring_bytes;
     double *s_dx;          // per right-hand side relative correction size
+    int lda;               // leading dimension of the factor
+};
+
+// Correction solve of the CUDA-core mixed kernel: the factor streamed through the strip ring.
+template <int RPT>
+struct RingSolve {
+    const float2 *A;
+    int n;
+    unsigned char *ring;
+    int ring_bytes;
+    const float2 *dinv;
+    __device__ void operator()(float2 *B, int nrhs) const { solve_ring<RPT>(A, n, B, nrhs, ring, ring_bytes, dinv); }
 };
 
 // Refinement of one system after its complex-FP32 factorisation (A32, ld n, LAPACK layout with
 // rows in the factor's order; info = the factorisation's zero-pivot report): x_0 from the FP32
-// factors, then r = b - A(w) x in FP64 and x += LU \ r until the predicted error
+// factors, then r = b - A(w) x in FP64 and x += LU \ r (solve(B32, r) replaces the right-hand
+// sides in B32 by the correction) until the predicted error
 // rho * ||d_s|| / ||x||, rho = 2 ||d_s|| / ||d_s-1||, is at most tol for every right-hand side
 // (default 2^-34), at most max_refine corrections.  Non-converged systems are appended to the
 // FP64 fallback list when one is given (write_status = false: that launch writes the results).
-template <int RPT>
+template <int RPT, class Solve>
 __device__ void mixed_refine(const GlobalArgs &a, const RomDev &R, const Item &wi, double w, const float2 *A32,
-                             const MixedWork &W, int &info, int &steps, double &berr, bool &write_status) {
+                             const MixedWork &W, const Solve &solve, int &info, int &steps, double &berr,
+                             bool &write_status) {
     const int tid = threadIdx.x;
     const int n = R.n;
     for (int l = tid; l < n; l += NT) {
         W.s_pos[W.s_ptot[l]] = l;
-        W.s_dinv[l] = CT<float2>::recip(A32[l + (int64_t)l * n]);
+        W.s_dinv[l] = CT<float2>::recip(A32[l + (int64_t)l * W.lda]);
     }
     __syncthreads();
     for (int e = tid; e < n * R.r; e += NT) {
@@ -506,7 +522,7 @@ __device__ void mixed_refine(const GlobalArgs &a, const RomDev &R, const Item &w
     double prev = 1.0;  // relative size of the previous correction (the first is x itself)
     for (int s = 0;; ++s) {
         if (s > 0) residual64<RPT>(R, w, W.X, W.B32, W.s_pos);
-        solve_ring<RPT>(A32, n, W.B32, R.r, W.ring, W.ring_bytes, W.s_dinv);
+        solve(W.B32, R.r);
         apply_correction(W.X, W.B32, n, R.r, W.s_dx);
         if (s > 0) {
             // error left after this correction ~ rho * ||d||, rho ~ ||d_s|| / ||d_{s-1}||

@@ -13,14 +13,15 @@
 // columns 0..63 hold the real parts and 64..127 the imaginary parts.
 //
 // FP32 accuracy from bf16 tensor cores.  Every FP32 operand value x is split into three bf16
-// pieces x = x0 + x1 + x2 (+ a remainder below 2^-24 |x|, each piece the round-to-nearest of
-// what the previous ones left) and the product is accumulated from the six piece products
-// a_i b_j with i + j <= 2, smallest first, into FP32 accumulators in tensor memory
-// (tcgen05.mma kind::f16, 24 MMAs of 128 x 128 x 16 per tile).  The dropped terms are below
-// 2^-25 relative, so the factor is as accurate as a CUDA-core FP32 factorisation and the FP64
-// refinement converges as fast.  (The split-operand scheme for emulating a higher precision on
-// lower-precision tensor cores is the published one of Henry, Tang and Heinecke, "Leveraging
-// the bfloat16 Artificial Intelligence Datatype For Higher-Precision Computations", 2019.)
+// pieces x = x0 + x1 + x2, each the round-to-nearest of what the previous ones left; for a
+// normal FP32 value the split is exact (8 + 8 + 8 significant bits).  The product is
+// accumulated from the eight piece products a_i b_j with i + j <= 3, smallest first, into FP32
+// accumulators in tensor memory (tcgen05.mma kind::f16, 32 MMAs of 128 x 128 x 16 per tile);
+// the one dropped term a_2 b_2 is below 2^-32 relative, so the products are exact to well
+// under an FP32 rounding and the factor is as accurate as a CUDA-core FP32 factorisation.
+// (The split-operand scheme for emulating a higher precision on lower-precision tensor cores
+// is the published one of Henry, Tang and Heinecke, "Leveraging the bfloat16 Artificial
+// Intelligence Datatype For Higher-Precision Computations", 2019.)
 //
 // Data flow of one panel step j0 (matrix in the CTA's global scratch slot, L2-resident):
 //   A  panel: columns j0..j0+31 staged in shared memory and factored (panel_factor_par); the
@@ -32,7 +33,7 @@
 //   C  Schur tiles (row tiles of 128 outer, column tiles of 64 inner): operand tiles are
 //      brought into shared memory by bulk asynchronous copies (cp.async.bulk with mbarrier
 //      completion; the A tile once per row tile, the B tiles through a 3-deep ring), one thread
-//      issues the 24 MMAs of a tile into one of two TMEM accumulators, and while the tensor
+//      issues the 32 MMAs of a tile into one of two TMEM accumulators, and while the tensor
 //      cores work on tile t all 8 warps subtract tile t-1's accumulator (tcgen05.ld) from the
 //      matrix in place.
 // No cluster, no multicast: every copy reads this GPU's own memory into this CTA.
@@ -54,39 +55,45 @@ namespace tcm {
 constexpr int NB = 32;                 // panel width (complex columns)
 constexpr int KP = 2 * NB;             // depth of the real Schur GEMM: [Re L | Im L]
 constexpr int TM = 128;                // rows of a tile (TMEM lanes)
-constexpr int TNC = 64;                // complex columns of a tile
+constexpr int TNC = 32;                // complex columns of a tile
 constexpr int TN = 2 * TNC;            // real accumulator columns of a tile: [Re | Im]
 constexpr int PIECES = 3;              // bf16 pieces per FP32 value
 constexpr int MMA_K = 16;              // depth of one kind::f16 MMA
 constexpr int KSTEPS = KP / MMA_K;     // MMAs per piece product
 constexpr int STAGES = 3;              // B-operand ring depth
-constexpr int PIECE_BYTES = 128 * KP * 2;           // one bf16 piece of a 128-row operand tile
-constexpr int TILE_BYTES = PIECES * PIECE_BYTES;    // 48 KB
-constexpr int OP_BYTES = (1 + STAGES) * TILE_BYTES; // A tile + B ring
+constexpr int A_PIECE = TM * KP * 2;                // one bf16 piece of an A tile (128 rows)
+constexpr int B_PIECE = TN * KP * 2;                // one bf16 piece of a B tile (64 rows)
+constexpr int A_TILE = PIECES * A_PIECE;            // 48 KB
+constexpr int B_TILE = PIECES * B_PIECE;            // 24 KB
+constexpr int C_TILE = TM * TNC * 8;                // 32 KB: a tile of the trailing matrix
+constexpr int OP_B = A_TILE;                        // B ring offset in the operand region
+constexpr int OP_C = OP_B + STAGES * B_TILE;        // C tiles (two) offset
+constexpr int OP_BYTES = OP_C + 2 * C_TILE;         // A tile + B ring + two C tiles
 constexpr int TMEM_COLS = 2 * TN;                   // two accumulator buffers
 constexpr int LDL = 33;                             // leading dimension of L11^-1 in smem
 constexpr int CPW = 4;                              // trailing columns per warp pass (phase B)
 constexpr int INFO_TIMEOUT = -2;
 
-// Instruction descriptor: D f32, A and B bf16, both K-major, M = 128, N = 128.
+// Instruction descriptor: D f32, A and B bf16, both K-major, M = 128, N = 64.
 constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
                            ((uint32_t)(TM >> 4) << 24);
 
 static_assert(TN % 16 == 0 && TN >= 16 && TN <= 256, "N of an M = 128 MMA");
+static_assert(TMEM_COLS >= 32 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "TMEM allocations are powers of two >= 32");
 static_assert(OP_BYTES >= (512 | 1) * NB * 8, "the panel of an n = 512 system fits the operand region");
 
 // Byte offset of element (row, k) in one operand piece: K-major core matrices of 8 rows x 16
 // bytes (8 bf16), the K-adjacent ones 128 bytes apart (LBO), the 8-row groups 1024 bytes apart
-// (SBO = 8 core matrices of the 64-deep row).
+// (SBO = 8 core matrices of the 64-deep row).  A pieces have 128 rows, B pieces 64.
 __host__ __device__ constexpr int op_off(int row, int k) {
     return (row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
 // Shared-memory layout (offsets from a 1024-byte aligned base).  The operand region holds the
-// panel during phase A, the A tile and the B ring during phase C, and the refinement's
-// iterate, right-hand sides and staging ring after the factorisation.
+// panel during phase A, the A tile, the B ring and two C tiles during phase C, and the
+// refinement's iterate, right-hand sides and staging ring after the factorisation.
 struct TcSmem {
-    size_t op, perm, ptot, pos, ipiv, moved, dinv, linv, bars, tmem, total;
+    size_t op, perm, ptot, pos, ipiv, moved, dinv, linv, bars, tmem, flags, total;
     size_t work64, work32, ring;
     static __host__ __device__ size_t up(size_t b) { return (b + 255) / 256 * 256; }
     __host__ __device__ TcSmem(int ldp, int n_max, int r_max) {
@@ -99,23 +106,31 @@ struct TcSmem {
         dinv = moved + up((size_t)2 * 2 * NB * 4);
         linv = dinv + up((size_t)ldp * 8);
         bars = linv + up((size_t)NB * LDL * 8);
-        tmem = bars + up((size_t)(1 + STAGES + 2) * 8);
-        total = tmem + 256;
+        tmem = bars + up((size_t)(1 + STAGES + 2 + 2) * 8);
+        flags = tmem + 256;
+        total = flags + up((size_t)((ldp + NB - 1) / NB) * 4);
         work64 = op;
         work32 = work64 + up((size_t)n_max * r_max * 16);
         ring = work32 + up((size_t)n_max * r_max * 8);
     }
 };
 
-// Global scratch of one CTA: the complex-FP32 matrix, then the A- and B-operand tile buffers.
+// Leading dimension of the scratch matrix: even, so that every column starts on a 16-byte
+// boundary (the C tiles are moved by bulk copies, one per column).
+__host__ __device__ constexpr int tc_lda(int n) { return n + (n & 1); }
+
+// Global scratch of one CTA: the complex-FP32 matrix (ld tc_lda(n)), the A- and B-operand tile
+// buffers, and the inverse diagonal blocks of the factor (L_bb^-1, U_bb^-1 of every 32-row
+// block b, each 32 x 32 column-major, zero outside the block) used by the correction solves.
 struct TcSlot {
-    size_t a32, abuf, bbuf, total;
+    size_t a32, abuf, bbuf, inv, total;
     __host__ __device__ TcSlot(int n_max) {
         const int mt = n_max > NB ? n_max - NB : 1;
         a32 = 0;
-        abuf = ((size_t)n_max * n_max * 8 + 1023) / 1024 * 1024;
-        bbuf = abuf + (size_t)((mt + TM - 1) / TM) * TILE_BYTES;
-        total = bbuf + (size_t)((mt + TNC - 1) / TNC) * TILE_BYTES;
+        abuf = ((size_t)tc_lda(n_max) * n_max * 8 + 1023) / 1024 * 1024;
+        bbuf = abuf + (size_t)((mt + TM - 1) / TM) * A_TILE;
+        inv = bbuf + (size_t)((mt + TNC - 1) / TNC) * B_TILE;
+        total = inv + (size_t)((n_max + NB - 1) / NB) * 2 * NB * NB * 8;
     }
 };
 
@@ -223,22 +238,25 @@ __device__ __forceinline__ float2 cfma(float2 u, float2 a, float2 b) {
 }
 
 // ---------------------------------------------------------------------------- pipeline state
-// Barrier words: bar_a (A tile), bar_full[s] (ring slot s), bar_mma[b] (accumulator b).
+// Barrier words: bar_a (A tile), bar_full[s] (ring slot s), bar_mma[b] (accumulator b),
+// bar_c[b] (C tile buffer b).
 struct Bars {
     uint32_t base;
     __device__ uint32_t a() const { return base; }
     __device__ uint32_t full(int s) const { return base + 8u * (uint32_t)(1 + s); }
     __device__ uint32_t mma(int b) const { return base + 8u * (uint32_t)(1 + STAGES + b); }
+    __device__ uint32_t c(int b) const { return base + 8u * (uint32_t)(1 + STAGES + 2 + b); }
 };
 
 // Counters that give every barrier wait its parity.  Tiles are numbered over the CTA's life
-// (g): tile g uses ring slot g % STAGES (its (g / STAGES)-th fill) and accumulator g & 1 (its
-// (g >> 1)-th commit).  All threads keep g; thread 0 (the issuer) also keeps the fill and A
-// counts for the drain after a timeout.
+// (g): tile g uses ring slot g % STAGES (its (g / STAGES)-th fill), accumulator g & 1 and C
+// buffer g & 1 (their (g >> 1)-th commit / fill).  All threads keep g; thread 0 (the issuer)
+// also keeps the fill counts for the drain after a timeout.
 struct TcState {
     int g;         // tiles issued so far
     int loaded;    // B tiles whose copies were issued (global tile numbers [0, loaded))
     int a_loads;   // A tiles issued
+    int c_loaded;  // C tiles whose copies were issued (global tile numbers [0, c_loaded))
 };
 
 __device__ __forceinline__ void set_abort(int *s_abort, int *err_flag) {
@@ -260,22 +278,90 @@ __device__ void drain(const Bars &B, const TcState &S) {
         mbar_wait(B.full(g % STAGES), (uint32_t)(g / STAGES) & 1u);
     }
     if (S.a_loads > 0) mbar_wait(B.a(), (uint32_t)(S.a_loads - 1) & 1u);
+    for (int k = 1; k <= 2 && S.c_loaded - k >= 0; ++k) {
+        const int g = S.c_loaded - k;
+        mbar_wait(B.c(g & 1), (uint32_t)(g >> 1) & 1u);
+    }
+}
+
+// ---------------------------------------------------------------------------- assembly
+// A(w) = (1 + i eta) K + (-w^2) M + (i w) D rounded to complex FP32 into A (ld lda), with the
+// FP64 arithmetic of assemble_entry.  Thread t converts the column-major entries t, t + NT, ...
+// eight at a time, every load of a batch issued before any of them is used.
+__device__ __noinline__ void assemble_fp32(float2 *A, int lda, const RomDev &R, double w) {
+    constexpr int U = 8;
+    const int n = R.n, total = n * n;
+    const double s = -__dmul_rn(w, w);
+    const uint64_t pol = l2_keep_policy();
+    for (int base = threadIdx.x; base < total; base += NT * U) {
+        double2 kv[U], mv[U], dv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int idx = base + u * NT;
+            if (idx < total) {
+                const int j = idx / n, i = idx - j * n;
+                const int64_t e = i + (int64_t)j * R.ldk;
+                kv[u] = ld_keep(R.K + e, pol);
+                mv[u] = ld_keep(R.M + e, pol);
+                dv[u] = R.D ? ld_keep(R.D + e, pol) : make_double2(0.0, 0.0);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int idx = base + u * NT;
+            if (idx < total) {
+                double2 k = kv[u];
+                if (R.eta != 0.0) {
+                    const double t1 = __dmul_rn(R.eta, k.y), t2 = __dmul_rn(R.eta, k.x);
+                    k.x = __dsub_rn(k.x, t1);
+                    k.y = __dadd_rn(k.y, t2);
+                }
+                double2 v;
+                v.x = __dadd_rn(k.x, __dmul_rn(s, mv[u].x));
+                v.y = __dadd_rn(k.y, __dmul_rn(s, mv[u].y));
+                if (R.D) {
+                    v.x = __dsub_rn(v.x, __dmul_rn(w, dv[u].y));
+                    v.y = __dadd_rn(v.y, __dmul_rn(w, dv[u].x));
+                }
+                const int j = idx / n, i = idx - j * n;
+                A[i + (int64_t)j * lda] = make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------- phase A helpers
-// L11^-1 of the factored panel (unit lower triangle of logical rows 0..31), column j by warp
-// j % NW: y = e_j, then y_i -= L[i][k] y_k for k = j..30, i > k.  Stored column-major (LDL).
-__device__ void build_linv(const float2 *P, int ldp, const int *s_perm, float2 *s_linv) {
+// Inverse diagonal blocks of the factored panel (logical rows and columns 0..bs-1): column j of
+// L11^-1 by warp j % NW (y = e_j; y_i -= L[i][k] y_k for k = j..bs-2, i > k) and of U11^-1
+// (back substitution of U y = e_j, y_k = (e_j - sum_{m>k} U[k][m] y_m) / U[k][k] for k = j..0).
+// L11^-1 goes to shared memory (phase B) and both to the CTA's global inverse buffer (the
+// correction solves), 32 x 32 column-major with zeros outside bs x bs.
+__device__ void build_inverses(const float2 *P, int ldp, const int *s_perm, int bs, float2 *s_linv,
+                               float2 *ginv) {
     using C = CT<float2>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int pr = s_perm[lane];
+    const bool act = lane < bs;
+    const int pr = act ? s_perm[lane] : 0;
     for (int j = warp; j < NB; j += NW) {
-        float2 y = lane == j ? make_float2(1.f, 0.f) : C::zero();
-        for (int k = j; k < NB - 1; ++k) {
+        float2 y = (act && lane == j) ? make_float2(1.f, 0.f) : C::zero();
+        for (int k = j; k < bs - 1; ++k) {
             const float2 yk = C::shfl(y, k, 32);
-            if (lane > k) y = C::subm(y, P[pr + (int64_t)k * ldp], yk);
+            if (act && lane > k) y = C::subm(y, P[pr + (int64_t)k * ldp], yk);
         }
-        s_linv[lane + j * LDL] = lane >= j ? y : C::zero();
+        const float2 v = (act && j < bs && lane >= j) ? y : C::zero();
+        s_linv[lane + j * LDL] = v;
+        ginv[lane + j * NB] = v;
+    }
+    for (int j = warp; j < NB; j += NW) {
+        float2 y = C::zero();
+        float2 acc = (act && lane == j) ? make_float2(1.f, 0.f) : C::zero();
+        for (int k = min(j, bs - 1); k >= 0; --k) {
+            if (lane == k) y = C::div(acc, P[pr + (int64_t)k * ldp]);
+            const float2 yk = C::shfl(y, k, 32);
+            if (act && lane < k) acc = C::subm(acc, P[pr + (int64_t)k * ldp], yk);
+        }
+        const float2 v = (act && j < bs && lane <= j) ? y : C::zero();
+        ginv[NB * NB + lane + j * NB] = v;
     }
 }
 
@@ -316,7 +402,7 @@ __device__ void build_abuf(const float2 *P, int ldp, const int *s_perm, int mt, 
                 pi_[p][t] = bfbits(b[p]);
             }
         }
-        unsigned char *tile = abuf + (size_t)rt * TILE_BYTES;
+        unsigned char *tile = abuf + (size_t)rt * A_TILE;
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
             uint4 vr, vi;
@@ -328,7 +414,7 @@ __device__ void build_abuf(const float2 *P, int ldp, const int *s_perm, int mt, 
             vi.y = pi_[p][2] | ((uint32_t)pi_[p][3] << 16);
             vi.z = pi_[p][4] | ((uint32_t)pi_[p][5] << 16);
             vi.w = pi_[p][6] | ((uint32_t)pi_[p][7] << 16);
-            unsigned char *piece = tile + (size_t)p * PIECE_BYTES;
+            unsigned char *piece = tile + (size_t)p * A_PIECE;
             *reinterpret_cast<uint4 *>(piece + op_off(rr, 8 * kc)) = vr;
             *reinterpret_cast<uint4 *>(piece + op_off(rr, 32 + 8 * kc)) = vi;
         }
@@ -336,7 +422,7 @@ __device__ void build_abuf(const float2 *P, int ldp, const int *s_perm, int mt, 
 }
 
 // Row interchanges of the panel applied to the columns left of it (LAPACK's laswp on A(:, 0:j0)).
-__device__ void swap_left(float2 *A, int n, int j0, const int *s_mdst, const int *s_msrc, int nmoved) {
+__device__ void swap_left(float2 *A, int lda, int j0, const int *s_mdst, const int *s_msrc, int nmoved) {
     constexpr int CB = 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int cb = warp * CB; cb < j0; cb += NW * CB) {
@@ -344,7 +430,7 @@ __device__ void swap_left(float2 *A, int n, int j0, const int *s_mdst, const int
 #pragma unroll
         for (int t = 0; t < CB; ++t) {
             if (cb + t < j0) {
-                const float2 *col = A + (int64_t)(cb + t) * n + j0;
+                const float2 *col = A + (int64_t)(cb + t) * lda + j0;
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     const int e = lane + 32 * q;
@@ -356,7 +442,7 @@ __device__ void swap_left(float2 *A, int n, int j0, const int *s_mdst, const int
 #pragma unroll
         for (int t = 0; t < CB; ++t) {
             if (cb + t < j0) {
-                float2 *col = A + (int64_t)(cb + t) * n + j0;
+                float2 *col = A + (int64_t)(cb + t) * lda + j0;
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     const int e = lane + 32 * q;
@@ -374,8 +460,8 @@ __device__ void swap_left(float2 *A, int n, int j0, const int *s_mdst, const int
 // U12 = L11^-1 x written to the matrix, and the column's 4M entries (Ur, Ui; -Ui, Ur) as three
 // bf16 pieces into the B-operand tiles.  After this phase rows j0+32.. of the trailing matrix
 // are in the factor's (logical) order.
-__device__ void trailing_rows(float2 *A, int n, int j0, const int *s_perm, const int *s_mdst, const int *s_msrc,
-                              int nmoved, const float2 *s_linv, unsigned char *bbuf) {
+__device__ void trailing_rows(float2 *A, int n, int lda, int j0, const int *s_perm, const int *s_mdst,
+                              const int *s_msrc, int nmoved, const float2 *s_linv, unsigned char *bbuf) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int c0 = j0 + NB;
     const int ncols = n - c0;
@@ -389,25 +475,37 @@ __device__ void trailing_rows(float2 *A, int n, int j0, const int *s_perm, const
         md[q] = mvok[q] ? j0 + s_mdst[e] : 0;
         ms[q] = mvok[q] ? j0 + s_msrc[e] : 0;
     }
+    // the next pass's loads are issued before this pass's arithmetic (two register sets)
+    float2 nx[CPW], nmv[CPW][2];
+    auto load = [&](int cb) {
+#pragma unroll
+        for (int t = 0; t < CPW; ++t) {
+            if (cb + t < ncols) {
+                const float2 *col = A + (int64_t)(c0 + cb + t) * lda;
+                nx[t] = col[prow];
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                    if (mvok[q]) nmv[t][q] = col[ms[q]];
+            } else {
+                nx[t] = make_float2(0.f, 0.f);
+            }
+        }
+    };
+    if (warp * CPW < ncols) load(warp * CPW);
     for (int cb = warp * CPW; cb < ncols; cb += NW * CPW) {
         float2 x[CPW], mv[CPW][2];
 #pragma unroll
         for (int t = 0; t < CPW; ++t) {
-            if (cb + t < ncols) {
-                const float2 *col = A + (int64_t)(c0 + cb + t) * n;
-                x[t] = col[prow];
+            x[t] = nx[t];
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
-                    if (mvok[q]) mv[t][q] = col[ms[q]];
-            } else {
-                x[t] = make_float2(0.f, 0.f);
-            }
+            for (int q = 0; q < 2; ++q) mv[t][q] = nmv[t][q];
         }
+        if (cb + NW * CPW < ncols) load(cb + NW * CPW);
         __syncwarp();
 #pragma unroll
         for (int t = 0; t < CPW; ++t) {
             if (cb + t < ncols) {
-                float2 *col = A + (int64_t)(c0 + cb + t) * n;
+                float2 *col = A + (int64_t)(c0 + cb + t) * lda;
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
                     if (mvok[q]) col[md[q]] = mv[t][q];
@@ -428,15 +526,15 @@ __device__ void trailing_rows(float2 *A, int n, int j0, const int *s_perm, const
 #pragma unroll
         for (int t = 0; t < CPW; ++t) {
             if (cb + t >= ncols) continue;
-            A[(int64_t)(c0 + cb + t) * n + j0 + lane] = u[t];
+            A[(int64_t)(c0 + cb + t) * lda + j0 + lane] = u[t];
             const int cc = cb + t, ct = cc / TNC, q = cc % TNC;
             __nv_bfloat16 pr[3], pi[3];
             split3(u[t].x, pr);
             split3(u[t].y, pi);
-            unsigned char *tile = bbuf + (size_t)ct * TILE_BYTES;
+            unsigned char *tile = bbuf + (size_t)ct * B_TILE;
 #pragma unroll
             for (int p = 0; p < 3; ++p) {
-                unsigned char *piece = tile + (size_t)p * PIECE_BYTES;
+                unsigned char *piece = tile + (size_t)p * B_PIECE;
                 const unsigned short rb = bfbits(pr[p]), ib = bfbits(pi[p]);
                 *reinterpret_cast<unsigned short *>(piece + op_off(q, lane)) = rb;
                 *reinterpret_cast<unsigned short *>(piece + op_off(TNC + q, lane)) = ib;
@@ -448,57 +546,79 @@ __device__ void trailing_rows(float2 *A, int n, int j0, const int *s_perm, const
 }
 
 // ---------------------------------------------------------------------------- phase C
+// C tile (rows r0.., complex columns c0..c0+31 of the trailing matrix) into a C buffer: one bulk
+// copy per column, issued by the lanes of warp 0 and all counted on the buffer's barrier.  A
+// column's rows are rounded up to an even count (bulk sizes are multiples of 16 bytes); the row
+// past n of an odd order is the scratch matrix's padding row.  Called by warp 0 only.
+__device__ void load_c_tile(const float2 *A, int n, int lda, int r0, int c0, uint32_t cbuf, uint32_t bar) {
+    const int lane = threadIdx.x & 31;
+    const int rows = min(TM, n - r0), rows_copy = (rows + 1) & ~1;
+    const int cols = min(TNC, n - c0);
+    if (lane == 0) mbar_expect_tx(bar, (uint32_t)(cols * rows_copy * 8));
+    __syncwarp();
+    if (lane < cols)
+        bulk_load(cbuf + (uint32_t)(lane * TM * 8), A + r0 + (int64_t)(c0 + lane) * lda, (uint32_t)(rows_copy * 8), bar);
+}
+
 // C(tile) -= accumulator: warp w reads TMEM lanes 32 (w & 3) .. +31 (its rows) and complex
-// columns 32 (w >> 2) .. +31 of the tile, 16 at a time (real parts from column c, imaginary
-// from c + 64), and updates the matrix in place (column-major: a warp's 32 rows of one column
-// are one 256-byte segment).
-__device__ void epilogue(float2 *A, int n, int r0, int c0, uint32_t tbuf, bool ok) {
+// columns 16 (w >> 2) .. +15 of the tile (real parts from accumulator column c, imaginary from
+// c + 32), takes the old values from the tile's C buffer (column-major, 128 rows) and stores the
+// results to the matrix (a warp's 32 rows of one column are one 256-byte segment).
+__device__ void epilogue(float2 *A, int n, int lda, int r0, int c0, uint32_t tbuf, const float2 *cs, bool ok) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int q4 = warp & 3, h = warp >> 2;
-    const int gr = r0 + 32 * q4 + lane;
+    const int q4 = warp & 3, cb = 16 * (warp >> 2);
+    const int row = 32 * q4 + lane, gr = r0 + row;
     const uint32_t tb = tbuf + ((uint32_t)(32 * q4) << 16);
+    float re[16], im[16];
+    tmem_ld16(tb + (uint32_t)cb, re);
+    tmem_ld16(tb + (uint32_t)(TNC + cb), im);
+    if (!ok || gr >= n) return;
+    const int gc = c0 + cb;
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
-        const int cb = 32 * h + 16 * r;
-        float re[16], im[16];
-        tmem_ld16(tb + (uint32_t)cb, re);
-        tmem_ld16(tb + (uint32_t)(TNC + cb), im);
-        if (!ok || gr >= n) continue;
-        const int gc = c0 + cb;
-        float2 cv[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-            if (gc + i < n) cv[i] = A[gr + (int64_t)(gc + i) * n];
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-            if (gc + i < n) A[gr + (int64_t)(gc + i) * n] = make_float2(cv[i].x - re[i], cv[i].y - im[i]);
-    }
+    for (int i = 0; i < 16; ++i)
+        if (gc + i < n) {
+            const float2 v = cs[row + (cb + i) * TM];
+            A[gr + (int64_t)(gc + i) * lda] = make_float2(v.x - re[i], v.y - im[i]);
+        }
 }
 
 // Schur update of rows and columns [j0 + 32, n) from the operand buffers (see the file header).
-__device__ void schur_tc(float2 *A, int n, int j0, unsigned char *op, const unsigned char *abuf,
+// Tiles t = 0..T-1 (row tiles outer): in iteration t thread 0 issues tile t's MMAs, all warps
+// run tile t-1's epilogue, then (after a CTA barrier) thread 0 refills tile t-1's B slot with
+// tile t-1+STAGES and warp 0 refills tile t-1's C buffer with tile t+1.
+__device__ void schur_tc(float2 *A, int n, int lda, int j0, unsigned char *op, const unsigned char *abuf,
                          const unsigned char *bbuf, uint32_t tmem, const Bars &B, TcState &S, int *s_abort,
                          int *err_flag) {
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5;
     const int mt = n - j0 - NB;
     const int nrt = (mt + TM - 1) / TM, nct = (mt + TNC - 1) / TNC, T = nrt * nct;
     const uint32_t opa = su32(op);
-    auto slot = [&](int s) { return opa + (uint32_t)((1 + s) * TILE_BYTES); };
+    auto slot = [&](int s) { return opa + (uint32_t)(OP_B + s * B_TILE); };
+    auto cbuf = [&](int b) { return opa + (uint32_t)(OP_C + b * C_TILE); };
+    auto tile_r0 = [&](int t) { return j0 + NB + (t / nct) * TM; };
+    auto tile_c0 = [&](int t) { return j0 + NB + (t % nct) * TNC; };
+    const float2 *cs = reinterpret_cast<const float2 *>(op + OP_C);
     const int g0 = S.g;
     if (tid == 0 && !aborted(s_abort)) {
-        mbar_expect_tx(B.a(), TILE_BYTES);
-        bulk_load(opa, abuf, TILE_BYTES, B.a());
+        mbar_expect_tx(B.a(), A_TILE);
+        bulk_load(opa, abuf, A_TILE, B.a());
         S.a_loads++;
         for (int i = 0; i < STAGES && i < T; ++i) {
             const int g = g0 + i;
-            mbar_expect_tx(B.full(g % STAGES), TILE_BYTES);
-            bulk_load(slot(g % STAGES), bbuf + (size_t)(i % nct) * TILE_BYTES, TILE_BYTES, B.full(g % STAGES));
+            mbar_expect_tx(B.full(g % STAGES), B_TILE);
+            bulk_load(slot(g % STAGES), bbuf + (size_t)(i % nct) * B_TILE, B_TILE, B.full(g % STAGES));
             S.loaded = g + 1;
         }
     }
-    // piece products (A piece, B piece), smallest first
-    constexpr int PA[6] = {2, 1, 0, 1, 0, 0};
-    constexpr int PB[6] = {0, 1, 2, 0, 1, 0};
+    if (warp == 0 && !aborted(s_abort)) {
+        for (int i = 0; i < 2 && i < T; ++i)
+            load_c_tile(A, n, lda, tile_r0(i), tile_c0(i), cbuf((g0 + i) & 1), B.c((g0 + i) & 1));
+        S.c_loaded = g0 + min(2, T);
+    }
+    // piece products (A piece, B piece), smallest first: all i + j <= 3 (a_2 b_2 dropped)
+    constexpr int NPROD = 8;
+    constexpr int PA[NPROD] = {2, 1, 2, 1, 0, 1, 0, 0};
+    constexpr int PB[NPROD] = {1, 2, 0, 1, 2, 0, 1, 0};
     for (int t = 0; t <= T; ++t) {
         const int g = g0 + t;
         if (tid == 0 && t < T && !aborted(s_abort)) {
@@ -509,8 +629,8 @@ __device__ void schur_tc(float2 *A, int n, int j0, unsigned char *op, const unsi
                 // the A tile is free once every MMA reading it has completed, i.e. tile t-1's
                 ok = mbar_wait(B.mma((g - 1) & 1), (uint32_t)((g - 1) >> 1) & 1u);
                 if (ok) {
-                    mbar_expect_tx(B.a(), TILE_BYTES);
-                    bulk_load(opa, abuf + (size_t)rt * TILE_BYTES, TILE_BYTES, B.a());
+                    mbar_expect_tx(B.a(), A_TILE);
+                    bulk_load(opa, abuf + (size_t)rt * A_TILE, A_TILE, B.a());
                     S.a_loads++;
                 }
             }
@@ -522,11 +642,11 @@ __device__ void schur_tc(float2 *A, int n, int j0, unsigned char *op, const unsi
                 const uint32_t bsl = slot(g % STAGES);
                 int acc = 0;
 #pragma unroll
-                for (int p = 0; p < 6; ++p)
+                for (int p = 0; p < NPROD; ++p)
 #pragma unroll
                     for (int ks = 0; ks < KSTEPS; ++ks) {
-                        const uint64_t ad = sdesc(opa + (uint32_t)(PA[p] * PIECE_BYTES + ks * 256));
-                        const uint64_t bd = sdesc(bsl + (uint32_t)(PB[p] * PIECE_BYTES + ks * 256));
+                        const uint64_t ad = sdesc(opa + (uint32_t)(PA[p] * A_PIECE + ks * 256));
+                        const uint64_t bd = sdesc(bsl + (uint32_t)(PB[p] * B_PIECE + ks * 256));
                         mma_bf16(d, ad, bd, (uint32_t)acc);
                         acc = 1;
                     }
@@ -537,38 +657,202 @@ __device__ void schur_tc(float2 *A, int n, int j0, unsigned char *op, const unsi
             }
         }
         if (t > 0) {
-            // epilogue of tile t-1 (its MMAs were issued one iteration ago)
+            // epilogue of tile t-1 (its MMAs were issued one iteration ago, its C tile two)
             const int tp = t - 1, gp = g - 1;
-            bool ok = !aborted(s_abort) && mbar_wait(B.mma(gp & 1), (uint32_t)(gp >> 1) & 1u);
+            bool ok = !aborted(s_abort) && mbar_wait(B.mma(gp & 1), (uint32_t)(gp >> 1) & 1u) &&
+                      mbar_wait(B.c(gp & 1), (uint32_t)(gp >> 1) & 1u);
             ok = __all_sync(FULL_MASK, ok);
             if (!ok) set_abort(s_abort, err_flag);
             tc_fence_after();
-            epilogue(A, n, j0 + NB + (tp / nct) * TM, j0 + NB + (tp % nct) * TNC, tmem + (uint32_t)((gp & 1) * TN), ok);
+            epilogue(A, n, lda, tile_r0(tp), tile_c0(tp), tmem + (uint32_t)((gp & 1) * TN),
+                     cs + (size_t)(gp & 1) * (C_TILE / 8), ok);
         }
         tc_fence_before();
         __syncthreads();
-        if (tid == 0 && t > 0 && !aborted(s_abort)) {
-            // ring slot of tile t-1 is free (its MMAs completed): fill it with tile t-1+STAGES
+        if (t > 0 && !aborted(s_abort)) {
+            // tile t-1 is done: its B slot takes tile t-1+STAGES, its C buffer tile t+1
             const int tn = t - 1 + STAGES;
-            if (tn < T) {
+            if (tid == 0 && tn < T) {
                 const int gn = g0 + tn;
-                mbar_expect_tx(B.full(gn % STAGES), TILE_BYTES);
-                bulk_load(slot(gn % STAGES), bbuf + (size_t)(tn % nct) * TILE_BYTES, TILE_BYTES, B.full(gn % STAGES));
+                mbar_expect_tx(B.full(gn % STAGES), B_TILE);
+                bulk_load(slot(gn % STAGES), bbuf + (size_t)(tn % nct) * B_TILE, B_TILE, B.full(gn % STAGES));
                 S.loaded = gn + 1;
+            }
+            if (warp == 0 && t + 1 < T) {
+                const int gc = g0 + t + 1;
+                load_c_tile(A, n, lda, tile_r0(t + 1), tile_c0(t + 1), cbuf(gc & 1), B.c(gc & 1));
+                S.c_loaded = gc + 1;
             }
         }
     }
     if (tid != 0) S.g = g0 + T;  // thread 0 counted its issues (fewer after a timeout)
 }
 
+// ---------------------------------------------------------------------------- correction solves
+// LU x = b for the complex-FP32 factor in A (ld lda, LAPACK layout, rows in the factor's order) and
+// b (n x nrhs, ld n) in shared memory; x replaces b.  Blocked by the 32-row blocks of the
+// factorisation, with the inverse diagonal blocks formed there (ginv), and run as a warp-level
+// dataflow instead of CTA-wide steps:
+//   forward  y_b = L_bb^-1 (b_b - sum_{c<b} L_bc y_c),    blocks b = w, w + 8, ... on warp w;
+//   backward x_b = U_bb^-1 (y_b - sum_{c>b} U_bc x_c),    blocks b = nb-1-w, nb-1-w-8, ...
+// A warp streams the 32 x 32 tiles its blocks need (L_bc / U_bc from the factor, then the
+// block's inverse) through its own ring of ns shared-memory tiles with cp.async, so its copies
+// run ahead of the dependencies; before using y_c (x_c) it waits for block c's flag, which the
+// owner sets after writing the block's rows of b.  Flags carry a phase that grows with every
+// solve (forward phase, backward phase + 1), so they are never reset.  Every wait is bounded.
+constexpr int DF_TILE = NB * NB;  // float2 per tile
+constexpr uint32_t DF_SPIN_LIMIT = 1u << 24;
+
+__device__ __forceinline__ bool df_wait(const int *flag, int target) {
+    for (uint32_t it = 0; it < DF_SPIN_LIMIT; ++it) {
+        if (*reinterpret_cast<const volatile int *>(flag) >= target) {
+            __threadfence_block();
+            return true;
+        }
+        __nanosleep(32);
+    }
+    return false;
+}
+
+template <int RC>
+__device__ __noinline__ void solve_df(const float2 *A, int n, int lda, float2 *B, int nrhs, const float2 *ginv,
+                                      float2 *stage, int ns, int *s_flag, int phase, int *s_abort, int *err_flag) {
+    using C = CT<float2>;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nb = (n + NB - 1) / NB;
+    float2 *ring = stage + (size_t)warp * ns * DF_TILE;
+    bool ok = true;
+    for (int dir = 0; dir < 2; ++dir) {
+        const int target = phase + dir;
+        auto block_of = [&](int k) { return dir == 0 ? warp + NW * k : nb - 1 - warp - NW * k; };
+        auto valid = [&](int k) {
+            const int b = block_of(k);
+            return b >= 0 && b < nb;
+        };
+        auto ntiles = [&](int b) { return (dir == 0 ? b : nb - 1 - b) + 1; };
+        auto col_of = [&](int t) { return dir == 0 ? t : nb - 1 - t; };
+        int ik = 0, it = 0, qi = 0;  // issue position: owned block ik, its tile it; tiles issued
+        auto issue = [&]() {
+            if (valid(ik)) {
+                const int b = block_of(ik);
+                float2 *dst = ring + (qi % ns) * DF_TILE;
+                if (it < ntiles(b) - 1) {
+                    const int row = NB * b + lane, c0 = NB * col_of(it);
+                    const int kmax = min(NB, n - c0);
+                    if (row < n)
+                        for (int kk = 0; kk < kmax; ++kk)
+                            cp_async_elem(dst + kk * NB + lane, A + row + (int64_t)(c0 + kk) * lda);
+                } else {
+                    const float2 *src = ginv + (size_t)(2 * b + dir) * DF_TILE;
+                    for (int kk = 0; kk < NB; ++kk) cp_async_elem(dst + kk * NB + lane, src + kk * NB + lane);
+                }
+                if (++it == ntiles(b)) {
+                    ++ik;
+                    it = 0;
+                }
+            }
+            cp_async_commit();
+            ++qi;
+        };
+        // backward: no block's rows of b may be overwritten before every forward reader is done,
+        // which the last block's forward flag implies
+        if (dir == 1 && !df_wait(s_flag + nb - 1, phase)) ok = false;
+        for (int q = 0; q < ns - 1; ++q) issue();
+        int q = 0;
+        float2 acc[RC];
+        for (int k = 0; valid(k); ++k) {
+            const int b = block_of(k), nt = ntiles(b);
+            const int r0 = NB * b, bs = min(NB, n - r0);
+#pragma unroll
+            for (int c = 0; c < RC; ++c)
+                if (c < nrhs) acc[c] = lane < bs ? B[r0 + lane + (int64_t)c * n] : C::zero();
+            for (int t = 0; t < nt; ++t, ++q) {
+                issue();
+                cp_async_wait_dyn(ns - 1);
+                __syncwarp();
+                const float2 *S = ring + (q % ns) * DF_TILE;
+                if (t < nt - 1) {
+                    const int cb = col_of(t), c0 = NB * cb, kmax = min(NB, n - c0);
+                    if (!df_wait(s_flag + cb, target)) ok = false;
+                    for (int kk = 0; kk < kmax; ++kk) {
+                        const float2 a = S[kk * NB + lane];
+#pragma unroll
+                        for (int c = 0; c < RC; ++c)
+                            if (c < nrhs) acc[c] = C::subm(acc[c], a, B[c0 + kk + (int64_t)c * n]);
+                    }
+                } else {
+                    if (lane < bs) {
+#pragma unroll
+                        for (int c = 0; c < RC; ++c)
+                            if (c < nrhs) B[r0 + lane + (int64_t)c * n] = acc[c];
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (int c = 0; c < RC; ++c) acc[c] = C::zero();
+                    for (int kk = 0; kk < bs; ++kk) {
+                        const float2 a = S[kk * NB + lane];
+#pragma unroll
+                        for (int c = 0; c < RC; ++c)
+                            if (c < nrhs) acc[c] = cfma(acc[c], a, B[r0 + kk + (int64_t)c * n]);
+                    }
+                    __syncwarp();
+                    if (lane < bs) {
+#pragma unroll
+                        for (int c = 0; c < RC; ++c)
+                            if (c < nrhs) B[r0 + lane + (int64_t)c * n] = acc[c];
+                    }
+                    __threadfence_block();
+                    __syncwarp();
+                    if (lane == 0) *reinterpret_cast<volatile int *>(s_flag + b) = target;
+                }
+                __syncwarp();
+            }
+        }
+        cp_async_wait<0>();
+        __syncwarp();
+    }
+    if (!__all_sync(FULL_MASK, ok)) set_abort(s_abort, err_flag);
+    __syncthreads();
+}
+
+// Correction solve of the tensor-core kernel (the launch guarantees every warp's ring at least
+// two tiles: DF_MIN_RING bytes).
+constexpr int DF_MIN_RING = 2 * NW * DF_TILE * (int)sizeof(float2);
+
+struct TcSolve {
+    const float2 *A;
+    int n, lda;
+    const float2 *ginv;
+    unsigned char *ring;
+    int ring_bytes;
+    int *s_flag;
+    int *s_phase;
+    int *s_abort;
+    int *err_flag;
+    __device__ void operator()(float2 *B, int nrhs) const {
+        const int ns = min(4, ring_bytes / (NW * DF_TILE * (int)sizeof(float2)));
+        const int phase = *s_phase;
+        float2 *st = reinterpret_cast<float2 *>(ring);
+        // right-hand sides in registers: the smallest instantiation that holds nrhs (a predicated
+        // column still costs its issue slots)
+        if (nrhs <= 1) solve_df<1>(A, n, lda, B, nrhs, ginv, st, ns, s_flag, phase, s_abort, err_flag);
+        else if (nrhs <= 2) solve_df<2>(A, n, lda, B, nrhs, ginv, st, ns, s_flag, phase, s_abort, err_flag);
+        else if (nrhs <= 4) solve_df<4>(A, n, lda, B, nrhs, ginv, st, ns, s_flag, phase, s_abort, err_flag);
+        else if (nrhs <= 8) solve_df<8>(A, n, lda, B, nrhs, ginv, st, ns, s_flag, phase, s_abort, err_flag);
+        else solve_df<RMAX_MIXED>(A, n, lda, B, nrhs, ginv, st, ns, s_flag, phase, s_abort, err_flag);
+        if (threadIdx.x == 0) *s_phase = phase + 2;  // read again only after the next CTA barrier
+    }
+};
+
 // ---------------------------------------------------------------------------- factorisation
-// Blocked LU of the complex-FP32 system in A (n x n, ld n): the same output as factor_global
+// Blocked LU of the complex-FP32 system in A (n x n, ld lda): the same output as factor_global
 // (LAPACK layout, rows in final order, s_ptot the composite permutation, s_ipiv the pivots,
 // PL.info the first zero pivot), with the Schur updates on the tensor cores.
 template <int RPT>
-__device__ void factor_tc(float2 *A, int n, int ldp, unsigned char *sm, const TcSmem &L, unsigned char *abuf,
-                          unsigned char *bbuf, PanelLists &PL, PivotXchg<float> &X, int *s_pivlg, uint32_t tmem,
-                          const Bars &B, TcState &S, int *s_abort, int *err_flag) {
+__device__ __noinline__ void factor_tc(float2 *A, int n, int lda, int ldp, unsigned char *sm, const TcSmem &L,
+                                       unsigned char *abuf, unsigned char *bbuf, float2 *ginv, PanelLists &PL,
+                                       PivotXchg<float> &X, int *s_pivlg, uint32_t tmem, const Bars &B, TcState &S,
+                                       int *s_abort, int *err_flag) {
     float2 *P = reinterpret_cast<float2 *>(sm + L.op);
     int *s_perm = reinterpret_cast<int *>(sm + L.perm);
     int *s_ptot = reinterpret_cast<int *>(sm + L.ptot);
@@ -584,7 +868,7 @@ __device__ void factor_tc(float2 *A, int n, int ldp, unsigned char *sm, const Tc
         const int m = n - j0;
         const int mt = m - NB;  // trailing rows and columns (> 0 only for full panels)
         for (int c = warp; c < nbc; c += NW)
-            for (int i = lane; i < m; i += 32) P[i + (int64_t)c * ldp] = A[(j0 + i) + (int64_t)(j0 + c) * n];
+            for (int i = lane; i < m; i += 32) P[i + (int64_t)c * ldp] = A[(j0 + i) + (int64_t)(j0 + c) * lda];
         if (tid == 0) {
             PL.nmoved = 0;
             PL.grp = 0;
@@ -593,7 +877,7 @@ __device__ void factor_tc(float2 *A, int n, int ldp, unsigned char *sm, const Tc
         panel_factor_par<float2, RPT>(P, ldp, m, nbc, s_perm, s_pivlg, s_mdst, s_msrc, PL, j0, X);
         const int nmoved = PL.nmoved;
         for (int c = warp; c < nbc; c += NW)
-            for (int i = lane; i < m; i += 32) A[(j0 + i) + (int64_t)(j0 + c) * n] = P[s_perm[i] + (int64_t)c * ldp];
+            for (int i = lane; i < m; i += 32) A[(j0 + i) + (int64_t)(j0 + c) * lda] = P[s_perm[i] + (int64_t)c * ldp];
         if (tid < nbc) s_ipiv[j0 + tid] = j0 + s_pivlg[tid] + 1;
         if (warp == NW - 1) {
             int v[2];
@@ -610,17 +894,15 @@ __device__ void factor_tc(float2 *A, int n, int ldp, unsigned char *sm, const Tc
             }
             __syncwarp();
         }
-        if (mt > 0) {
-            build_linv(P, ldp, s_perm, s_linv);
-            build_abuf(P, ldp, s_perm, mt, abuf);
-        }
-        swap_left(A, n, j0, s_mdst, s_msrc, nmoved);
+        build_inverses(P, ldp, s_perm, nbc, s_linv, ginv + (size_t)(j0 / NB) * 2 * NB * NB);
+        if (mt > 0) build_abuf(P, ldp, s_perm, mt, abuf);
+        swap_left(A, lda, j0, s_mdst, s_msrc, nmoved);
         __syncthreads();
         if (mt > 0) {
-            trailing_rows(A, n, j0, s_perm, s_mdst, s_msrc, nmoved, s_linv, bbuf);
+            trailing_rows(A, n, lda, j0, s_perm, s_mdst, s_msrc, nmoved, s_linv, bbuf);
             fence_proxy_async();  // generic writes (operand buffers, panel smem) before async-proxy use
             __syncthreads();
-            schur_tc(A, n, j0, sm + L.op, abuf, bbuf, tmem, B, S, s_abort, err_flag);
+            schur_tc(A, n, lda, j0, sm + L.op, abuf, bbuf, tmem, B, S, s_abort, err_flag);
             fence_proxy_async();  // async-proxy writes of the operand region before generic reuse
             if (aborted(s_abort)) return;
         }
@@ -636,7 +918,7 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
     __shared__ PanelLists PL;
     __shared__ PivotXchg<float> Xx;
     __shared__ double s_dx[RMAX_MIXED];
-    __shared__ int s_abort;
+    __shared__ int s_abort, s_phase;
     unsigned char *sm = sm_raw + ((1024u - (su32(sm_raw) & 1023u)) & 1023u);
     const TcSmem L(a.ldp, a.n_max, a.r_max);
     const TcSlot SL(a.n_max);
@@ -646,10 +928,16 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
     if (tid == 0) {
         mbar_init(B.a(), 1);
         for (int s = 0; s < STAGES; ++s) mbar_init(B.full(s), 1);
-        for (int b = 0; b < 2; ++b) mbar_init(B.mma(b), 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(B.mma(b), 1);
+            mbar_init(B.c(b), 1);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_abort = 0;
+        s_phase = 1;
     }
+    int *s_flag = reinterpret_cast<int *>(sm + L.flags);
+    for (int i = tid; i < (a.ldp + NB - 1) / NB; i += NT) s_flag[i] = 0;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(s_tmem)),
                      "r"(TMEM_COLS)
@@ -660,11 +948,12 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *s_tmem;
-    TcState S{0, 0, 0};
+    TcState S{0, 0, 0, 0};
     unsigned char *slotp = a.scratch + (int64_t)blockIdx.x * a.slot_bytes;
     float2 *A32 = reinterpret_cast<float2 *>(slotp + SL.a32);
     unsigned char *abuf = slotp + SL.abuf;
     unsigned char *bbuf = slotp + SL.bbuf;
+    float2 *ginv = reinterpret_cast<float2 *>(slotp + SL.inv);
 
     for (;;) {
         const int it = next_item(a.counter, &s_item);
@@ -676,9 +965,11 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
         int steps = 0, info = 0;
         double berr = 0.0;
         bool write_status = true;
-        assemble_into<float2>(A32, n, R, w);
+        const int lda = tc_lda(n);
+        assemble_fp32(A32, lda, R, w);
         __syncthreads();
-        factor_tc<RPT>(A32, n, a.ldp, sm, L, abuf, bbuf, PL, Xx, s_pivlg, tmem, B, S, &s_abort, a.err_flag);
+        factor_tc<RPT>(A32, n, lda, a.ldp, sm, L, abuf, bbuf, ginv, PL, Xx, s_pivlg, tmem, B, S, &s_abort,
+                       a.err_flag);
         __syncthreads();
         if (aborted(&s_abort)) {
             if (tid == 0 && R.info) R.info[wi.f] = INFO_TIMEOUT;
@@ -692,8 +983,15 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
                     reinterpret_cast<float2 *>(sm + L.dinv),
                     sm + L.ring,
                     (int)(OP_BYTES - L.ring),
-                    s_dx};
-        mixed_refine<RPT>(a, R, wi, w, A32, W, info, steps, berr, write_status);
+                    s_dx,
+                    lda};
+        const TcSolve solve{A32, n, lda, ginv, W.ring, W.ring_bytes, s_flag, &s_phase, &s_abort, a.err_flag};
+        mixed_refine<RPT>(a, R, wi, w, A32, W, solve, info, steps, berr, write_status);
+        __syncthreads();
+        if (aborted(&s_abort)) {
+            if (tid == 0 && R.info) R.info[wi.f] = INFO_TIMEOUT;
+            break;
+        }
         if (tid == 0 && write_status) {
             if (R.info) R.info[wi.f] = info;
             if (R.steps) R.steps[wi.f] = steps;
@@ -722,7 +1020,7 @@ bool tc_supported(int n_max, int r_max, int smem_optin, const char **why) {
     else if (r_max > MIXED_MAX_R) w = "too many right-hand sides";
     else {
         const tcm::TcSmem L(n_max | 1, n_max, r_max);
-        if (tcm::OP_BYTES < (int64_t)L.ring || tcm::OP_BYTES - (int64_t)L.ring < 2 * 16 * (int64_t)n_max * 8)
+        if (tcm::OP_BYTES < (int64_t)L.ring || tcm::OP_BYTES - (int64_t)L.ring < tcm::DF_MIN_RING)
             w = "refinement work areas exceed shared memory";
         else if (tc_smem_bytes(n_max, r_max) + GLOBAL_STATIC_SMEM > (size_t)smem_optin)
             w = "shared memory";
