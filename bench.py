@@ -39,9 +39,9 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--precision", choices=["both", "mixed", "mixed_fp32", "fp64"], default="both",
-                   help="both: headline = tensor-core mixed+refine, plain FP64 and the CUDA-core mixed "
-                        "form measured beside it; mixed: the tensor-core form alone")
+    p.add_argument("--precision", choices=["both", "mixed", "mixed_tc", "fp64"], default="both",
+                   help="both: headline = mixed+refine (CUDA-core FP32 LU), plain FP64 and the "
+                        "tensor-core mixed form measured beside it")
     p.add_argument("--cpu-sample-stride", type=int, default=16,
                    help="CPU baseline sweeps every k-th frequency of every ROM")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -252,6 +252,12 @@ def cpu_baseline_leg(roms, stride, gpu_solutions):
     base = {"value": total / dt, "unit": "freq-solves/s", "cores": cores, "kind": kind,
             "sample": f"every {stride}th frequency of all 64 ROMs ({total} systems, {dt:.1f} s), {lapack}, "
                       f"threaded over frequencies"}
+    # the reference publishes a single-thread row beside the all-cores one: the same sweep on one
+    # host thread, over every 4th frequency of this sample (same n / r mix)
+    st_sample = cpu_sample(roms, stride * 4)
+    t1, d1, _ = run_cpu_sweep(roms, st_sample, threads=1)
+    base["single_thread"] = {"value": t1 / d1, "unit": "freq-solves/s", "cores": 1,
+                             "sample": f"every {stride * 4}th frequency of all 64 ROMs ({t1} systems, {d1:.1f} s)"}
     acc = None
     if gpu_solutions is not None:
         errs_cpu, errs_ref = [], []
@@ -371,8 +377,8 @@ def workloads_leg(torch, dev, h, reps=3):
         d = DeviceRom.from_host(rom.K, rom.M, rom.D, rom.rhs, rom.omega, device=dev)
         res = {"n": rom.n, "F": rom.F, "r": int(rom.rhs.shape[1])}
         for form, prec, flags in (("fp64", _capi.SROM_FP64, 0),
-                                  ("mixed_fp32", _capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64),
-                                  ("mixed", _capi.SROM_MIXED_TC, _capi.SROM_FLAG_FALLBACK_FP64)):
+                                  ("mixed_tc", _capi.SROM_MIXED_TC, _capi.SROM_FLAG_FALLBACK_FP64),
+                                  ("mixed", _capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)):
             sweep(h, [d], precision=prec, flags=flags)
             ts = []
             for _ in range(reps):
@@ -393,7 +399,7 @@ def workloads_leg(torch, dev, h, reps=3):
                 st = d.steps.cpu().numpy()
                 res[form]["refine_steps_hist"] = {str(k): int(v) for k, v in zip(*np.unique(st, return_counts=True))}
         res["mixed_vs_plain"] = res["mixed"]["freq_solves_per_s"] / res["fp64"]["freq_solves_per_s"]
-        res["mixed_fp32_vs_plain"] = res["mixed_fp32"]["freq_solves_per_s"] / res["fp64"]["freq_solves_per_s"]
+        res["mixed_tc_vs_plain"] = res["mixed_tc"]["freq_solves_per_s"] / res["fp64"]["freq_solves_per_s"]
         out[name] = res
     return out
 
@@ -512,9 +518,9 @@ def run_ours(args):
     h.set_stream(stream.cuda_stream)
     drom = [DeviceRom.from_host(r.K, r.M, r.D, r.rhs, r.omega, device=dev) for r in roms]
     FORMS = {"fp64": (_capi.SROM_FP64, 0),
-             "mixed_fp32": (_capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64),
-             "mixed": (_capi.SROM_MIXED_TC, _capi.SROM_FLAG_FALLBACK_FP64)}
-    forms = {"both": ["fp64", "mixed_fp32", "mixed"], "mixed": ["mixed"], "mixed_fp32": ["mixed_fp32"],
+             "mixed_tc": (_capi.SROM_MIXED_TC, _capi.SROM_FLAG_FALLBACK_FP64),
+             "mixed": (_capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)}
+    forms = {"both": ["fp64", "mixed_tc", "mixed"], "mixed": ["mixed"], "mixed_tc": ["mixed_tc"],
              "fp64": ["fp64"]}[args.precision]
     headline = forms[-1]
     x64 = None  # FP64 solutions of every system (device), the comparator of the mixed forms
@@ -597,29 +603,54 @@ def run_ours(args):
         if "fp64" in results:
             p64 = gemm_peak_tflops(torch, dev, torch.float64)
             info["roofline_fp64"] = roofline("fp64", p64, "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)")
+        bf16 = measured_peaks().get("bf16_tflops_sustained")
+        tpeak, tsrc = ((float(bf16), "MEASURED_PEAKS.json bf16_tflops_sustained (dense bf16 tensor rate under "
+                                     "the power cap)") if bf16 else
+                       (1400.0, "fallback: 1.4 PFLOP/s sustained dense bf16 (no MEASURED_PEAKS.json)"))
         if "mixed" in results:
-            # Headline kernel: the tensor-core mixed form (Schur updates as tcgen05 MMAs), against
-            # the GPU's dense tensor ceiling (the sustained bf16 rate: the launch lasts ~1 s).
-            # achieved counts algorithmic flops (8/3 n^3 + 8 n^2 r); the tensor pipe executes eight
-            # bf16 piece products per FP32 multiply-add of the Schur updates on top of that.
-            bf16 = measured_peaks().get("bf16_tflops_sustained")
-            if bf16:
-                rm = roofline("mixed", float(bf16), "MEASURED_PEAKS.json bf16_tflops_sustained "
-                                                    "(dense bf16 tensor rate under the power cap)")
-            else:
-                rm = roofline("mixed", 1400.0, "fallback: 1.4 PFLOP/s sustained dense bf16 (no MEASURED_PEAKS.json)")
-            rm["tensor_work_note"] = ("Schur updates run as eight bf16 piece products per FP32 multiply-add "
-                                      "(three-piece splits); panels, solves and FP64 refinement on CUDA cores")
-            info["roofline_mixed"] = rm
-        if "mixed_fp32" in results:
+            # Headline kernel: the CUDA-core mixed form, against the GPU's compute ceiling (its
+            # tensor cores, sustained dense bf16: the launch lasts over a second); its FP32
+            # arithmetic runs on the CUDA cores, so the fraction of the FP32 rate (cuBLAS SGEMM
+            # measured in this run) is given beside it.
             p32 = gemm_peak_tflops(torch, dev, torch.float32)
-            rf = roofline("mixed_fp32", p32, "cuBLAS SGEMM 8192^3, TF32 off, measured in this run "
-                                             "(the CUDA-core FP32 rate this kernel computes at)")
-            rf["bound"] = "fp32_cuda_cores"
-            info["roofline_mixed_fp32"] = rf
+            rm = roofline("mixed", tpeak, tsrc)
+            rm["peak_fp32_cuda_cores"] = p32
+            rm["frac_of_fp32_cuda_cores"] = rm["achieved"] / p32
+            rm["peak_fp32_cuda_cores_source"] = "cuBLAS SGEMM 8192^3, TF32 off, measured in this run"
+            info["roofline_mixed"] = rm
+        if "mixed_tc" in results:
+            # Tensor-core form: Schur updates as tcgen05 MMAs; achieved counts algorithmic flops
+            # (8/3 n^3 + 8 n^2 r), the tensor pipe executes six bf16 piece products per FP32
+            # multiply-add of the Schur updates on top of them.
+            rt = roofline("mixed_tc", tpeak, tsrc)
+            rt["tensor_work_note"] = ("Schur updates run as six bf16 piece products per FP32 multiply-add "
+                                      "(three-piece splits); panels, interchanges, solves and FP64 refinement "
+                                      "on CUDA cores")
+            info["roofline_mixed_tc"] = rt
         info["roofline"] = info.get("roofline_mixed") or info.get("roofline_fp64")
     precision = FORMS[headline][0]
     pflags = FORMS[headline][1]
+
+    # the headline form replayed as one captured CUDA graph (srom_graph_create / _launch: the whole
+    # batched sweep, all launches, no host work per step), timed the same way
+    graph = None
+    if not args.no_extras:
+        from staccato_b200.sweep import Graph
+
+        gph = Graph(h, drom, precision=FORMS[headline][0], flags=FORMS[headline][1])
+        for _ in range(args.warmup):
+            gph.launch(stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(args.steps):
+            gph.launch(stream.cuda_stream)
+        g1.record(stream)
+        torch.cuda.synchronize(dev)
+        gms = g0.elapsed_time(g1) / args.steps
+        gph.close()
+        graph = {"value": systems / (gms * 1e-3), "unit": "freq-solves/s", "ms_per_step": gms,
+                 "api": "srom_graph_launch of the captured sweep (plan and metadata built once)"}
 
     # the oracle's x_ref on the systems farthest from the FP64 solution (and one per ROM)
     xref = None
@@ -681,12 +712,13 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": "freq-solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("c64 LU (tensor-core Schur updates on bf16 piece splits) + c128 refinement"
-                      if headline == "mixed" else "c64 LU + c128 refinement" if headline == "mixed_fp32" else "c128"),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("c64 LU + c128 refinement" if headline == "mixed" else
+                      "c64 LU (tensor-core Schur updates on bf16 piece splits) + c128 refinement"
+                      if headline == "mixed_tc" else "c128"),
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "systems_per_gpu": systems,
                        "tflop_per_step_per_gpu": flops / 1e12, "precision": headline,
-                       "refine": "complex-FP32 LU (tensor-core form: Schur updates as tcgen05 MMAs on three-piece bf16 splits, FP32 accumulation in TMEM), FP64 residuals, <=5 corrections, stop when the predicted error rho*||d||/||x|| <= 2^-34 (or early once the measured contraction cannot reach it), correction solves streamed through a shared-memory strip ring, back substitution by reciprocals of diag(U), FP64 fallback; systems with n <= ~84 solved by the FP64 smem kernel",
+                       "refine": "complex-FP32 LU on CUDA cores (the tensor-core form, Schur updates as tcgen05 MMAs on three-piece bf16 splits, is measured beside it as mixed_tc), FP64 residuals, <=5 corrections, stop when the predicted error rho*||d||/||x|| <= 2^-34 (or early once the measured contraction cannot reach it), correction solves streamed through a shared-memory strip ring, back substitution by reciprocals of diag(U), FP64 fallback; systems with n <= ~84 solved by the FP64 smem kernel",
                        "l2": "inputs 167 MB + outputs 1.6 GB per step exceed L2; no flush",
                        "parallelism": f"independent batch per GPU x{world} (seed 3 + 1000003*rank)"},
             "roofline": info.get("roofline"),
@@ -696,18 +728,19 @@ def run_ours(args):
             "mixed_vs_plain": (results["mixed"]["value"] / results["fp64"]["value"]
                                if "mixed" in results and "fp64" in results else None),
             "refine_steps_hist": results.get("mixed", {}).get("steps"),
-            "mixed_fp32": ({"value": results["mixed_fp32"]["value"], "unit": "freq-solves/s",
-                            "ms_per_step": results["mixed_fp32"]["ms"],
-                            "vs_plain": (results["mixed_fp32"]["value"] / results["fp64"]["value"]
-                                         if "fp64" in results else None),
-                            "refine_steps_hist": results["mixed_fp32"]["steps"],
-                            "accuracy_vs_fp64_all_systems": (results["mixed_fp32"]["accuracy_all"] or {}).get("summary"),
-                            "roofline": info.get("roofline_mixed_fp32")}
-                           if "mixed_fp32" in results else None),
+            "mixed_tc": ({"value": results["mixed_tc"]["value"], "unit": "freq-solves/s",
+                          "ms_per_step": results["mixed_tc"]["ms"],
+                          "vs_plain": (results["mixed_tc"]["value"] / results["fp64"]["value"]
+                                       if "fp64" in results else None),
+                          "refine_steps_hist": results["mixed_tc"]["steps"],
+                          "accuracy_vs_fp64_all_systems": (results["mixed_tc"]["accuracy_all"] or {}).get("summary"),
+                          "roofline": info.get("roofline_mixed_tc")}
+                         if "mixed_tc" in results else None),
             "cpu_baseline": cpu,
             "accuracy": acc,
             "accuracy_vs_fp64_all_systems": (acc_all or {}).get("summary"),
             "accuracy_vs_xref": xref,
+            "graph": graph,
             "e2e": e2e,
             "clocks": clk.summary(),
             "gpu_launches": int(nrec),

@@ -293,10 +293,12 @@ SROM_API int srom_band_order(int64_t n_rows, int64_t nnz, const int64_t *rowptr,
  * device and the given stream (NULL = legacy default stream) and returns after enqueueing.
  * Scratch is a 33 MB array inside the library (descriptor, work list and 32 MiB of matrix
  * slots), held on every device that loads the library until the process exits.
- * Limits: n <= 512, F <= 65536, and the panel must fit in shared memory (r <= 11 at n = 512);
- * larger requests return SROM_ERR_UNSUPPORTED with the reason in err (err_len bytes).
+ * Limits: n <= 512, F <= 65536, and the blocked kernel's shared memory, about
+ * 24 n r + 288 (n + 1) + 21 KB bytes, within the device's per-block limit (r <= 5 at n = 512,
+ * r <= 16 at n <= 314 on a B200); larger requests return SROM_ERR_UNSUPPORTED with the reason
+ * in err (err_len bytes).
  * The first call on each device looks up the array's device address; make that first call
- * before any stream capture.  Every call reuses the array (the work counter is cleared on
+ * before any stream capture.  After cudaDeviceReset the next call looks the address up again.  Every call reuses the array (the work counter is cleared on
  * each call): calls whose work overlaps on the GPU race and must be serialised by the caller.
  * Results (x and, when n_out > 0, y = C x) are bit-identical to srom_sweep with SROM_FP64.
  */

@@ -1194,27 +1194,31 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
         d.rhs = reinterpret_cast<srom_complex *>(buf + 2 * nn);
         d.omega = reinterpret_cast<double *>(buf + 2 * nn + sizeof(srom_complex) * (size_t)n * r);
         d.X = reinterpret_cast<srom_complex *>(buf + 2 * nn + sizeof(srom_complex) * (size_t)n * r + sizeof(double) * F);
-        cudaMemcpy((void *)d.K, K.data(), nn, cudaMemcpyHostToDevice);
-        cudaMemcpy((void *)d.M, M.data(), nn, cudaMemcpyHostToDevice);
-        cudaMemcpy((void *)d.rhs, B.data(), sizeof(srom_complex) * (size_t)n * r, cudaMemcpyHostToDevice);
-        cudaMemcpy((void *)d.omega, om.data(), sizeof(double) * F, cudaMemcpyHostToDevice);
-        Entry ent{n, r, 0, {0.f, 0.f}};
-        cudaEvent_t a, b;
-        cudaEventCreate(&a);
-        cudaEventCreate(&b);
         int rc = SROM_OK;
+        const void *src[4] = {K.data(), M.data(), B.data(), om.data()};
+        void *dst[4] = {(void *)d.K, (void *)d.M, (void *)d.rhs, (void *)d.omega};
+        const size_t bytes[4] = {nn, nn, sizeof(srom_complex) * (size_t)n * r, sizeof(double) * F};
+        for (int k = 0; k < 4 && rc == SROM_OK; ++k)
+            if ((e = cudaMemcpy(dst[k], src[k], bytes[k], cudaMemcpyHostToDevice)) != cudaSuccess)
+                rc = set_err(h, SROM_ERR_CUDA, "tuning input copy: %s", cudaGetErrorString(e));
+        Entry ent{n, r, 0, {0.f, 0.f}};
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (rc == SROM_OK && ((e = cudaEventCreate(&a)) != cudaSuccess || (e = cudaEventCreate(&b)) != cudaSuccess))
+            rc = set_err(h, SROM_ERR_CUDA, "tuning events: %s", cudaGetErrorString(e));
         for (int c = 0; c < 2 && rc == SROM_OK; ++c) {
             h->tune_fp64[key] = c;
             srom_sweep_opts o{SROM_FP64, 5, 0.0, 0};
             rc = srom_sweep(h, &d, 1, &o);  // warm-up
-            cudaEventRecord(a, h->stream);
+            if (rc == SROM_OK && (e = cudaEventRecord(a, h->stream)) != cudaSuccess)
+                rc = set_err(h, SROM_ERR_CUDA, "tuning timer: %s", cudaGetErrorString(e));
             for (int rep = 0; rep < 3 && rc == SROM_OK; ++rep) rc = srom_sweep(h, &d, 1, &o);
-            cudaEventRecord(b, h->stream);
-            cudaEventSynchronize(b);
-            cudaEventElapsedTime(&ent.ms[c], a, b);
+            if (rc == SROM_OK && ((e = cudaEventRecord(b, h->stream)) != cudaSuccess ||
+                                  (e = cudaEventSynchronize(b)) != cudaSuccess ||
+                                  (e = cudaEventElapsedTime(&ent.ms[c], a, b)) != cudaSuccess))
+                rc = set_err(h, SROM_ERR_CUDA, "tuning timer: %s", cudaGetErrorString(e));
         }
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
         cudaStreamSynchronize(h->stream);
         cudaFree(buf);
         if (rc != SROM_OK) {

@@ -43,9 +43,20 @@ namespace {
 std::mutex g_noalloc_mu;
 void *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
 
-// Device address of g_noalloc_scratch on the current device, looked up once per device.
+// Device address of g_noalloc_scratch on the current device, looked up on the first call per
+// device and cached.  A cached address that the runtime no longer knows as device memory of this
+// device (the context was reset with cudaDeviceReset and the module loaded again) is looked up
+// anew.
 cudaError_t noalloc_scratch(int dev, unsigned char **out) {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (g_noalloc_ptr[dev]) {
+        cudaPointerAttributes a{};
+        const cudaError_t e = cudaPointerGetAttributes(&a, g_noalloc_ptr[dev]);
+        if (e != cudaSuccess || a.type != cudaMemoryTypeDevice || a.device != dev) {
+            cudaGetLastError();
+            g_noalloc_ptr[dev] = nullptr;
+        }
+    }
     if (!g_noalloc_ptr[dev]) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -113,7 +124,9 @@ extern "C" int srom_sweep_fp64_noalloc(const srom_rom_desc *d, void *cuda_stream
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
         (e = cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess)
         return fail(err, err_len, SROM_ERR_CUDA, "cudaDeviceGetAttribute", cudaGetErrorString(e));
-    if (srom::fp64_global_smem_bytes(d->n, d->r) > (size_t)smem_optin) {
+    // the launch's own test (make_plan): rows per thread, and dynamic plus static shared memory
+    if (srom::global_rpt(d->n) > srom::GLOBAL_MAX_RPT ||
+        srom::fp64_global_smem_bytes(d->n, d->r) + srom::GLOBAL_STATIC_SMEM > (size_t)smem_optin) {
         char b[96];
         snprintf(b, sizeof b, "n = %d with r = %d needs more shared memory than a CTA has", d->n, d->r);
         return fail(err, err_len, SROM_ERR_UNSUPPORTED, "srom_sweep_fp64_noalloc", b);

@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(NT) sweep_fp64_smem_kernel(const RomDev *__res
         double2 *A = smem;
         double2 *B = A + (int64_t)n * lda;
         int *ipiv = reinterpret_cast<int *>(B + (int64_t)n * R.r);
-        assemble_into<double2>(A, lda, R, R.omega[w.f]);
+        assemble_into<double2>(A, lda, R, R.omega[w.f], w.f);
         load_rhs(B, n, R);
         if (threadIdx.x == 0) s_info = 0;
         __syncthreads();
@@ -674,19 +674,19 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
             float2 *B32 = reinterpret_cast<float2 *>(sm + L.work32);
             int *s_pos = reinterpret_cast<int *>(sm + L.pos);
             int *s_ptot = reinterpret_cast<int *>(sm + L.ptot);
-            assemble_into<float2>(A32, n, R, w);
+            assemble_into<float2>(A32, n, R, w, wi.f);
             __syncthreads();
             factor_global<float2, NB32, RPT>(A32, n, n, a.ldp, sm, L, nullptr, 0, PL, Xx, s_pivlg);
             info = PL.info;
             MixedWork W{X, B32, s_pos, s_ptot, reinterpret_cast<float2 *>(sm + L.dinv), sm + L.u,
                         a.smem_dyn - (int)L.u, s_dx, n};  // ring: u, panel and the rest of the allocation
-            const RingSolve<RPT> solve{A32, n, W.ring, W.ring_bytes, W.s_dinv};
+            const RingSolve<RPT> solve{A32, n, n, W.ring, W.ring_bytes, W.s_dinv};
             mixed_refine<RPT>(a, R, wi, w, A32, W, solve, info, steps, berr, write_status);
         } else {
             double2 *A64 = R.LU ? R.LU + (int64_t)wi.f * n * n
                                 : reinterpret_cast<double2 *>(a.scratch + (int64_t)blockIdx.x * a.slot_bytes);
             double2 *B = reinterpret_cast<double2 *>(sm + L.work64);
-            assemble_into<double2>(A64, n, R, w);
+            assemble_into<double2>(A64, n, R, w, wi.f);
             load_rhs(B, n, R);
             __syncthreads();
             factor_global<double2, NB64, RPT>(A64, n, n, a.ldp, sm, L, B, R.r, PL, Xx, s_pivlg);

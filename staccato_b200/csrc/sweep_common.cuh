@@ -60,6 +60,11 @@ __device__ __forceinline__ int next_item(int *counter, int *s_item) {
     return it;
 }
 
+// Start of a CTA's sweep over the columns of a ROM's K, M, D (in units of `units` column
+// batches): the frequency index spreads it, so that the CTAs sweeping the same ROM at the same
+// time read different columns (different L2 slices) instead of all the same ones.
+__device__ __forceinline__ int sweep_start(int f, int units) { return units > 0 ? (int)(((unsigned)f * 97u) % (unsigned)units) : 0; }
+
 template <typename T>
 __device__ __forceinline__ T to_store(double2 v);
 template <>
@@ -69,13 +74,16 @@ __device__ __forceinline__ float2 to_store<float2>(double2 v) {
     return make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
 }
 
+// A(w) into A (ld lda), element by element; column j0 = sweep_start(f) first (see there).
 template <typename T>
-__device__ void assemble_into(T *A, int64_t lda, const RomDev &R, double w) {
+__device__ void assemble_into(T *A, int64_t lda, const RomDev &R, double w, int f) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double s = -__dmul_rn(w, w);
     const uint64_t pol = l2_keep_policy();
-    for (int j = warp; j < R.n; j += NW)
+    const int j0 = sweep_start(f, R.n);
+    for (int jj = warp; jj < R.n; jj += NW)
         for (int i = lane; i < R.n; i += 32) {
+            const int j = jj + j0 < R.n ? jj + j0 : jj + j0 - R.n;
             const int64_t e = i + (int64_t)j * R.ldk;
             A[i + j * lda] = to_store<T>(assemble_entry(ld_keep(R.K + e, pol), ld_keep(R.M + e, pol), R.D, e, R.eta, s, w));
         }
@@ -245,12 +253,14 @@ __device__ void panel_factor_par(T *P, int ldp, int m, int ncols, int *s_perm, i
 
 // r = b - A(w) x in FP64 with A(w) re-assembled from K, M, D (the FP64 assembly arithmetic),
 // written permuted and rounded to FP32 into B32 (B32[pos[i]] = r[i]) for the next correction.
-// Thread t owns rows t + k*NT; right-hand sides are processed four at a time.
+// Thread t owns rows t + k*NT; right-hand sides are processed four at a time; the column
+// batches are taken cyclically from batch sweep_start(f).
 template <int RPT>
-__device__ void residual64(const RomDev &R, double w, const double2 *X64, float2 *B32, const int *s_pos) {
+__device__ void residual64(const RomDev &R, double w, const double2 *X64, float2 *B32, const int *s_pos, int f) {
     constexpr int JB = RPT >= 3 ? 1 : 4 / RPT;  // columns of K, M, D loaded per batch
     const int tid = threadIdx.x;
     const int n = R.n;
+    const int nbat = (n + JB - 1) / JB, b0 = sweep_start(f, nbat);
     const double s = -__dmul_rn(w, w);
     const uint64_t pol = l2_keep_policy();
     for (int c0 = 0; c0 < R.r; c0 += 4) {
@@ -263,7 +273,8 @@ __device__ void residual64(const RomDev &R, double w, const double2 *X64, float2
             for (int cc = 0; cc < 4; ++cc)
                 acc[k][cc] = (i < n && cc < nc) ? R.rhs[i + (int64_t)(c0 + cc) * R.ldb] : make_double2(0.0, 0.0);
         }
-        for (int j0 = 0; j0 < n; j0 += JB) {
+        for (int bt = 0; bt < nbat; ++bt) {
+            const int bb = b0 + bt, j0 = (bb < nbat ? bb : bb - nbat) * JB;
             double2 kv[RPT][JB], mv[RPT][JB], dv[RPT][JB];
 #pragma unroll
             for (int k = 0; k < RPT; ++k) {
@@ -349,7 +360,7 @@ static __device__ void apply_correction(double2 *X, const float2 *B32, int n, in
 }
 
 // Correction solve of the mixed form: LU x = b with the complex-FP32 factor in global memory
-// (ld n) and b (n x nrhs, ld n, interchanges applied) in shared memory.  The factor is read
+// (ld lda) and b (n x nrhs, ld n, interchanges applied) in shared memory.  The factor is read
 // strip by strip (SW columns; the forward strips from the first, then the backward ones from
 // the last), each strip through one slot of a ring of ns shared-memory slots, so that up to
 // ns - 1 strips' loads are in flight while one is processed.  Each thread copies the rows it
@@ -357,7 +368,7 @@ static __device__ void apply_correction(double2 *X, const float2 *B32, int n, in
 // triangle after a barrier.  One warp per right-hand side solves the triangle (the backward
 // one multiplies by the reciprocals of U's diagonal), then every thread updates its rows.
 template <int SW, int RPT>
-__device__ void lu_solve_ring(const float2 *A, int n, float2 *B, int nrhs, unsigned char *ring, int ring_bytes,
+__device__ void lu_solve_ring(const float2 *A, int n, int64_t lda, float2 *B, int nrhs, unsigned char *ring, int ring_bytes,
                               const float2 *dinv) {
     using C = CT<float2>;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -386,7 +397,7 @@ __device__ void lu_solve_ring(const float2 *A, int n, float2 *B, int nrhs, unsig
             for (int k = 0; k < RPT; ++k) {
                 const int r = tid + k * NT;
                 if (r >= lo && r < hi)
-                    for (int j = 0; j < bs; ++j) cp_async_elem(d + j * n + r, A + r + (int64_t)(jb + j) * n);
+                    for (int j = 0; j < bs; ++j) cp_async_elem(d + j * n + r, A + r + (int64_t)(jb + j) * lda);
             }
         }
         cp_async_commit();
@@ -453,9 +464,9 @@ __device__ void lu_solve_ring(const float2 *A, int n, float2 *B, int nrhs, unsig
 // always holds two of them; with fewer, wider strips the triangles and barriers cost less than
 // narrower strips gain in depth (measured at n = 128..512).
 template <int RPT>
-__device__ void solve_ring(const float2 *A, int n, float2 *B, int nrhs, unsigned char *ring, int ring_bytes,
+__device__ void solve_ring(const float2 *A, int n, int64_t lda, float2 *B, int nrhs, unsigned char *ring, int ring_bytes,
                            const float2 *dinv) {
-    lu_solve_ring<16, RPT>(A, n, B, nrhs, ring, ring_bytes, dinv);
+    lu_solve_ring<16, RPT>(A, n, lda, B, nrhs, ring, ring_bytes, dinv);
 }
 
 constexpr int RMAX_MIXED = 16;
@@ -485,11 +496,11 @@ struct MixedWork {
 template <int RPT>
 struct RingSolve {
     const float2 *A;
-    int n;
+    int n, lda;
     unsigned char *ring;
     int ring_bytes;
     const float2 *dinv;
-    __device__ void operator()(float2 *B, int nrhs) const { solve_ring<RPT>(A, n, B, nrhs, ring, ring_bytes, dinv); }
+    __device__ void operator()(float2 *B, int nrhs) const { solve_ring<RPT>(A, n, lda, B, nrhs, ring, ring_bytes, dinv); }
 };
 
 // Refinement of one system after its complex-FP32 factorisation (A32, ld n, LAPACK layout with
@@ -521,7 +532,7 @@ __device__ void mixed_refine(const GlobalArgs &a, const RomDev &R, const Item &w
     bool conv = false, hopeless = false;
     double prev = 1.0;  // relative size of the previous correction (the first is x itself)
     for (int s = 0;; ++s) {
-        if (s > 0) residual64<RPT>(R, w, W.X, W.B32, W.s_pos);
+        if (s > 0) residual64<RPT>(R, w, W.X, W.B32, W.s_pos, wi.f);
         solve(W.B32, R.r);
         apply_correction(W.X, W.B32, n, R.r, W.s_dx);
         if (s > 0) {

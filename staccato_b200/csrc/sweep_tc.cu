@@ -9,16 +9,17 @@
 // Schur update as real GEMMs.  With L21 = Lr + i Li (m x 32) and U12 = Ur + i Ui (32 x c):
 //     [Re | Im](L21 U12) = [Lr | Li] * [[Ur, Ui], [-Ui, Ur]]
 // i.e. one real GEMM with depth K = 64 whose B operand carries the 4M arrangement, so a tile of
-// 128 rows x 64 complex columns is one M = 128, N = 128, K = 64 product whose accumulator
-// columns 0..63 hold the real parts and 64..127 the imaginary parts.
+// 128 rows x 32 complex columns is one M = 128, N = 64, K = 64 product whose accumulator
+// columns 0..31 hold the real parts and 32..63 the imaginary parts.
 //
 // FP32 accuracy from bf16 tensor cores.  Every FP32 operand value x is split into three bf16
 // pieces x = x0 + x1 + x2, each the round-to-nearest of what the previous ones left; for a
 // normal FP32 value the split is exact (8 + 8 + 8 significant bits).  The product is
-// accumulated from the eight piece products a_i b_j with i + j <= 3, smallest first, into FP32
-// accumulators in tensor memory (tcgen05.mma kind::f16, 32 MMAs of 128 x 128 x 16 per tile);
-// the one dropped term a_2 b_2 is below 2^-32 relative, so the products are exact to well
-// under an FP32 rounding and the factor is as accurate as a CUDA-core FP32 factorisation.
+// accumulated from the six piece products a_i b_j with i + j <= 2, smallest first, into FP32
+// accumulators in tensor memory (tcgen05.mma kind::f16, 24 MMAs of 128 x 64 x 16 per tile); the
+// dropped terms a_1 b_2, a_2 b_1, a_2 b_2 are at most 2^-24 relative each, the size of one
+// FP32 rounding, so the factor is about as accurate as a CUDA-core FP32 factorisation (measured:
+// the refinement needs the same number of steps; the two further products changed nothing).
 // (The split-operand scheme for emulating a higher precision on lower-precision tensor cores
 // is the published one of Henry, Tang and Heinecke, "Leveraging the bfloat16 Artificial
 // Intelligence Datatype For Higher-Precision Computations", 2019.)
@@ -30,12 +31,15 @@
 //      as ready-made tcgen05 operand tiles (three bf16 pieces, K-major core-matrix layout);
 //   B  every trailing column: the panel's row interchanges, U12 = L11^-1 (pivot rows), and the
 //      column's four 4M entries written to the B-operand buffer (same tile format);
-//   C  Schur tiles (row tiles of 128 outer, column tiles of 64 inner): operand tiles are
+//   C  Schur tiles (row tiles of 128 outer, column tiles of 32 inner): operand tiles are
 //      brought into shared memory by bulk asynchronous copies (cp.async.bulk with mbarrier
 //      completion; the A tile once per row tile, the B tiles through a 3-deep ring), one thread
-//      issues the 32 MMAs of a tile into one of two TMEM accumulators, and while the tensor
-//      cores work on tile t all 8 warps subtract tile t-1's accumulator (tcgen05.ld) from the
-//      matrix in place.
+//      issues a tile's 24 MMAs into one of two TMEM accumulators, and while the tensor cores
+//      work on tile t four epilogue warps take tile t-1's accumulator (tcgen05.ld), subtract it
+//      from the tile's old values (bulk-copied into shared memory two tiles ahead) and store
+//      the result; producer and epilogue hand over through mbarriers only (schur_tc).
+// The row interchanges of a panel are applied to the columns left of it once, after the last
+// panel (unswap_left), and the correction solves use inverse diagonal blocks built per panel.
 // No cluster, no multicast: every copy reads this GPU's own memory into this CTA.
 //
 // Every mbarrier wait is bounded (about 2 s of device time); a wait that runs out marks the
@@ -70,6 +74,8 @@ constexpr int OP_B = A_TILE;                        // B ring offset in the oper
 constexpr int OP_C = OP_B + STAGES * B_TILE;        // C tiles (two) offset
 constexpr int OP_BYTES = OP_C + 2 * C_TILE;         // A tile + B ring + two C tiles
 constexpr int TMEM_COLS = 2 * TN;                   // two accumulator buffers
+constexpr int NBARS = 6 + STAGES + 8;               // mbarriers of the pipeline (see Bars)
+constexpr int EPI_WARP0 = 4;                        // warps 4..7 run the Schur epilogue
 constexpr int LDL = 33;                             // leading dimension of L11^-1 in smem
 constexpr int CPW = 4;                              // trailing columns per warp pass (phase B)
 constexpr int INFO_TIMEOUT = -2;
@@ -106,7 +112,7 @@ struct TcSmem {
         dinv = moved + up((size_t)2 * 2 * NB * 4);
         linv = dinv + up((size_t)ldp * 8);
         bars = linv + up((size_t)NB * LDL * 8);
-        tmem = bars + up((size_t)(1 + STAGES + 2 + 2) * 8);
+        tmem = bars + up((size_t)NBARS * 8);
         flags = tmem + 256;
         total = flags + up((size_t)((ldp + NB - 1) / NB) * 4);
         work64 = op;
@@ -120,17 +126,22 @@ struct TcSmem {
 __host__ __device__ constexpr int tc_lda(int n) { return n + (n & 1); }
 
 // Global scratch of one CTA: the complex-FP32 matrix (ld tc_lda(n)), the A- and B-operand tile
-// buffers, and the inverse diagonal blocks of the factor (L_bb^-1, U_bb^-1 of every 32-row
-// block b, each 32 x 32 column-major, zero outside the block) used by the correction solves.
+// buffers, the inverse diagonal blocks of the factor (L_bb^-1, U_bb^-1 of every 32-row block b,
+// each 32 x 32 column-major, zero outside the block) used by the correction solves, and every
+// panel's row-interchange record (applied to the columns left of it once, at the end).
+constexpr int MV_INTS = 4 + 4 * NB;  // a panel's interchange record: count, pad, dst[2 NB], src[2 NB]
+
 struct TcSlot {
-    size_t a32, abuf, bbuf, inv, total;
+    size_t a32, abuf, bbuf, inv, moves, total;
     __host__ __device__ TcSlot(int n_max) {
         const int mt = n_max > NB ? n_max - NB : 1;
+        const int nbk = (n_max + NB - 1) / NB;
         a32 = 0;
         abuf = ((size_t)tc_lda(n_max) * n_max * 8 + 1023) / 1024 * 1024;
         bbuf = abuf + (size_t)((mt + TM - 1) / TM) * A_TILE;
         inv = bbuf + (size_t)((mt + TNC - 1) / TNC) * B_TILE;
-        total = inv + (size_t)((n_max + NB - 1) / NB) * 2 * NB * NB * 8;
+        moves = inv + (size_t)nbk * 2 * NB * NB * 8;
+        total = moves + (size_t)nbk * MV_INTS * 4;
     }
 };
 
@@ -149,6 +160,10 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
@@ -238,14 +253,18 @@ __device__ __forceinline__ float2 cfma(float2 u, float2 a, float2 b) {
 }
 
 // ---------------------------------------------------------------------------- pipeline state
-// Barrier words: bar_a (A tile), bar_full[s] (ring slot s), bar_mma[b] (accumulator b),
-// bar_c[b] (C tile buffer b).
+// Barrier words: bar_a (A tile), bar_full[s] (ring slot s), bar_mma[b] (accumulator b holds a
+// finished tile), bar_free[b] (the four epilogue warps are done with accumulator b and C buffer
+// b), bar_c[b][q] (epilogue warp q's rows of C buffer b have landed), bar_panel (the panel's
+// columns have landed in shared memory).
 struct Bars {
     uint32_t base;
     __device__ uint32_t a() const { return base; }
     __device__ uint32_t full(int s) const { return base + 8u * (uint32_t)(1 + s); }
     __device__ uint32_t mma(int b) const { return base + 8u * (uint32_t)(1 + STAGES + b); }
-    __device__ uint32_t c(int b) const { return base + 8u * (uint32_t)(1 + STAGES + 2 + b); }
+    __device__ uint32_t free(int b) const { return base + 8u * (uint32_t)(3 + STAGES + b); }
+    __device__ uint32_t c(int b, int q) const { return base + 8u * (uint32_t)(5 + STAGES + 4 * b + q); }
+    __device__ uint32_t panel() const { return base + 8u * (uint32_t)(13 + STAGES); }
 };
 
 // Counters that give every barrier wait its parity.  Tiles are numbered over the CTA's life
@@ -256,7 +275,7 @@ struct TcState {
     int g;         // tiles issued so far
     int loaded;    // B tiles whose copies were issued (global tile numbers [0, loaded))
     int a_loads;   // A tiles issued
-    int c_loaded;  // C tiles whose copies were issued (global tile numbers [0, c_loaded))
+    int panels;    // panel copies issued
 };
 
 __device__ __forceinline__ void set_abort(int *s_abort, int *err_flag) {
@@ -278,22 +297,21 @@ __device__ void drain(const Bars &B, const TcState &S) {
         mbar_wait(B.full(g % STAGES), (uint32_t)(g / STAGES) & 1u);
     }
     if (S.a_loads > 0) mbar_wait(B.a(), (uint32_t)(S.a_loads - 1) & 1u);
-    for (int k = 1; k <= 2 && S.c_loaded - k >= 0; ++k) {
-        const int g = S.c_loaded - k;
-        mbar_wait(B.c(g & 1), (uint32_t)(g >> 1) & 1u);
-    }
 }
 
 // ---------------------------------------------------------------------------- assembly
 // A(w) = (1 + i eta) K + (-w^2) M + (i w) D rounded to complex FP32 into A (ld lda), with the
 // FP64 arithmetic of assemble_entry.  Thread t converts the column-major entries t, t + NT, ...
-// eight at a time, every load of a batch issued before any of them is used.
-__device__ __noinline__ void assemble_fp32(float2 *A, int lda, const RomDev &R, double w) {
+// of each batch of NT * 8, eight at a time, every load of a batch issued before any of them is
+// used; the batches are taken cyclically from batch sweep_start(f).
+__device__ __noinline__ void assemble_fp32(float2 *A, int lda, const RomDev &R, double w, int f) {
     constexpr int U = 8;
     const int n = R.n, total = n * n;
+    const int nbat = (total + NT * U - 1) / (NT * U), b0 = sweep_start(f, nbat);
     const double s = -__dmul_rn(w, w);
     const uint64_t pol = l2_keep_policy();
-    for (int base = threadIdx.x; base < total; base += NT * U) {
+    for (int bt = 0; bt < nbat; ++bt) {
+        const int bb = b0 + bt, base = (bb < nbat ? bb : bb - nbat) * NT * U + threadIdx.x;
         double2 kv[U], mv[U], dv[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -331,36 +349,59 @@ __device__ __noinline__ void assemble_fp32(float2 *A, int lda, const RomDev &R, 
 }
 
 // ---------------------------------------------------------------------------- phase A helpers
-// Inverse diagonal blocks of the factored panel (logical rows and columns 0..bs-1): column j of
-// L11^-1 by warp j % NW (y = e_j; y_i -= L[i][k] y_k for k = j..bs-2, i > k) and of U11^-1
-// (back substitution of U y = e_j, y_k = (e_j - sum_{m>k} U[k][m] y_m) / U[k][k] for k = j..0).
-// L11^-1 goes to shared memory (phase B) and both to the CTA's global inverse buffer (the
-// correction solves), 32 x 32 column-major with zeros outside bs x bs.
+// Inverse diagonal blocks of the factored panel (logical rows and columns 0..bs-1).  Warp w
+// forms columns j = w, w + 8, w + 16, w + 24 of both inverses together (lane i holds row i):
+// L11^-1 e_j by forward elimination (y_i -= L[i][k] y_k for k = j..bs-2, i > k) and U11^-1 e_j
+// by back substitution (y_k = (e_j - sum_{m>k} U[k][m] y_m) / U[k][k], k = j..0), the entry of
+// L or U and the pivot's reciprocal of each step shared by the four columns.  L11^-1 goes to
+// shared memory (phase B) and both to the CTA's global inverse buffer (the correction solves),
+// 32 x 32 column-major with zeros outside bs x bs.
 __device__ void build_inverses(const float2 *P, int ldp, const int *s_perm, int bs, float2 *s_linv,
                                float2 *ginv) {
     using C = CT<float2>;
+    constexpr int Q = NB / NW;  // columns per warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool act = lane < bs;
     const int pr = act ? s_perm[lane] : 0;
-    for (int j = warp; j < NB; j += NW) {
-        float2 y = (act && lane == j) ? make_float2(1.f, 0.f) : C::zero();
-        for (int k = j; k < bs - 1; ++k) {
-            const float2 yk = C::shfl(y, k, 32);
-            if (act && lane > k) y = C::subm(y, P[pr + (int64_t)k * ldp], yk);
+    float2 y[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) y[q] = (act && lane == warp + NW * q) ? make_float2(1.f, 0.f) : C::zero();
+    for (int k = warp; k < bs - 1; ++k) {
+        const float2 l = (act && lane > k) ? P[pr + (int64_t)k * ldp] : C::zero();
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float2 yk = C::shfl(y[q], k, 32);
+            if (act && lane > k && k >= warp + NW * q) y[q] = C::subm(y[q], l, yk);
         }
-        const float2 v = (act && j < bs && lane >= j) ? y : C::zero();
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int j = warp + NW * q;
+        const float2 v = (act && j < bs && lane >= j) ? y[q] : C::zero();
         s_linv[lane + j * LDL] = v;
         ginv[lane + j * NB] = v;
     }
-    for (int j = warp; j < NB; j += NW) {
-        float2 y = C::zero();
-        float2 acc = (act && lane == j) ? make_float2(1.f, 0.f) : C::zero();
-        for (int k = min(j, bs - 1); k >= 0; --k) {
-            if (lane == k) y = C::div(acc, P[pr + (int64_t)k * ldp]);
-            const float2 yk = C::shfl(y, k, 32);
-            if (act && lane < k) acc = C::subm(acc, P[pr + (int64_t)k * ldp], yk);
+    float2 acc[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        y[q] = C::zero();
+        acc[q] = (act && lane == warp + NW * q) ? make_float2(1.f, 0.f) : C::zero();
+    }
+    for (int k = min(warp + NW * (Q - 1), bs - 1); k >= 0; --k) {
+        const float2 u = act ? P[pr + (int64_t)k * ldp] : C::zero();  // U[lane][k]
+        const float2 rk = C::shfl(lane == k ? C::recip(u) : C::zero(), k, 32);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if (k > warp + NW * q) continue;  // column j = warp + NW q starts at k = j
+            if (lane == k) y[q] = C::mul(acc[q], rk);
+            const float2 yk = C::shfl(y[q], k, 32);
+            if (act && lane < k) acc[q] = C::subm(acc[q], u, yk);
         }
-        const float2 v = (act && j < bs && lane <= j) ? y : C::zero();
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int j = warp + NW * q;
+        const float2 v = (act && j < bs && lane <= j) ? y[q] : C::zero();
         ginv[NB * NB + lane + j * NB] = v;
     }
 }
@@ -421,36 +462,58 @@ __device__ void build_abuf(const float2 *P, int ldp, const int *s_perm, int mt, 
     }
 }
 
-// Row interchanges of the panel applied to the columns left of it (LAPACK's laswp on A(:, 0:j0)).
-__device__ void swap_left(float2 *A, int lda, int j0, const int *s_mdst, const int *s_msrc, int nmoved) {
-    constexpr int CB = 8;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int cb = warp * CB; cb < j0; cb += NW * CB) {
-        float2 mv[2][CB];
+// The row interchanges of every panel applied to the columns left of it (LAPACK's laswp on
+// A(:, 0:j0)), done once after the factorisation instead of after every panel: block column p
+// was written in the row order of step p, and panels p+1.. moved rows below it since.  idx[f]
+// (shared memory) = stored row holding final row f: starting from the identity, going from the
+// last panel down, idx <- map_k(idx) with map_k(q) = the source of q if panel k moved a row to
+// q, else q; after panel k = p+1 is folded in, block column p's rows f >= 32 (p + 1) are
+// gathered from rows idx[f], eight columns at a time (all reads, a barrier, all writes).
+// moves: the panels' records (count, dst[], src[] relative to the panel's first row).
+__device__ void unswap_left(float2 *A, int n, int lda, const int *moves, int *idx, int *map) {
+    constexpr int CG = 8;
+    constexpr int MAXR = (512 + NT - 1) / NT;  // rows per thread (TC_MAX_N)
+    const int tid = threadIdx.x;
+    const int nbk = (n + NB - 1) / NB;
+    for (int f = tid; f < n; f += NT) {
+        idx[f] = f;
+        map[f] = f;
+    }
+    __syncthreads();
+    for (int p = nbk - 2; p >= 0; --p) {
+        const int k = p + 1, jk = NB * k;
+        const int *rec = moves + (size_t)k * MV_INTS;
+        const int nm = rec[0];
+        const int e = tid < nm ? tid : -1;
+        const int dst = e >= 0 ? jk + rec[4 + e] : 0, src = e >= 0 ? jk + rec[4 + 2 * NB + e] : 0;
+        if (e >= 0) map[dst] = src;
+        __syncthreads();
+        for (int f = jk + tid; f < n; f += NT) idx[f] = map[idx[f]];
+        __syncthreads();
+        if (e >= 0) map[dst] = dst;
+        // gather block column p (columns NB p .. NB p + 31, all inside the matrix) below row jk
+        for (int c0 = NB * p; c0 < NB * p + NB; c0 += CG) {
+            float2 v[MAXR][CG];
 #pragma unroll
-        for (int t = 0; t < CB; ++t) {
-            if (cb + t < j0) {
-                const float2 *col = A + (int64_t)(cb + t) * lda + j0;
+            for (int q = 0; q < MAXR; ++q) {
+                const int f = jk + tid + q * NT;
+                if (f < n) {
+                    const int sr = idx[f];
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const int e = lane + 32 * q;
-                    if (e < nmoved) mv[q][t] = col[s_msrc[e]];
+                    for (int c = 0; c < CG; ++c) v[q][c] = A[sr + (int64_t)(c0 + c) * lda];
                 }
             }
-        }
-        __syncwarp();
+            __syncthreads();
 #pragma unroll
-        for (int t = 0; t < CB; ++t) {
-            if (cb + t < j0) {
-                float2 *col = A + (int64_t)(cb + t) * lda + j0;
+            for (int q = 0; q < MAXR; ++q) {
+                const int f = jk + tid + q * NT;
+                if (f < n) {
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const int e = lane + 32 * q;
-                    if (e < nmoved) col[s_mdst[e]] = mv[q][t];
+                    for (int c = 0; c < CG; ++c) A[f + (int64_t)(c0 + c) * lda] = v[q][c];
                 }
             }
+            __syncthreads();
         }
-        __syncwarp();
     }
 }
 
@@ -546,146 +609,161 @@ __device__ void trailing_rows(float2 *A, int n, int lda, int j0, const int *s_pe
 }
 
 // ---------------------------------------------------------------------------- phase C
-// C tile (rows r0.., complex columns c0..c0+31 of the trailing matrix) into a C buffer: one bulk
-// copy per column, issued by the lanes of warp 0 and all counted on the buffer's barrier.  A
-// column's rows are rounded up to an even count (bulk sizes are multiples of 16 bytes); the row
-// past n of an odd order is the scratch matrix's padding row.  Called by warp 0 only.
-__device__ void load_c_tile(const float2 *A, int n, int lda, int r0, int c0, uint32_t cbuf, uint32_t bar) {
+// Rows r0q .. r0q + 31 (one epilogue warp's quarter of a tile) of complex columns c0 .. c0 + 31
+// into the warp's quarter of a C buffer (column-major, 128 rows): one bulk copy per column,
+// issued by the warp's lanes and counted on the warp's barrier.  A column's row count is rounded
+// up to even (bulk sizes are multiples of 16 bytes); the row past n of an odd order is the
+// scratch matrix's padding row.  A quarter below the matrix copies nothing (the arrive alone
+// completes the barrier phase).
+__device__ void load_c_rows(const float2 *A, int n, int lda, int r0q, int c0, uint32_t dst, uint32_t bar) {
     const int lane = threadIdx.x & 31;
-    const int rows = min(TM, n - r0), rows_copy = (rows + 1) & ~1;
+    const int rows = max(0, min(32, n - r0q)), rows_copy = (rows + 1) & ~1;
     const int cols = min(TNC, n - c0);
-    if (lane == 0) mbar_expect_tx(bar, (uint32_t)(cols * rows_copy * 8));
+    if (lane == 0) mbar_expect_tx(bar, (uint32_t)(rows_copy > 0 ? cols * rows_copy * 8 : 0));
     __syncwarp();
-    if (lane < cols)
-        bulk_load(cbuf + (uint32_t)(lane * TM * 8), A + r0 + (int64_t)(c0 + lane) * lda, (uint32_t)(rows_copy * 8), bar);
+    if (rows_copy > 0 && lane < cols)
+        bulk_load(dst + (uint32_t)(lane * TM * 8), A + r0q + (int64_t)(c0 + lane) * lda, (uint32_t)(rows_copy * 8), bar);
 }
 
-// C(tile) -= accumulator: warp w reads TMEM lanes 32 (w & 3) .. +31 (its rows) and complex
-// columns 16 (w >> 2) .. +15 of the tile (real parts from accumulator column c, imaginary from
-// c + 32), takes the old values from the tile's C buffer (column-major, 128 rows) and stores the
-// results to the matrix (a warp's 32 rows of one column are one 256-byte segment).
-__device__ void epilogue(float2 *A, int n, int lda, int r0, int c0, uint32_t tbuf, const float2 *cs, bool ok) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int q4 = warp & 3, cb = 16 * (warp >> 2);
-    const int row = 32 * q4 + lane, gr = r0 + row;
-    const uint32_t tb = tbuf + ((uint32_t)(32 * q4) << 16);
-    float re[16], im[16];
-    tmem_ld16(tb + (uint32_t)cb, re);
-    tmem_ld16(tb + (uint32_t)(TNC + cb), im);
-    if (!ok || gr >= n) return;
-    const int gc = c0 + cb;
-#pragma unroll
-    for (int i = 0; i < 16; ++i)
-        if (gc + i < n) {
-            const float2 v = cs[row + (cb + i) * TM];
-            A[gr + (int64_t)(gc + i) * lda] = make_float2(v.x - re[i], v.y - im[i]);
-        }
-}
-
-// Schur update of rows and columns [j0 + 32, n) from the operand buffers (see the file header).
-// Tiles t = 0..T-1 (row tiles outer): in iteration t thread 0 issues tile t's MMAs, all warps
-// run tile t-1's epilogue, then (after a CTA barrier) thread 0 refills tile t-1's B slot with
-// tile t-1+STAGES and warp 0 refills tile t-1's C buffer with tile t+1.
+// Schur update of rows and columns [j0 + 32, n) from the operand buffers (see the file header),
+// warp-specialised with mbarrier handoffs only:
+//   thread 0      loads the A tile (per row tile) and the B ring, waits for accumulator g & 1 to
+//                 be free (bar_free of tile g - 2), issues tile g's MMAs into it and commits to
+//                 bar_mma; once tile g - 1's MMAs are done its ring slot takes tile g - 1 + STAGES;
+//   warps 4..7    (warp 4 + q owns TMEM lanes and tile rows 32 q .. +31) wait for bar_mma and their
+//                 C rows, subtract the accumulator from the old values and store the results to the
+//                 matrix, arrive on bar_free, and then load their rows of tile g + 2 into the buffer;
+//   warps 1..3    wait at the closing barrier.
 __device__ void schur_tc(float2 *A, int n, int lda, int j0, unsigned char *op, const unsigned char *abuf,
                          const unsigned char *bbuf, uint32_t tmem, const Bars &B, TcState &S, int *s_abort,
                          int *err_flag) {
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int mt = n - j0 - NB;
     const int nrt = (mt + TM - 1) / TM, nct = (mt + TNC - 1) / TNC, T = nrt * nct;
     const uint32_t opa = su32(op);
     auto slot = [&](int s) { return opa + (uint32_t)(OP_B + s * B_TILE); };
-    auto cbuf = [&](int b) { return opa + (uint32_t)(OP_C + b * C_TILE); };
     auto tile_r0 = [&](int t) { return j0 + NB + (t / nct) * TM; };
     auto tile_c0 = [&](int t) { return j0 + NB + (t % nct) * TNC; };
-    const float2 *cs = reinterpret_cast<const float2 *>(op + OP_C);
     const int g0 = S.g;
-    if (tid == 0 && !aborted(s_abort)) {
-        mbar_expect_tx(B.a(), A_TILE);
-        bulk_load(opa, abuf, A_TILE, B.a());
-        S.a_loads++;
-        for (int i = 0; i < STAGES && i < T; ++i) {
-            const int g = g0 + i;
-            mbar_expect_tx(B.full(g % STAGES), B_TILE);
-            bulk_load(slot(g % STAGES), bbuf + (size_t)(i % nct) * B_TILE, B_TILE, B.full(g % STAGES));
-            S.loaded = g + 1;
+    if (tid == 0) {
+        // piece products (A piece, B piece), smallest first: all i + j <= 2
+        constexpr int NPROD = 6;
+        constexpr int PA[NPROD] = {2, 1, 0, 1, 0, 0};
+        constexpr int PB[NPROD] = {0, 1, 2, 0, 1, 0};
+        bool ok = !aborted(s_abort);
+        if (ok) {
+            mbar_expect_tx(B.a(), A_TILE);
+            bulk_load(opa, abuf, A_TILE, B.a());
+            S.a_loads++;
+            for (int i = 0; i < STAGES && i < T; ++i) {
+                const int g = g0 + i;
+                mbar_expect_tx(B.full(g % STAGES), B_TILE);
+                bulk_load(slot(g % STAGES), bbuf + (size_t)(i % nct) * B_TILE, B_TILE, B.full(g % STAGES));
+                S.loaded = g + 1;
+            }
         }
-    }
-    if (warp == 0 && !aborted(s_abort)) {
-        for (int i = 0; i < 2 && i < T; ++i)
-            load_c_tile(A, n, lda, tile_r0(i), tile_c0(i), cbuf((g0 + i) & 1), B.c((g0 + i) & 1));
-        S.c_loaded = g0 + min(2, T);
-    }
-    // piece products (A piece, B piece), smallest first: all i + j <= 3 (a_2 b_2 dropped)
-    constexpr int NPROD = 8;
-    constexpr int PA[NPROD] = {2, 1, 2, 1, 0, 1, 0, 0};
-    constexpr int PB[NPROD] = {1, 2, 0, 1, 2, 0, 1, 0};
-    for (int t = 0; t <= T; ++t) {
-        const int g = g0 + t;
-        if (tid == 0 && t < T && !aborted(s_abort)) {
+        for (int t = 0; t < T && ok; ++t) {
+            const int g = g0 + t;
             const int rt = t / nct;
             const bool new_rt = t == 0 || rt != (t - 1) / nct;
-            bool ok = true;
             if (t > 0 && new_rt) {
                 // the A tile is free once every MMA reading it has completed, i.e. tile t-1's
                 ok = mbar_wait(B.mma((g - 1) & 1), (uint32_t)((g - 1) >> 1) & 1u);
-                if (ok) {
-                    mbar_expect_tx(B.a(), A_TILE);
-                    bulk_load(opa, abuf + (size_t)rt * A_TILE, A_TILE, B.a());
-                    S.a_loads++;
-                }
+                if (!ok) break;
+                mbar_expect_tx(B.a(), A_TILE);
+                bulk_load(opa, abuf + (size_t)rt * A_TILE, A_TILE, B.a());
+                S.a_loads++;
             }
-            if (ok && new_rt) ok = mbar_wait(B.a(), (uint32_t)(S.a_loads - 1) & 1u);
+            if (new_rt) ok = mbar_wait(B.a(), (uint32_t)(S.a_loads - 1) & 1u);
             if (ok) ok = mbar_wait(B.full(g % STAGES), (uint32_t)(g / STAGES) & 1u);
-            if (ok) {
-                tc_fence_after();
-                const uint32_t d = tmem + (uint32_t)((g & 1) * TN);
-                const uint32_t bsl = slot(g % STAGES);
-                int acc = 0;
-#pragma unroll
-                for (int p = 0; p < NPROD; ++p)
-#pragma unroll
-                    for (int ks = 0; ks < KSTEPS; ++ks) {
-                        const uint64_t ad = sdesc(opa + (uint32_t)(PA[p] * A_PIECE + ks * 256));
-                        const uint64_t bd = sdesc(bsl + (uint32_t)(PB[p] * B_PIECE + ks * 256));
-                        mma_bf16(d, ad, bd, (uint32_t)acc);
-                        acc = 1;
-                    }
-                mma_commit(B.mma(g & 1));
-                S.g = g + 1;
-            } else {
-                set_abort(s_abort, err_flag);
-            }
-        }
-        if (t > 0) {
-            // epilogue of tile t-1 (its MMAs were issued one iteration ago, its C tile two)
-            const int tp = t - 1, gp = g - 1;
-            bool ok = !aborted(s_abort) && mbar_wait(B.mma(gp & 1), (uint32_t)(gp >> 1) & 1u) &&
-                      mbar_wait(B.c(gp & 1), (uint32_t)(gp >> 1) & 1u);
-            ok = __all_sync(FULL_MASK, ok);
-            if (!ok) set_abort(s_abort, err_flag);
+            if (ok && t >= 2) ok = mbar_wait(B.free(g & 1), (uint32_t)((g - 2) >> 1) & 1u);
+            if (!ok) break;
             tc_fence_after();
-            epilogue(A, n, lda, tile_r0(tp), tile_c0(tp), tmem + (uint32_t)((gp & 1) * TN),
-                     cs + (size_t)(gp & 1) * (C_TILE / 8), ok);
-        }
-        tc_fence_before();
-        __syncthreads();
-        if (t > 0 && !aborted(s_abort)) {
-            // tile t-1 is done: its B slot takes tile t-1+STAGES, its C buffer tile t+1
+            const uint32_t d = tmem + (uint32_t)((g & 1) * TN);
+            const uint32_t bsl = slot(g % STAGES);
+#pragma unroll
+            for (int p = 0; p < NPROD; ++p)
+#pragma unroll
+                for (int ks = 0; ks < KSTEPS; ++ks) {
+                    const uint64_t ad = sdesc(opa + (uint32_t)(PA[p] * A_PIECE + ks * 256));
+                    const uint64_t bd = sdesc(bsl + (uint32_t)(PB[p] * B_PIECE + ks * 256));
+                    mma_bf16(d, ad, bd, (uint32_t)(p | ks));
+                }
+            mma_commit(B.mma(g & 1));
+            S.g = g + 1;
             const int tn = t - 1 + STAGES;
-            if (tid == 0 && tn < T) {
+            if (t > 0 && tn < T) {
+                // tile t-1's MMAs are done (they precede tile t's): its slot takes tile t-1+STAGES
+                ok = mbar_wait(B.mma((g - 1) & 1), (uint32_t)((g - 1) >> 1) & 1u);
+                if (!ok) break;
                 const int gn = g0 + tn;
                 mbar_expect_tx(B.full(gn % STAGES), B_TILE);
                 bulk_load(slot(gn % STAGES), bbuf + (size_t)(tn % nct) * B_TILE, B_TILE, B.full(gn % STAGES));
                 S.loaded = gn + 1;
             }
-            if (warp == 0 && t + 1 < T) {
-                const int gc = g0 + t + 1;
-                load_c_tile(A, n, lda, tile_r0(t + 1), tile_c0(t + 1), cbuf(gc & 1), B.c(gc & 1));
-                S.c_loaded = gc + 1;
+        }
+        if (!ok) {
+            set_abort(s_abort, err_flag);
+            drain(B, S);
+        }
+    } else if (warp >= EPI_WARP0) {
+        const int q = warp - EPI_WARP0;
+        const uint32_t cb0 = opa + (uint32_t)OP_C;
+        const float2 *cs = reinterpret_cast<const float2 *>(op + OP_C);
+        int issued = 0;  // C loads of this warp (tiles g0 .. g0 + issued - 1)
+        bool ok = !aborted(s_abort);
+        for (int i = 0; i < 2 && i < T && ok; ++i, ++issued) {
+            const int g = g0 + i;
+            load_c_rows(A, n, lda, tile_r0(i) + 32 * q, tile_c0(i), cb0 + (uint32_t)((g & 1) * C_TILE + 32 * q * 8),
+                        B.c(g & 1, q));
+        }
+        for (int t = 0; t < T && ok; ++t) {
+            const int g = g0 + t, b = g & 1;
+            const uint32_t par = (uint32_t)(g >> 1) & 1u;
+            ok = !aborted(s_abort) && mbar_wait(B.mma(b), par) && mbar_wait(B.c(b, q), par);
+            ok = __all_sync(FULL_MASK, ok);
+            if (!ok) break;
+            tc_fence_after();
+            const int row = 32 * q + lane, gr = tile_r0(t) + row, c0 = tile_c0(t);
+            const uint32_t tb = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * TN);
+            const float2 *cbuf = cs + (size_t)b * (C_TILE / 8);
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                float re[16], im[16];
+                tmem_ld16(tb + (uint32_t)(16 * r), re);
+                tmem_ld16(tb + (uint32_t)(TNC + 16 * r), im);
+                if (gr < n) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const int c = 16 * r + i;
+                        if (c0 + c < n) {
+                            const float2 v = cbuf[row + c * TM];
+                            A[gr + (int64_t)(c0 + c) * lda] = make_float2(v.x - re[i], v.y - im[i]);
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            fence_proxy_async();  // this warp's reads of its C rows before the next copy into them
+            __syncwarp();
+            if (lane == 0) mbar_arrive(B.free(b));
+            if (t + 2 < T) {
+                load_c_rows(A, n, lda, tile_r0(t + 2) + 32 * q, tile_c0(t + 2),
+                            cb0 + (uint32_t)(b * C_TILE + 32 * q * 8), B.c(b, q));
+                ++issued;
             }
         }
+        if (!ok) {
+            set_abort(s_abort, err_flag);
+            if (lane == 0)
+                for (int k = 1; k <= 2 && issued - k >= 0; ++k) {
+                    const int g = g0 + issued - k;
+                    mbar_wait(B.c(g & 1, q), (uint32_t)(g >> 1) & 1u);
+                }
+        }
     }
-    if (tid != 0) S.g = g0 + T;  // thread 0 counted its issues (fewer after a timeout)
+    __syncthreads();
+    if (!aborted(s_abort)) S.g = g0 + T;  // after a timeout thread 0 keeps its count of issued tiles
 }
 
 // ---------------------------------------------------------------------------- correction solves
@@ -815,31 +893,33 @@ __device__ __noinline__ void solve_df(const float2 *A, int n, int lda, float2 *B
     __syncthreads();
 }
 
-// Correction solve of the tensor-core kernel (the launch guarantees every warp's ring at least
-// two tiles: DF_MIN_RING bytes).
+// Correction solve of the tensor-core kernel.  One right-hand side: the dataflow solve (its
+// critical path is short when a tile step is one complex multiply-add per entry).  More: the
+// strip-ring solve of the CUDA-core kernel, whose CTA-wide strips amortise the per-block
+// latency over all right-hand sides.  The launch guarantees the ring DF_MIN_RING bytes (two
+// tiles per warp, which is also two 16-column strips of the largest system).
 constexpr int DF_MIN_RING = 2 * NW * DF_TILE * (int)sizeof(float2);
 
+template <int RPT>
 struct TcSolve {
     const float2 *A;
     int n, lda;
     const float2 *ginv;
     unsigned char *ring;
     int ring_bytes;
+    const float2 *dinv;
     int *s_flag;
     int *s_phase;
     int *s_abort;
     int *err_flag;
     __device__ void operator()(float2 *B, int nrhs) const {
+        if (nrhs > 1) {
+            solve_ring<RPT>(A, n, lda, B, nrhs, ring, ring_bytes, dinv);
+            return;
+        }
         const int ns = min(4, ring_bytes / (NW * DF_TILE * (int)sizeof(float2)));
         const int phase = *s_phase;
-        float2 *st = reinterpret_cast<float2 *>(ring);
-        // right-hand sides in registers: the smallest instantiation that holds nrhs (a predicated
-        // column still costs its issue slots)
-        if (nrhs <= 1) solve_df<1>(A, n, lda, B, nrhs, ginv, st, ns, s_flag, phase, s_abort, err_flag);
-        else if (nrhs <= 2) solve_df<2>(A, n, lda, B, nrhs, ginv, st, ns, s_flag, phase, s_abort, err_flag);
-        else if (nrhs <= 4) solve_df<4>(A, n, lda, B, nrhs, ginv, st, ns, s_flag, phase, s_abort, err_flag);
-        else if (nrhs <= 8) solve_df<8>(A, n, lda, B, nrhs, ginv, st, ns, s_flag, phase, s_abort, err_flag);
-        else solve_df<RMAX_MIXED>(A, n, lda, B, nrhs, ginv, st, ns, s_flag, phase, s_abort, err_flag);
+        solve_df<1>(A, n, lda, B, nrhs, ginv, reinterpret_cast<float2 *>(ring), ns, s_flag, phase, s_abort, err_flag);
         if (threadIdx.x == 0) *s_phase = phase + 2;  // read again only after the next CTA barrier
     }
 };
@@ -850,7 +930,7 @@ struct TcSolve {
 // PL.info the first zero pivot), with the Schur updates on the tensor cores.
 template <int RPT>
 __device__ __noinline__ void factor_tc(float2 *A, int n, int lda, int ldp, unsigned char *sm, const TcSmem &L,
-                                       unsigned char *abuf, unsigned char *bbuf, float2 *ginv, PanelLists &PL,
+                                       unsigned char *abuf, unsigned char *bbuf, float2 *ginv, int *moves, PanelLists &PL,
                                        PivotXchg<float> &X, int *s_pivlg, uint32_t tmem, const Bars &B, TcState &S,
                                        int *s_abort, int *err_flag) {
     float2 *P = reinterpret_cast<float2 *>(sm + L.op);
@@ -863,17 +943,30 @@ __device__ __noinline__ void factor_tc(float2 *A, int n, int lda, int ldp, unsig
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < n; i += NT) s_ptot[i] = i;
     if (tid == 0) PL.info = 0;
+    fence_proxy_async();  // the assembly's stores and earlier generic use of the panel region
+    __syncthreads();
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int nbc = min(NB, n - j0);
         const int m = n - j0;
         const int mt = m - NB;  // trailing rows and columns (> 0 only for full panels)
-        for (int c = warp; c < nbc; c += NW)
-            for (int i = lane; i < m; i += 32) P[i + (int64_t)c * ldp] = A[(j0 + i) + (int64_t)(j0 + c) * lda];
+        // the panel's columns into shared memory, one bulk copy per column (rows rounded up to
+        // an even count: the row past n of an odd order is the scratch matrix's padding row)
+        if (warp == 0) {
+            const int rows_copy = (m + 1) & ~1;
+            if (lane == 0) mbar_expect_tx(B.panel(), (uint32_t)(nbc * rows_copy * 8));
+            __syncwarp();
+            if (lane < nbc)
+                bulk_load(su32(P + (int64_t)lane * ldp), A + j0 + (int64_t)(j0 + lane) * lda, (uint32_t)(rows_copy * 8),
+                          B.panel());
+        }
         if (tid == 0) {
             PL.nmoved = 0;
             PL.grp = 0;
         }
+        if (!mbar_wait(B.panel(), (uint32_t)S.panels & 1u)) set_abort(s_abort, err_flag);
+        ++S.panels;
         __syncthreads();
+        if (aborted(s_abort)) return;
         panel_factor_par<float2, RPT>(P, ldp, m, nbc, s_perm, s_pivlg, s_mdst, s_msrc, PL, j0, X);
         const int nmoved = PL.nmoved;
         for (int c = warp; c < nbc; c += NW)
@@ -896,7 +989,14 @@ __device__ __noinline__ void factor_tc(float2 *A, int n, int lda, int ldp, unsig
         }
         build_inverses(P, ldp, s_perm, nbc, s_linv, ginv + (size_t)(j0 / NB) * 2 * NB * NB);
         if (mt > 0) build_abuf(P, ldp, s_perm, mt, abuf);
-        swap_left(A, lda, j0, s_mdst, s_msrc, nmoved);
+        {
+            int *rec = moves + (size_t)(j0 / NB) * MV_INTS;
+            if (tid == 0) rec[0] = nmoved;
+            if (tid < nmoved) {
+                rec[4 + tid] = s_mdst[tid];
+                rec[4 + 2 * NB + tid] = s_msrc[tid];
+            }
+        }
         __syncthreads();
         if (mt > 0) {
             trailing_rows(A, n, lda, j0, s_perm, s_mdst, s_msrc, nmoved, s_linv, bbuf);
@@ -906,8 +1006,13 @@ __device__ __noinline__ void factor_tc(float2 *A, int n, int lda, int ldp, unsig
             fence_proxy_async();  // async-proxy writes of the operand region before generic reuse
             if (aborted(s_abort)) return;
         }
+        fence_proxy_async();  // this step's generic use of the panel region before the next copy
         __syncthreads();
     }
+    // the operand region is free again: index maps of the deferred interchanges
+    int *idx = reinterpret_cast<int *>(sm + L.op);
+    unswap_left(A, n, lda, moves, idx, idx + ldp);
+    __syncthreads();
 }
 
 template <int RPT>
@@ -930,8 +1035,10 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
         for (int s = 0; s < STAGES; ++s) mbar_init(B.full(s), 1);
         for (int b = 0; b < 2; ++b) {
             mbar_init(B.mma(b), 1);
-            mbar_init(B.c(b), 1);
+            mbar_init(B.free(b), NW - EPI_WARP0);
+            for (int q = 0; q < 4; ++q) mbar_init(B.c(b, q), 1);
         }
+        mbar_init(B.panel(), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_abort = 0;
         s_phase = 1;
@@ -954,6 +1061,7 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
     unsigned char *abuf = slotp + SL.abuf;
     unsigned char *bbuf = slotp + SL.bbuf;
     float2 *ginv = reinterpret_cast<float2 *>(slotp + SL.inv);
+    int *moves = reinterpret_cast<int *>(slotp + SL.moves);
 
     for (;;) {
         const int it = next_item(a.counter, &s_item);
@@ -966,9 +1074,9 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
         double berr = 0.0;
         bool write_status = true;
         const int lda = tc_lda(n);
-        assemble_fp32(A32, lda, R, w);
+        assemble_fp32(A32, lda, R, w, wi.f);
         __syncthreads();
-        factor_tc<RPT>(A32, n, lda, a.ldp, sm, L, abuf, bbuf, ginv, PL, Xx, s_pivlg, tmem, B, S, &s_abort,
+        factor_tc<RPT>(A32, n, lda, a.ldp, sm, L, abuf, bbuf, ginv, moves, PL, Xx, s_pivlg, tmem, B, S, &s_abort,
                        a.err_flag);
         __syncthreads();
         if (aborted(&s_abort)) {
@@ -985,7 +1093,7 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
                     (int)(OP_BYTES - L.ring),
                     s_dx,
                     lda};
-        const TcSolve solve{A32, n, lda, ginv, W.ring, W.ring_bytes, s_flag, &s_phase, &s_abort, a.err_flag};
+        const TcSolve<RPT> solve{A32, n, lda, ginv, W.ring, W.ring_bytes, W.s_dinv, s_flag, &s_phase, &s_abort, a.err_flag};
         mixed_refine<RPT>(a, R, wi, w, A32, W, solve, info, steps, berr, write_status);
         __syncthreads();
         if (aborted(&s_abort)) {
@@ -1012,14 +1120,14 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
 // ---------------------------------------------------------------------------- host side
 size_t tc_slot_bytes(int n_max) { return tcm::TcSlot(n_max).total; }
 
-size_t tc_smem_bytes(int n_max, int r_max) { return tcm::TcSmem(n_max | 1, n_max, r_max).total + 1024; }
+size_t tc_smem_bytes(int n_max, int r_max) { return tcm::TcSmem(tcm::tc_lda(n_max), n_max, r_max).total + 1024; }
 
 bool tc_supported(int n_max, int r_max, int smem_optin, const char **why) {
     const char *w = nullptr;
     if (n_max > TC_MAX_N) w = "order above the tensor-core kernel's limit";
     else if (r_max > MIXED_MAX_R) w = "too many right-hand sides";
     else {
-        const tcm::TcSmem L(n_max | 1, n_max, r_max);
+        const tcm::TcSmem L(tcm::tc_lda(n_max), n_max, r_max);
         if (tcm::OP_BYTES < (int64_t)L.ring || tcm::OP_BYTES - (int64_t)L.ring < tcm::DF_MIN_RING)
             w = "refinement work areas exceed shared memory";
         else if (tc_smem_bytes(n_max, r_max) + GLOBAL_STATIC_SMEM > (size_t)smem_optin)
@@ -1043,7 +1151,7 @@ static cudaError_t launch_tc_t(const GlobalArgs &a0, int grid, cudaStream_t st) 
 
 cudaError_t launch_tc(const GlobalArgs &a0, int grid, cudaStream_t st) {
     GlobalArgs a = a0;
-    a.ldp = a.n_max | 1;
+    a.ldp = tcm::tc_lda(a.n_max);  // even: the panel's columns are bulk-copy destinations
     if (a.n_max > TC_MAX_N || a.r_max > MIXED_MAX_R || a.slot_bytes < (int64_t)tc_slot_bytes(a.n_max))
         return cudaErrorInvalidValue;
     const int rpt = global_rpt(a.n_max);

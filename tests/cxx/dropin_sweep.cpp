@@ -1,5 +1,5 @@
 // C++ caller of the C ABI, shaped like the body of KrylovROMSubstructure::backTransformKMOR
-// (src/analysis/KrylovROMSubstructure.cpp:1393-1460) after the change shown in INTEGRATION.md:
+// (src/analysis/KrylovROMSubstructure.cpp:1393-1460) with its frequency loop replaced by the C ABI:
 // the reduced operators live in host std::vectors of an MKL_Complex16-like struct, the whole
 // frequency loop is one srom_sweep_host call, and y = C_r x comes back stacked [w][n_out x r].
 //

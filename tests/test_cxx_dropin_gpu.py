@@ -1,5 +1,5 @@
 """The C ABI from C++: tests/cxx/dropin_sweep.cpp, written like the body of
-backTransformKMOR (KrylovROMSubstructure.cpp:1393-1460) after the change INTEGRATION.md shows,
+backTransformKMOR (KrylovROMSubstructure.cpp:1393-1460) with its frequency loop replaced by the C ABI,
 is compiled with g++ against include/staccato_rom.h and the library, reads its ROM from dense
 Matrix Market files, sweeps it through srom_sweep_host with the fused back-projection and
 writes y.  y must equal the oracle's C_r x bit for bit (FP64 form)."""

@@ -77,6 +77,47 @@ def test_noalloc_rejects_sizes_beyond_its_limit(handle):
     torch.cuda.synchronize()
 
 
+def test_noalloc_shared_memory_limit_at_the_largest_order(handle):
+    """At n = 512 the blocked kernel's shared memory holds r <= 5 right-hand sides: r = 5 runs
+    (bit-identical to srom_sweep), r = 6 is refused before anything is launched."""
+    import torch
+
+    stream = torch.cuda.current_stream().cuda_stream
+    handle.set_stream(stream)
+    rom = _rom(15, 512, 5, 3, False)
+    sweep(handle, [rom])
+    torch.cuda.synchronize()
+    X = rom.solutions().copy()
+    rom.X.fill_(float("nan"))
+    st, msg = _noalloc(rom, stream)
+    assert st == _capi.SROM_OK, msg
+    torch.cuda.synchronize()
+    assert _same(rom.solutions(), X)
+    big = _rom(16, 512, 6, 2, False)
+    st, msg = _noalloc(big, stream)
+    assert st == _capi.SROM_ERR_UNSUPPORTED and "shared memory" in msg, msg
+
+
+def test_noalloc_allocates_no_device_memory(handle):
+    """Free device memory (the driver's count) is the same before and after a run of calls: the
+    entry point takes its scratch from the library's static array.  The first call, which may
+    load the library's device code (and with it the array), is made before the first count."""
+    import torch
+
+    stream = torch.cuda.current_stream().cuda_stream
+    roms = [_rom(17, 200, 2, 64, True), _rom(18, 512, 1, 40, False)]
+    st, msg = _noalloc(roms[0], stream)
+    assert st == _capi.SROM_OK, msg
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        for rom in roms:
+            st, msg = _noalloc(rom, stream)
+            assert st == _capi.SROM_OK, msg
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_noalloc_backprojection_matches_srom_sweep(handle):
     """With n_out > 0 the entry point also writes y = C x, bit-identical to srom_sweep."""
     import torch
