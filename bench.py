@@ -127,6 +127,13 @@ TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, 
                   "(8 n^2 B per FP32 system, 16 n^2 B per FP64 system)")
 
 
+# DRAM bytes (read + write) of one projection of the Tet10 block (K and M, k = 96): transpose,
+# SpMM, V^T Y and the partial reduction, from a one-pass ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum) of the third projection of three; filled in from the capture.
+PROJ_TRAFFIC = 784.7e6
+PROJ_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the launches of one projection"
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -320,13 +327,26 @@ def projection_leg(torch, dev, h, peaks, reps=5):
         kms[name] = kms.get(name, 0.0) + t / reps
     hbm = float(peaks.get("hbm_gbs", 0.0)) or None
     achieved = alg_bytes / (ms * 1e-3) / 1e9
+    # The arithmetic bound is the tighter one: 7.2 GFLOP of FP64 (SpMM on the CUDA cores, V^T Y
+    # on the FP64 tensor cores) against 254 MB of algorithmic bytes, i.e. 28 FLOP/B, above the
+    # machine balance of DGEMM-rate / copy-bandwidth (about 5.4 FLOP/B).
+    p64 = gemm_peak_tflops(torch, dev, torch.float64)
+    tf = flops / (ms * 1e-3) / 1e12
+    spmm_fl, vty_fl = 2 * (2 * nnz * k), 2 * (2 * N * k * k)
     return {"workload": "Tet10 block 10x10x40, h=0.01 m, steel, z=0 clamped; N=107,163, nnz=%d; V 107,163 x 96 seeded N(0,1)" % nnz,
             "ms_per_projection": ms, "kernels_ms": kms, "gram_schmidt_ms": gs_ms,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": (achieved / hbm) if hbm else None, "traffic": None,
-                         "algorithmic_bytes": alg_bytes,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)"},
-            "fp64_tflops": flops / (ms * 1e-3) / 1e12}
+            "roofline": {"bound": "fp64", "achieved": tf, "peak": p64, "unit": "TFLOP/s", "frac": tf / p64,
+                         "traffic": PROJ_TRAFFIC, "traffic_source": PROJ_TRAFFIC_SOURCE,
+                         "algorithmic_flops": flops,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)",
+                         "kernels_tflops": {"spmm": spmm_fl / (kms.get("spmm", 0.0) * 1e-3) / 1e12
+                                            if kms.get("spmm") else None,
+                                            "vty_dmma": vty_fl / (kms.get("vty_dmma", 0.0) * 1e-3) / 1e12
+                                            if kms.get("vty_dmma") else None}},
+            "roofline_hbm": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                             "frac": (achieved / hbm) if hbm else None, "algorithmic_bytes": alg_bytes,
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)"},
+            "fp64_tflops": tf}
 
 
 def adjoint_leg(torch, dev, h):
@@ -404,6 +424,67 @@ def workloads_leg(torch, dev, h, reps=3):
     return out
 
 
+REFERENCE_PER_OMEGA_MS = {
+    # test/krylovTestGPU/matrixInSingleLoop/timeMeasurements.txt:6 (GPU, sm_70) and :12 (MKL, 20 threads)
+    21: {"gpu_sm70_ms": 0.380, "mkl_20thr_ms": 0.051},
+    189: {"gpu_sm70_ms": 2.087, "mkl_20thr_ms": 40.6},
+    2520: {"gpu_sm70_ms": 41.26, "mkl_20thr_ms": 230.1},
+}
+
+
+def reference_orders_leg(torch, dev, h, reps=2):
+    """The reference's own dense ROM orders (r21, r189, r2520; 1 RHS; hysteretic eta = 0.02
+    ROMs built like the plain workload): device time per frequency of the FP64 sweep (and of
+    the mixed form, which at n = 2520 is the FP64 kernel), beside the reference's published
+    per-frequency times.  n = 2520 runs 296 frequencies (two per SM); the others 1000.
+    Accuracy at n = 2520: normwise backward error ||A x - b|| / (||A|| ||x|| + ||b||) of four
+    frequencies, in FP64 with torch."""
+    from staccato_b200 import _capi, workloads as W
+    from staccato_b200.sweep import DeviceRom, sweep
+
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for n, F in ((21, 1000), (189, 1000), (2520, 296)):
+        rom = W.plain_rom(seed=21 + n, n=n, F=F)
+        d = DeviceRom.from_host(rom.K, rom.M, rom.D, rom.rhs, rom.omega, device=dev)
+        res = {"n": n, "F": F, "r": 1, "reference": REFERENCE_PER_OMEGA_MS[n]}
+        for form, prec, flags in (("fp64", _capi.SROM_FP64, 0),
+                                  ("mixed", _capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)):
+            sweep(h, [d], precision=prec, flags=flags)
+            ts = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                sweep(h, [d], precision=prec, flags=flags)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                ts.append(e0.elapsed_time(e1))
+            ms = float(np.median(ts))
+            res[form] = {"ms": ms, "ms_per_omega": ms / F, "freq_solves_per_s": F / (ms * 1e-3),
+                         "tflops": (8.0 / 3.0 * n ** 3 + 8.0 * n * n) * F / (ms * 1e-3) / 1e12,
+                         "vs_reference_gpu": REFERENCE_PER_OMEGA_MS[n]["gpu_sm70_ms"] / (ms / F)}
+        if n == 2520:
+            K = torch.from_numpy(rom.K).to(dev)
+            M = torch.from_numpy(rom.M).to(dev)
+            b = torch.from_numpy(np.ascontiguousarray(rom.rhs[:, 0])).to(dev)
+            X = torch.from_numpy(np.ascontiguousarray(d.solutions())).to(dev)
+            be = []
+            for f in (0, 97, 201, F - 1):
+                w = float(rom.omega[f])
+                A = K - (w * w) * M
+                x = X[f].reshape(-1)
+                rr = torch.linalg.vector_norm(A @ x - b)
+                den = torch.linalg.matrix_norm(A, ord=float("inf")) * torch.linalg.vector_norm(x, ord=float("inf")) \
+                    + torch.linalg.vector_norm(b, ord=float("inf"))
+                be.append(float(rr / den))
+            res["backward_error_max"] = max(be)
+            del K, M, b, X
+        out[f"r{n}"] = res
+        del d
+        torch.cuda.empty_cache()
+    return out
+
+
 def krylov_leg(torch, dev, h):
     """Krylov basis generation (srom_krylov_basis) on the Tet10 block of the projection leg
     (10 x 10 x 40 hexes, z = 0 face clamped and removed, N = 105,840): D = 1e-5 K + 2 M, four
@@ -431,7 +512,7 @@ def krylov_leg(torch, dev, h):
     csr = DeviceCsr.from_host(K.indptr, K.indices, device=dev)
     Kd, Md, Dd, Bd = c(K.data), c(M.data), c(1e-5 * K.data + 2.0 * M.data), c(B.T)
     out = {"workload": "Tet10 block 10x10x40, N=%d, nnz=%d, 4 inputs" % (n, K.nnz), "bandwidth": bw,
-           "band_gb": band_b / 1e9, "solver": "band LDL^T (RCM order), cuBLAS ZGEMM trailing updates"}
+           "band_gb": band_b / 1e9, "solver": "band LDL^T (RCM order), trailing and solve updates on the library's complex FP64 tensor-core GEMM"}
     for name, pts, order in (("one_point_order1", [100.0], 1), ("two_points_order4", [100.0, 800.0], 4)):
         krylov_basis(h, csr, Kd, Md, Dd, Bd, pts, order)  # warm-up
         torch.cuda.synchronize(dev)
@@ -699,6 +780,7 @@ def run_ours(args):
         extras["projection"] = projection_leg(torch, dev, h, measured_peaks())
         extras["adjoint"] = adjoint_leg(torch, dev, h)
         extras["workloads"] = workloads_leg(torch, dev, h)
+        extras["reference_orders"] = reference_orders_leg(torch, dev, h)
         extras["krylov"] = krylov_leg(torch, dev, h)
 
     cpu = acc = None
@@ -747,6 +829,7 @@ def run_ours(args):
             "projection": extras.get("projection"),
             "adjoint": extras.get("adjoint"),
             "workloads": extras.get("workloads"),
+            "reference_orders": extras.get("reference_orders"),
             "krylov": extras.get("krylov"),
         }
         print(json.dumps(line), flush=True)

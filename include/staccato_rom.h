@@ -111,7 +111,9 @@ typedef struct {
 typedef struct {
     int precision;   /* SROM_FP64 / SROM_MIXED_FP32 / SROM_MIXED_TC                  */
     int max_refine;  /* refinement steps for the mixed forms (default 5 when <= 0)   */
-    double tol;      /* stop refining when the error estimate 2 (||d_s||/||d_s-1||) ||d_s||/||x|| <= tol; 0 = 2^-34 */
+    double tol;      /* stop refining when the error estimate c (||d_s||/||d_s-1||) ||d_s||/||x|| <= tol
+                        (2-norms per right-hand side; c = 2, after the first correction c = 4
+                        with d_0 = x); 0 = 2^-34 */
     int flags;       /* SROM_FLAG_*                                                  */
 } srom_sweep_opts;
 
@@ -131,6 +133,13 @@ SROM_API int srom_version(void);
  * test/krylovTestGPU/matrixInSingleLoop/gpu/src/main.cu:236-387 and
  * test/krylovMidsizeTest/gpu/concurrent/batchedLU/src/main.cu:209-268 (which do not pivot).
  * All descriptor pointers are device pointers.  Asynchronous on the handle's stream.
+ *
+ * Sizes (B200, 227 KB of shared memory per block): the right-hand sides of a system live in
+ * shared memory.  Orders whose 16-column panel also fits there (n <= 673 at r = 1, 548 at
+ * r = 4, 314 at r = 16) run on the global kernel in every precision; larger ones, up to
+ * n = 2560, on the large-order FP64 kernel, which needs n * r * 16 bytes + 64 KB (r <= 4 up to
+ * n = 2559, r <= 8 up to n = 1388, r <= 16 up to n = 724); the mixed precisions solve those in
+ * FP64 (steps = 0).  Requests beyond these limits return SROM_ERR_UNSUPPORTED.
  */
 SROM_API int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts);
 
@@ -197,6 +206,24 @@ typedef struct {
 SROM_API int srom_sweep_backward(srom_handle *h, const srom_rom_desc *rom, const srom_complex *gbar, int ldg,
                                  const srom_dparam *params, int n_params, double *dJdp, srom_complex *lambda);
 
+/* ---- dense complex GEMM ------------------------------------------------------------ */
+#define SROM_OP_N 0 /* op(X) = X   */
+#define SROM_OP_T 1 /* op(X) = X^T */
+#define SROM_OP_C 2 /* op(X) = X^H */
+
+/*
+ * Strided-batched complex FP64 GEMM on the FP64 tensor cores: C_b = alpha op(A_b) op(B_b) +
+ * beta C_b for b < batch, with A_b = A + b * stride_a (likewise B, C; strides in elements, 0
+ * broadcasts one matrix), column-major, op(A) m x k, op(B) k x n.  beta = 0 does not read C.
+ * The batched products of the substructure coupling (the reference's cublasGemmBatchedEx calls,
+ * test/IJCSA/src/IJSA.cu:875-979).  Summation order is fixed: results are deterministic.
+ * batch <= 65535.  Asynchronous on the handle's stream.
+ */
+SROM_API int srom_zgemm_batched(srom_handle *h, int opa, int opb, int m, int n, int k, srom_complex alpha,
+                                const srom_complex *A, int64_t lda, int64_t stride_a, const srom_complex *B,
+                                int64_t ldb, int64_t stride_b, srom_complex beta, srom_complex *C, int64_t ldc,
+                                int64_t stride_c, int batch);
+
 /*
  * ROM projection R_m = V^T A_m V for up to three sparse FE matrices A_m (K, M, D) that share
  * one CSR pattern -- the real-valued form of generateROM (KrylovROMSubstructure.cpp:709-765:
@@ -205,7 +232,9 @@ SROM_API int srom_sweep_backward(srom_handle *h, const srom_rom_desc *rom, const
  * (int32), base 0 or 1 (the reference uses 1); upper != 0 means only the upper triangle of a
  * symmetric matrix is stored (the reference's SPARSE_FILL_MODE_UPPER, MathLibrary.cpp:502-507).
  * vals: host array of n_mats device pointers to the value arrays.  V: n_rows x k
- * column-major (ldv), k <= 128.  R: host array of n_mats device pointers, each k x k
+ * column-major (ldv), k <= 4096: bases wider than 128 columns are projected in windows of 128
+ * columns (one SpMM pass per window, one V^T Y pass per 128 x 128 block of R).  Device
+ * workspace: (n_mats + 1) n_rows k doubles.  R: host array of n_mats device pointers, each k x k
  * column-major.  Summation order is fixed (deterministic results).
  */
 SROM_API int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *rowptr, const int *colind, int base,
@@ -218,7 +247,7 @@ SROM_API int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *ro
  * Z^H y, with Z the left basis of non-symmetric MIMO systems).  A_m: complex values (nnz each,
  * host array of n_mats device pointers) on one CSR pattern as in srom_project_real; upper != 0
  * stores the upper triangle of a complex-symmetric matrix (A_ji = A_ij, the reference's
- * SPARSE_MATRIX_TYPE_SYMMETRIC).  V, Z: n_rows x k complex column-major (ldv, ldz), k <= 64.
+ * SPARSE_MATRIX_TYPE_SYMMETRIC).  V, Z: n_rows x k complex column-major (ldv, ldz), k <= 2048.
  * R: host array of n_mats device pointers, each k x k complex column-major.  Runs on the real
  * kernels: the basis is split into [Re V | Im V] rows, A's real and imaginary parts are applied
  * as two value arrays of the same pattern, and the four real blocks of [Re Z | Im Z]^T

@@ -37,8 +37,12 @@ EXPORTS = [
     "srom_sweep_backward",
     "srom_graph_create", "srom_graph_launch", "srom_graph_destroy", "srom_tune",
     "srom_mtx_read_dense", "srom_mtx_write_dense", "srom_write_solution",
-    "srom_krylov_basis", "srom_band_order", "srom_fom_sweep",
+    "srom_krylov_basis", "srom_band_order", "srom_fom_sweep", "srom_zgemm_batched",
 ]
+
+SROM_OP_N = 0
+SROM_OP_T = 1
+SROM_OP_C = 2
 
 SROM_DPARAM_LOWRANK = 0
 SROM_DPARAM_DENSE = 1
@@ -123,6 +127,9 @@ def lib() -> C.CDLL:
         L.srom_band_order.argtypes = [C.c_int64, C.c_int64, vp, vp, i, i, vp, C.POINTER(C.c_int64),
                                       C.POINTER(C.c_int64), C.c_char_p, i]
         L.srom_band_order.restype = i
+        L.srom_zgemm_batched.argtypes = [vp, i, i, i, i, i, Complex, vp, C.c_int64, C.c_int64, vp, C.c_int64,
+                                         C.c_int64, Complex, vp, C.c_int64, C.c_int64, i]
+        L.srom_zgemm_batched.restype = i
         L.srom_orthonormalize.argtypes = [vp, vp, C.c_int64, i, C.c_int64, i]
         L.srom_orthonormalize.restype = i
         L.srom_graph_create.argtypes = [vp, C.POINTER(RomDesc), i, C.POINTER(SweepOpts), pp]

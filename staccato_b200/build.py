@@ -45,7 +45,7 @@ def build(verbose: bool = False, extra=None) -> str:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-Xcompiler", "-fPIC", "-o", LIB] + objs + ["-lcublas"]
+    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-Xcompiler", "-fPIC", "-o", LIB] + objs
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

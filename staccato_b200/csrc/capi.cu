@@ -17,6 +17,7 @@
 #include "adjoint_kernels.h"
 #include "krylov_kernels.h"
 #include "project_kernels.h"
+#include "zgemm.h"
 #include "sweep_kernels.h"
 
 using srom::Item;
@@ -49,6 +50,9 @@ struct srom_handle {
     // zeros standing in for M when a descriptor has none (see SweepPlan::null_m)
     void *d_zero = nullptr;
     size_t d_zero_bytes = 0;
+    // split-k partials of srom_zgemm_batched
+    void *d_zwork = nullptr;
+    size_t d_zwork_bytes = 0;
     // per-launch profiling
     struct ProfRec {
         std::string name;
@@ -291,6 +295,7 @@ int srom_destroy(srom_handle *h) {
     if (h->d_proj) cudaFree(h->d_proj);
     if (h->d_adj) cudaFree(h->d_adj);
     if (h->d_zero) cudaFree(h->d_zero);
+    if (h->d_zwork) cudaFree(h->d_zwork);
     if (h->h_meta) cudaFreeHost(h->h_meta);
     if (h->h_flag) cudaFreeHost(h->h_flag);
     if (h->meta_done) cudaEventDestroy(h->meta_done);
@@ -350,13 +355,14 @@ struct SweepPlan {
     bool tc = false;  // the mixed systems of class 1 run on the tensor-core kernel
     srom_sweep_opts o{};
     std::vector<char> meta;
-    size_t off_items0 = 0, off_items1 = 0, off_fb = 0, off_ctr = 0;
-    long long n_items[2] = {0, 0};
-    double flops[2] = {0.0, 0.0};
+    size_t off_items0 = 0, off_items1 = 0, off_items2 = 0, off_fb = 0, off_ctr = 0;
+    long long n_items[3] = {0, 0, 0};
+    double flops[3] = {0.0, 0.0, 0.0};
     size_t smem_max = 0;
-    int g_nmax = 0, g_rmax = 0;
-    long long grid0 = 0, grid1 = 0;
-    int64_t slot_bytes = 0;
+    int g_nmax = 0, g_rmax = 0;    // class 1: the global kernels' largest order and RHS count
+    int b_nmax = 0, b_rmax = 0;    // class 2: the large-order FP64 kernel's
+    long long grid0 = 0, grid1 = 0, grid2 = 0;
+    int64_t slot_bytes = 0, slot2_bytes = 0;
     bool need_scratch = false;
     std::vector<srom::BackProj> backproj;  // ROMs whose solutions are projected onto outputs
     // ROMs without a mass matrix.  Their descriptors point M at a zero matrix instead: for any
@@ -372,9 +378,15 @@ void patch_null_m(SweepPlan &P, const void *zero) {
     for (int i : P.null_m) rd[i].M = static_cast<const double2 *>(zero);
 }
 
+// Systems whose panel does not fit the global kernel's shared memory (n above ~690 for r = 1,
+// less for more right-hand sides; every n > 768) run on the large-order FP64 kernel (class 2).
+bool large_order(const srom_handle *h, int n, int r) { return !srom::global_panel_fits(n, r, h->max_smem_optin); }
+
 // FP64 storage class of an n x n system with r right-hand sides: 0 smem kernel, 1 global
-// kernel.  The tuning table (srom_tune) overrides the default "smem when it fits".
+// kernel, 2 large-order global kernel.  The tuning table (srom_tune) overrides the default
+// "smem when it fits".
 int fp64_class(const srom_handle *h, int n, int r) {
+    if (large_order(h, n, r)) return 2;
     const bool fits = srom::fp64_smem_bytes(n, r) <= (size_t)h->max_smem_optin;
     if (!fits) return 1;
     auto it = h->tune_fp64.find(((long long)n << 16) | r);
@@ -386,8 +398,11 @@ int fp64_class(const srom_handle *h, int n, int r) {
 // is solved there outright.  At those orders (n <= ~84 for r <= 4) one FP64 factorisation in
 // shared memory is faster than complex-FP32 factors in the global kernel plus refinement
 // (measured 1.5-2.2x at n = 32..80), and its result is the FP64 form's, bit for bit (steps = 0).
-// Larger systems, or any with SROM_FLAG_MIXED_EVERY, go to the mixed global kernel.
+// Larger systems, or any with SROM_FLAG_MIXED_EVERY, go to the mixed global kernel.  Orders
+// whose panel does not fit the global kernel's shared memory have no mixed kernel: they run on
+// the large-order FP64 kernel (steps = 0).
 int mixed_class(const srom_handle *h, int n, int r, int flags) {
+    if (large_order(h, n, r)) return 2;
     if (flags & SROM_FLAG_MIXED_EVERY) return 1;
     if (fp64_class(h, n, r) != 0) return 1;
     return srom::fp64_smem_blocks_per_sm(srom::fp64_smem_bytes(n, r)) >= 2 ? 0 : 1;
@@ -429,20 +444,44 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
         const srom_rom_desc &d = roms[i];
         if (d.n == 0 || d.F == 0 || d.r == 0) continue;
         cls[i] = mixed ? mixed_class(h, d.n, d.r, o.flags) : fp64_class(h, d.n, d.r);
+    }
+    // The global kernel runs with the largest n and the largest r of its systems: while that
+    // pair does not fit, the largest system moves to the large-order FP64 kernel.
+    for (;;) {
+        int gn = 0, gr = 0, big = -1;
+        for (int i = 0; i < n_roms; ++i)
+            if (cls[i] == 1) {
+                gn = std::max(gn, roms[i].n);
+                gr = std::max(gr, roms[i].r);
+                if (big < 0 || roms[i].n > roms[big].n) big = i;
+            }
+        if (big < 0 || srom::global_panel_fits(gn, gr, h->max_smem_optin)) break;
+        cls[big] = 2;
+    }
+    for (int i = 0; i < n_roms; ++i) {
+        const srom_rom_desc &d = roms[i];
+        if (cls[i] < 0) continue;
         if (cls[i] == 0) {
             P.smem_max = std::max(P.smem_max, srom::fp64_smem_bytes(d.n, d.r));
-        } else {
+        } else if (cls[i] == 1) {
             P.g_nmax = std::max(P.g_nmax, d.n);
             P.g_rmax = std::max(P.g_rmax, d.r);
+        } else {
+            P.b_nmax = std::max(P.b_nmax, d.n);
+            P.b_rmax = std::max(P.b_rmax, d.r);
         }
         P.n_items[cls[i]] += d.F;
         P.flops[cls[i]] += lu_flops(d.n, d.r) * d.F;
     }
-    if (P.g_nmax > 0 && (srom::global_rpt(P.g_nmax) > srom::GLOBAL_MAX_RPT ||
-                         srom::global_smem_bytes(P.g_nmax, P.g_rmax) + srom::GLOBAL_STATIC_SMEM > smem_cap))
-        return set_err(h, SROM_ERR_UNSUPPORTED, "n=%d with r=%d exceeds the shared-memory panel budget",
-                       P.g_nmax, P.g_rmax);
-    if (P.n_items[0] + P.n_items[1] > INT32_MAX) return set_err(h, SROM_ERR_UNSUPPORTED, "too many systems");
+    if (P.b_nmax > srom::BIG_MAX_N)
+        return set_err(h, SROM_ERR_UNSUPPORTED, "n=%d exceeds the largest supported order %d", P.b_nmax,
+                       srom::BIG_MAX_N);
+    if (P.b_nmax > 0 && srom::global_smem_bytes(P.b_nmax, P.b_rmax, true) + srom::GLOBAL_STATIC_SMEM > smem_cap)
+        return set_err(h, SROM_ERR_UNSUPPORTED,
+                       "n=%d with r=%d: the right-hand sides (n*r*16 bytes) exceed shared memory", P.b_nmax,
+                       P.b_rmax);
+    if (P.n_items[0] + P.n_items[1] + P.n_items[2] > INT32_MAX)
+        return set_err(h, SROM_ERR_UNSUPPORTED, "too many systems");
     if (P.n_items[0] > 0) {
         const int bps = srom::fp64_smem_blocks_per_sm(P.smem_max);
         if (bps <= 0) return set_err(h, SROM_ERR_UNSUPPORTED, "smem kernel cannot be resident (%zu B)", P.smem_max);
@@ -459,28 +498,39 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
         for (int i = 0; i < n_roms; ++i)
             if (cls[i] == 1 && !roms[i].LU) P.need_scratch = true;
     }
+    if (P.n_items[2] > 0) {
+        // one system per CTA: matrix (or the caller's LU buffer) and the panel in the CTA's slot;
+        // classes 1 and 2 run one after the other and share the scratch buffer
+        P.grid2 = std::min<long long>(P.n_items[2], h->sm_count);
+        P.slot2_bytes = srom::big_slot_bytes(P.b_nmax);
+        P.need_scratch = true;
+    }
     // Work lists: largest systems first (longest-processing-time order for the persistent CTAs).
     std::vector<int> order(n_roms);
     for (int i = 0; i < n_roms; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return roms[a].n > roms[b].n; });
     P.off_items0 = align_up(sizeof(RomDev) * std::max(n_roms, 1), 256);
     P.off_items1 = P.off_items0 + align_up(sizeof(Item) * (size_t)P.n_items[0] + 1, 256);
-    P.off_fb = P.off_items1 + align_up(sizeof(Item) * (size_t)P.n_items[1] + 1, 256);
+    P.off_items2 = P.off_items1 + align_up(sizeof(Item) * (size_t)P.n_items[1] + 1, 256);
+    P.off_fb = P.off_items2 + align_up(sizeof(Item) * (size_t)P.n_items[2] + 1, 256);
     P.off_ctr = P.off_fb + (mixed ? align_up(sizeof(Item) * (size_t)P.n_items[1] + 1, 256) : 0);
     P.meta.assign(P.off_ctr + 256, 0);
     char *hm = P.meta.data();
     if (n_roms) memcpy(hm, dev.data(), sizeof(RomDev) * n_roms);
     Item *it0 = reinterpret_cast<Item *>(hm + P.off_items0);
-    Item *it1 = reinterpret_cast<Item *>(hm + P.off_items1);
-    long long k0 = 0, k1 = 0;
+    Item *its[3] = {it0, reinterpret_cast<Item *>(hm + P.off_items1), reinterpret_cast<Item *>(hm + P.off_items2)};
+    long long k[3] = {0, 0, 0};
     for (int oi = 0; oi < n_roms; ++oi) {
         const int i = order[oi];
         if (cls[i] < 0) continue;
-        Item *dst = cls[i] == 0 ? it0 : it1;
-        long long &k = cls[i] == 0 ? k0 : k1;
-        for (int f = 0; f < roms[i].F; ++f) dst[k++] = Item{i, f};
+        for (int f = 0; f < roms[i].F; ++f) its[cls[i]][k[cls[i]]++] = Item{i, f};
     }
     return SROM_OK;
+}
+
+// Scratch bytes of a plan: classes 1 and 2 run one after the other on one stream and share it.
+size_t plan_scratch_bytes(const SweepPlan &P) {
+    return std::max((size_t)P.slot_bytes * P.grid1, (size_t)P.slot2_bytes * P.grid2);
 }
 
 // Counters (smem, global, fallback count, fallback work) live at off_ctr and must be zero
@@ -542,6 +592,20 @@ int enqueue_plan(srom_handle *h, const SweepPlan &P, char *dm, void *scratch, cu
             if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "fallback launch: %s", cudaGetErrorString(e));
         }
     }
+    if (rc == SROM_OK && P.n_items[2] > 0) {
+        srom::GlobalArgs a{};
+        a.roms = d_roms;
+        a.items = reinterpret_cast<const Item *>(dm + P.off_items2);
+        a.n_items = (int)P.n_items[2];
+        a.counter = d_ctr + 5;
+        a.scratch = static_cast<unsigned char *>(scratch);
+        a.slot_bytes = P.slot2_bytes;
+        a.n_max = P.b_nmax;
+        a.r_max = P.b_rmax;
+        ProfScope ps(h, "fp64_large", P.n_items[2], P.flops[2], 0.0);
+        cudaError_t e = srom::launch_global_big(a, (int)P.grid2, st);
+        if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "large-order launch: %s", cudaGetErrorString(e));
+    }
     for (size_t i = 0; rc == SROM_OK && i < P.backproj.size(); ++i) {
         const srom::BackProj &b = P.backproj[i];
         ProfScope ps(h, "backproject", b.F, 8.0 * (double)b.n_out * b.n * b.r * b.F, 0.0);
@@ -582,7 +646,7 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
     if (s) return s;
     void *scr = nullptr;
     if (P.need_scratch) {
-        s = ensure_device_buffer(h, &h->scratch, &h->scratch_bytes, (size_t)P.slot_bytes * P.grid1);
+        s = ensure_device_buffer(h, &h->scratch, &h->scratch_bytes, plan_scratch_bytes(P));
         if (s) return s;
         scr = h->scratch;
     }
@@ -623,7 +687,7 @@ int srom_graph_create(srom_handle *h, const srom_rom_desc *roms, int n_roms, con
     };
     cudaError_t e = cudaMalloc(&G->d_meta, P.meta.size());
     if (e != cudaSuccess) return fail(set_err(h, SROM_ERR_ALLOC, "graph metadata: %s", cudaGetErrorString(e)));
-    if (P.need_scratch && (e = cudaMalloc(&G->scratch, (size_t)P.slot_bytes * P.grid1)) != cudaSuccess)
+    if (P.need_scratch && (e = cudaMalloc(&G->scratch, plan_scratch_bytes(P))) != cudaSuccess)
         return fail(set_err(h, SROM_ERR_ALLOC, "graph scratch: %s", cudaGetErrorString(e)));
     if (P.zero_bytes > 0) {
         if ((e = cudaMalloc(&G->d_zero, P.zero_bytes)) != cudaSuccess)
@@ -679,13 +743,63 @@ int srom_graph_destroy(srom_graph *G) {
     return SROM_OK;
 }
 
+int srom_zgemm_batched(srom_handle *h, int opa, int opb, int m, int n, int k, srom_complex alpha, const srom_complex *A,
+                       int64_t lda, int64_t stride_a, const srom_complex *B, int64_t ldb, int64_t stride_b,
+                       srom_complex beta, srom_complex *C, int64_t ldc, int64_t stride_c, int batch) {
+    if (!h) return SROM_ERR_INVALID;
+    h->err.clear();
+    if (m < 0 || n < 0 || k < 0 || batch < 0) return set_err(h, SROM_ERR_INVALID, "negative size");
+    if (opa < SROM_OP_N || opa > SROM_OP_C || opb < SROM_OP_N || opb > SROM_OP_C)
+        return set_err(h, SROM_ERR_INVALID, "op must be SROM_OP_N, SROM_OP_T or SROM_OP_C");
+    if (m == 0 || n == 0 || batch == 0) return SROM_OK;
+    const int64_t arows = opa == SROM_OP_N ? m : k, brows = opb == SROM_OP_N ? k : n;
+    if (lda < std::max<int64_t>(1, arows) || ldb < std::max<int64_t>(1, brows) || ldc < std::max(1, m))
+        return set_err(h, SROM_ERR_INVALID, "leading dimension too small (lda %lld, ldb %lld, ldc %lld)",
+                       (long long)lda, (long long)ldb, (long long)ldc);
+    if (stride_a < 0 || stride_b < 0 || stride_c < 0) return set_err(h, SROM_ERR_INVALID, "negative stride");
+    if (!C || (k > 0 && (!A || !B))) return set_err(h, SROM_ERR_INVALID, "A, B and C must be non-null");
+    if (srom::misaligned(A, 16) || srom::misaligned(B, 16) || srom::misaligned(C, 16))
+        return set_err(h, SROM_ERR_INVALID, "A, B and C must be 16-byte aligned");
+    if ((int64_t)batch > 65535) return set_err(h, SROM_ERR_UNSUPPORTED, "batch %d exceeds 65535", batch);
+    DeviceGuard g(h->device);
+    srom::Zgemm z;
+    z.opa = opa;
+    z.opb = opb;
+    z.m = m;
+    z.n = n;
+    z.k = k;
+    z.alpha = make_double2(alpha.re, alpha.im);
+    z.beta = make_double2(beta.re, beta.im);
+    z.A = reinterpret_cast<const double2 *>(A);
+    z.lda = lda;
+    z.sa = stride_a;
+    z.B = reinterpret_cast<const double2 *>(B);
+    z.ldb = ldb;
+    z.sb = stride_b;
+    z.C = reinterpret_cast<double2 *>(C);
+    z.ldc = ldc;
+    z.sc = stride_c;
+    z.batch = batch;
+    z.sms = h->sm_count;
+    const int64_t we = srom::zgemm_work_elems(m, n, k, batch, h->sm_count);
+    if (we > 0) {
+        int s = ensure_device_buffer(h, &h->d_zwork, &h->d_zwork_bytes, sizeof(double2) * (size_t)we);
+        if (s) return s;
+        z.work = static_cast<double2 *>(h->d_zwork);
+        z.work_elems = (int64_t)(h->d_zwork_bytes / sizeof(double2));
+    }
+    ProfScope ps(h, "zgemm", batch, 8.0 * m * n * (double)k * batch, 0.0);
+    SROM_CUDA(h, srom::zgemm(z, h->stream));
+    return SROM_OK;
+}
+
 int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *rowptr, const int *colind, int base, int upper,
                       const double *const *vals, int n_mats, const double *V, int k, int64_t ldv, double *const *R) {
     if (!h) return SROM_ERR_INVALID;
     h->err.clear();
     if (n_rows < 0 || k < 0) return set_err(h, SROM_ERR_INVALID, "negative size");
     if (n_mats < 1 || n_mats > 3) return set_err(h, SROM_ERR_INVALID, "n_mats must be 1..3");
-    if (k > 128) return set_err(h, SROM_ERR_UNSUPPORTED, "k = %d exceeds 128", k);
+    if (k > srom::PRJ_MAX_K) return set_err(h, SROM_ERR_UNSUPPORTED, "k = %d exceeds %d", k, srom::PRJ_MAX_K);
     if (base != 0 && base != 1) return set_err(h, SROM_ERR_INVALID, "base must be 0 or 1");
     if (!vals || !R) return set_err(h, SROM_ERR_INVALID, "vals and R must be non-null");
     for (int m = 0; m < n_mats; ++m)
@@ -694,11 +808,10 @@ int srom_project_real(srom_handle *h, int64_t n_rows, const int64_t *rowptr, con
     if (!rowptr || !colind || !V) return set_err(h, SROM_ERR_INVALID, "rowptr, colind and V must be non-null");
     if (ldv < n_rows) return set_err(h, SROM_ERR_INVALID, "ldv < n_rows");
     DeviceGuard g(h->device);
-    const int kp = (k + 7) & ~7;
     const int nblk = h->sm_count;  // one V^T Y CTA per SM
     const size_t vt_b = align_up(sizeof(double) * (size_t)n_rows * k, 256);
     const size_t y_b = align_up(sizeof(double) * (size_t)n_rows * k * n_mats, 256);
-    const size_t p_b = align_up(sizeof(double) * (size_t)nblk * n_mats * kp * kp, 256);
+    const size_t p_b = align_up(sizeof(double) * srom::vty_partial_doubles(k, n_mats, nblk), 256);
     int s = ensure_device_buffer(h, &h->d_proj, &h->d_proj_bytes, vt_b + y_b + p_b);
     if (s) return s;
     char *base_p = static_cast<char *>(h->d_proj);
@@ -731,7 +844,8 @@ int srom_project_complex(srom_handle *h, int64_t n_rows, int64_t nnz, const int6
     h->err.clear();
     if (n_rows < 0 || k < 0 || nnz < 0) return set_err(h, SROM_ERR_INVALID, "negative size");
     if (n_mats < 1 || n_mats > 3) return set_err(h, SROM_ERR_INVALID, "n_mats must be 1..3");
-    if (k > 64) return set_err(h, SROM_ERR_UNSUPPORTED, "k = %d exceeds 64 (complex form)", k);
+    if (k > srom::PRJ_MAX_K / 2)
+        return set_err(h, SROM_ERR_UNSUPPORTED, "k = %d exceeds %d (complex form)", k, srom::PRJ_MAX_K / 2);
     if (base != 0 && base != 1) return set_err(h, SROM_ERR_INVALID, "base must be 0 or 1");
     if (!vals || !R) return set_err(h, SROM_ERR_INVALID, "vals and R must be non-null");
     for (int m = 0; m < n_mats; ++m)
@@ -744,11 +858,11 @@ int srom_project_complex(srom_handle *h, int64_t n_rows, int64_t nnz, const int6
     for (int m = 0; m < n_mats; ++m) bad = bad || srom::misaligned(vals[m], 16) || srom::misaligned(R[m], 16);
     if (bad) return set_err(h, SROM_ERR_INVALID, "complex arrays must be 16-byte aligned (rowptr 8, colind 4)");
     DeviceGuard g(h->device);
-    const int k2 = 2 * k, kp = (k2 + 7) & ~7;
+    const int k2 = 2 * k;
     const int nblk = h->sm_count;
     const size_t w_b = align_up(sizeof(double) * (size_t)n_rows * k2, 256);
     const size_t v_b = align_up(sizeof(double) * (size_t)nnz, 256);
-    const size_t p_b = align_up(sizeof(double) * (size_t)nblk * kp * kp, 256);
+    const size_t p_b = align_up(sizeof(double) * srom::vty_partial_doubles(k2, 1, nblk), 256);
     const size_t g_b = align_up(sizeof(double) * (size_t)k2 * k2, 256);
     // Vt2 [Re V | Im V], Zt2 (when Z is given), Ar, Ai, P_r, P_i, partials, G
     const size_t need = w_b * (Z ? 4 : 3) + 2 * v_b + p_b + g_b;

@@ -12,14 +12,15 @@
 //  * factor    -- blocked LDL^T without pivoting (K~ is complex symmetric), NB columns a step:
 //                 the NB x NB diagonal block in one CTA, the panel L21 = A21 L11^-T D^-1 by one
 //                 warp a row, and the trailing update A22 -= (L21 D) L21^T as one strided-batched
-//                 ZGEMM (cuBLAS) over the column blocks of the window;
-//  * solves    -- blocked forward / diagonal / backward substitution for all right-hand sides.
+//                 complex GEMM over the column blocks of the window (zgemm.cu, FP64 tensor cores);
+//  * solves    -- blocked forward / diagonal / backward substitution for all right-hand sides,
+//                 the off-diagonal block updates as complex GEMMs (split over k when short and wide).
 //
 // The rest of the process runs on the GPU as in the reference: M Q by a complex CSR SpMM, the
-// re-orthogonalisation Q <- Q - V (V^H Q) with ZGEMMs until the norm ratio exceeds 1/sqrt(2),
+// re-orthogonalisation Q <- Q - V (V^H Q) with complex GEMMs (V^H Q split over the rows, reduced
+// in a fixed order) until the norm ratio exceeds 1/sqrt(2),
 // and the column-pivoted Householder QR (the steps of zgeqp3 with exact partial column norms)
 // whose leading |R_ii| > tol decide the rank, Q formed from the reflectors (zungqr).
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,6 +33,7 @@
 
 #include "../../include/staccato_rom.h"
 #include "krylov_kernels.h"
+#include "zgemm.h"
 
 namespace srom {
 namespace kry {
@@ -405,11 +407,6 @@ struct Err {
         cudaError_t _e = (call);                                                            \
         if (_e != cudaSuccess) return E.set(SROM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
     } while (0)
-#define KBL(call)                                                                               \
-    do {                                                                                        \
-        cublasStatus_t _s = (call);                                                             \
-        if (_s != CUBLAS_STATUS_SUCCESS) return E.set(SROM_ERR_CUDA, std::string(#call) + " failed (cuBLAS status " + std::to_string((int)_s) + ")"); \
-    } while (0)
 
 // Device buffers freed at scope exit (after the stream has drained).
 struct Bufs {
@@ -567,10 +564,34 @@ struct BandLDLT {
     double2 *band = nullptr, *W = nullptr, *Lp = nullptr;
     int *d_info = nullptr;
     cudaStream_t st = nullptr;
-    cublasHandle_t cb = nullptr;
+    double2 *zwork = nullptr;  // split-k partials of the complex GEMMs
+    int64_t zwork_elems = 0;
+    int sms = 148;
+
+    // complex GEMM C -= op(A) op(B) (beta = 1) on this factor's stream and workspace
+    Zgemm gemm(int opa, int opb, int m, int nn, int k, const double2 *A, int64_t lda, const double2 *Bm, int64_t ldb,
+               double2 *C, int64_t ldc) const {
+        Zgemm z;
+        z.opa = opa;
+        z.opb = opb;
+        z.m = m;
+        z.n = nn;
+        z.k = k;
+        z.alpha = make_double2(-1.0, 0.0);
+        z.beta = make_double2(1.0, 0.0);
+        z.A = A;
+        z.lda = lda;
+        z.B = Bm;
+        z.ldb = ldb;
+        z.C = C;
+        z.ldc = ldc;
+        z.work = zwork;
+        z.work_elems = zwork_elems;
+        z.sms = sms;
+        return z;
+    }
 
     int factor(Err &E) {
-        const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0), one = make_cuDoubleComplex(1.0, 0.0);
         const size_t smem = sizeof(double2) * NB * SLD;
         KCU(cudaMemsetAsync(d_info, 0, sizeof(int), st));
         int prev_rows = ldw;
@@ -583,13 +604,16 @@ struct BandLDLT {
             prev_rows = rows;
             ldlt_panel_kernel<<<(zero_to + KT / 32 - 1) / (KT / 32), KT, smem + sizeof(double2) * NB, st>>>(
                 band, ldab, j0, nb, rows, zero_to, W, Lp, ldw);
+            // trailing update of the window: column block b (NB columns) -= W_b Lp_b^T, with
+            // W_b, Lp_b the panel rows from b NB on
             const int batches = (rows + NB - 1) / NB;
             double2 *C0 = band + (j0 + nb) * ldab + NB;
-            KBL(cublasZgemmStridedBatched(cb, CUBLAS_OP_N, CUBLAS_OP_T, rows, NB, nb, &mone,
-                                          reinterpret_cast<const cuDoubleComplex *>(W), ldw, NB,
-                                          reinterpret_cast<const cuDoubleComplex *>(Lp), ldw, NB, &one,
-                                          reinterpret_cast<cuDoubleComplex *>(C0), (int)(ldab - 1), (long long)NB * ldab,
-                                          batches));
+            Zgemm z = gemm(ZG_N, ZG_T, rows, NB, nb, W, ldw, Lp, ldw, C0, ldab - 1);
+            z.sa = NB;
+            z.sb = NB;
+            z.sc = (int64_t)NB * ldab;
+            z.batch = batches;
+            KCU(zgemm(z, st));
         }
         KCU(cudaGetLastError());
         int info = 0;
@@ -603,7 +627,6 @@ struct BandLDLT {
 
     // X (n x nrhs, ldx, permuted order) <- K~^-1 X
     int solve(double2 *X, int64_t ldx, int nrhs, Err &E) {
-        const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0), one = make_cuDoubleComplex(1.0, 0.0);
         const size_t smem = sizeof(double2) * NB * SLD;
         const int tgrid = (nrhs + KT / 32 - 1) / (KT / 32);
         for (int64_t j0 = 0; j0 < n; j0 += NB) {
@@ -611,10 +634,8 @@ struct BandLDLT {
             trsv_block_kernel<<<tgrid, KT, smem, st>>>(band, ldab, j0, nb, X, ldx, nrhs, 0);
             const int rows = (int)std::min<int64_t>(bw, n - j0 - nb);
             if (rows <= 0) continue;
-            KBL(cublasZgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, rows, nrhs, nb, &mone,
-                            reinterpret_cast<const cuDoubleComplex *>(band + j0 * ldab + NB + nb), (int)(ldab - 1),
-                            reinterpret_cast<const cuDoubleComplex *>(X + j0), (int)ldx, &one,
-                            reinterpret_cast<cuDoubleComplex *>(X + j0 + nb), (int)ldx));
+            KCU(zgemm(gemm(ZG_N, ZG_N, rows, nrhs, nb, band + j0 * ldab + NB + nb, ldab - 1, X + j0, ldx,
+                           X + j0 + nb, ldx), st));
         }
         diag_scale_kernel<<<grid_for(n * nrhs, KT), KT, 0, st>>>(band, ldab, n, X, ldx, nrhs);
         const int64_t last = ((n - 1) / NB) * NB;
@@ -622,10 +643,8 @@ struct BandLDLT {
             const int nb = (int)std::min<int64_t>(NB, n - j0);
             const int rows = (int)std::min<int64_t>(bw, n - j0 - nb);
             if (rows > 0)
-                KBL(cublasZgemm(cb, CUBLAS_OP_T, CUBLAS_OP_N, nb, nrhs, rows, &mone,
-                                reinterpret_cast<const cuDoubleComplex *>(band + j0 * ldab + NB + nb), (int)(ldab - 1),
-                                reinterpret_cast<const cuDoubleComplex *>(X + j0 + nb), (int)ldx, &one,
-                                reinterpret_cast<cuDoubleComplex *>(X + j0), (int)ldx));
+                KCU(zgemm(gemm(ZG_T, ZG_N, nb, nrhs, rows, band + j0 * ldab + NB + nb, ldab - 1, X + j0 + nb, ldx,
+                               X + j0, ldx), st));
             trsv_block_kernel<<<tgrid, KT, smem, st>>>(band, ldab, j0, nb, X, ldx, nrhs, 1);
         }
         KCU(cudaGetLastError());
@@ -634,23 +653,25 @@ struct BandLDLT {
 };
 
 // Q (n x m, ld n) <- Q - V (V^H Q) repeated until ||Q_new||_F / ||Q_old||_F > 1/sqrt(2).
-int reorthogonalize(cublasHandle_t cb, cudaStream_t st, const double2 *V, int64_t ldv, int kv, double2 *&Q,
-                    double2 *&U, int64_t n, int m, double2 *S, Err &E) {
+// S: kv x m; nrm: znorm2_work_doubles() + 2 doubles (the two norms end in its last two).
+int reorthogonalize(const BandLDLT &F, cudaStream_t st, const double2 *V, int64_t ldv, int kv, double2 *&Q,
+                    double2 *&U, int64_t n, int m, double2 *S, double *nrm, Err &E) {
     if (kv == 0 || m == 0) return SROM_OK;
-    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0),
-                          mone = make_cuDoubleComplex(-1.0, 0.0);
     const double eta = 1.0 / std::sqrt(2.0);
+    double *nrm_out = nrm + znorm2_work_doubles();
     for (int it = 0; it < 64; ++it) {
-        KBL(cublasZgemm(cb, CUBLAS_OP_C, CUBLAS_OP_N, kv, m, (int)n, &one, reinterpret_cast<const cuDoubleComplex *>(V),
-                        (int)ldv, reinterpret_cast<const cuDoubleComplex *>(Q), (int)n, &zero,
-                        reinterpret_cast<cuDoubleComplex *>(S), kv));
+        Zgemm h = F.gemm(ZG_C, ZG_N, kv, m, (int)n, V, ldv, Q, n, S, kv);  // S = V^H Q
+        h.alpha = make_double2(1.0, 0.0);
+        h.beta = make_double2(0.0, 0.0);
+        KCU(zgemm(h, st));
         KCU(cudaMemcpyAsync(U, Q, sizeof(double2) * n * m, cudaMemcpyDeviceToDevice, st));
-        KBL(cublasZgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, m, kv, &mone, reinterpret_cast<const cuDoubleComplex *>(V),
-                        (int)ldv, reinterpret_cast<const cuDoubleComplex *>(S), kv, &one,
-                        reinterpret_cast<cuDoubleComplex *>(U), (int)n));
-        double nu = 0.0, nq = 0.0;
-        KBL(cublasDznrm2(cb, (int)(n * m), reinterpret_cast<const cuDoubleComplex *>(U), 1, &nu));
-        KBL(cublasDznrm2(cb, (int)(n * m), reinterpret_cast<const cuDoubleComplex *>(Q), 1, &nq));
+        KCU(zgemm(F.gemm(ZG_N, ZG_N, (int)n, m, kv, V, ldv, S, kv, U, n), st));  // U = Q - V S
+        KCU(znorm2(U, n * m, nrm, nrm_out, st));
+        KCU(znorm2(Q, n * m, nrm, nrm_out + 1, st));
+        double nh[2] = {0.0, 0.0};
+        KCU(cudaMemcpyAsync(nh, nrm_out, sizeof nh, cudaMemcpyDeviceToHost, st));
+        KCU(cudaStreamSynchronize(st));
+        const double nu = nh[0], nq = nh[1];
         std::swap(Q, U);
         if (!(nu / nq <= eta)) return SROM_OK;  // also leaves on NaN
     }
@@ -719,27 +740,18 @@ int pivoted_qr(cudaStream_t st, double2 *A, int64_t n, int m, double tol, double
 namespace {
 
 // The factorisation context shared by the Krylov basis and the full-order sweep: the pattern
-// (full symmetric, on host and device), its RCM order, the band factor and its panels, and a
-// cuBLAS handle on the caller's stream.  Members are released in reverse order: the cuBLAS
-// handle (after the stream drains), then the device buffers.
+// (full symmetric, on host and device), its RCM order, the band factor and its panels, and the
+// split-k workspace of the complex GEMMs.  The device buffers are released after the stream
+// drains.
 struct BandContext {
     Bufs B;
-    struct CbGuard {
-        cublasHandle_t h = nullptr;
-        cudaStream_t st = nullptr;
-        ~CbGuard() {
-            if (h) {
-                cudaStreamSynchronize(st);  // nothing queued may still use the handle's workspace
-                cublasDestroy(h);
-            }
-        }
-    } cbg;
     cudaStream_t st = nullptr;
     int64_t n = 0;
     std::vector<int64_t> frp, fmap;
     std::vector<int> fci, perm, iperm;
     int64_t *d_frp = nullptr, *d_fmap = nullptr;
     int *d_fci = nullptr, *d_iperm = nullptr;
+    double *d_nrm = nullptr;
     BandLDLT F;
 
     int init(cudaStream_t stream, int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind, int base,
@@ -778,11 +790,16 @@ struct BandContext {
             !need(B.alloc(&d_frp, n + 1), "the pattern") || !need(B.alloc(&d_fci, frp[n]), "the pattern") ||
             !need(B.alloc(&d_fmap, frp[n]), "the pattern") || !need(B.alloc(&d_iperm, n), "the ordering"))
             return E.code;
-        if (cublasCreate(&cbg.h) != CUBLAS_STATUS_SUCCESS) return E.set(SROM_ERR_CUDA, "cublasCreate failed");
-        cbg.st = st;
-        F.cb = cbg.h;
-        KBL(cublasSetStream(cbg.h, st));
-        KBL(cublasSetPointerMode(cbg.h, CUBLAS_POINTER_MODE_HOST));
+        {
+            int dev = 0;
+            KCU(cudaGetDevice(&dev));
+            KCU(cudaDeviceGetAttribute(&F.sms, cudaDevAttrMultiProcessorCount, dev));
+        }
+        // split-k partials: at most (2 SMs' worth + the tiles) 64 x 64 blocks
+        F.zwork_elems = (int64_t)(4 * F.sms + 64) * 64 * 64;
+        if (!need(B.alloc(&F.zwork, (size_t)F.zwork_elems), "the GEMM workspace") ||
+            !need(B.alloc(&d_nrm, znorm2_work_doubles() + 2), "the norm workspace"))
+            return E.code;
         const size_t smem = sizeof(double2) * NB * SLD;
         KCU(cudaFuncSetAttribute(ldlt_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         KCU(cudaFuncSetAttribute(ldlt_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -843,7 +860,6 @@ int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *
             *msg = std::string("allocating the Krylov blocks: ") + cudaGetErrorString(e);
             return e == cudaErrorMemoryAllocation ? SROM_ERR_ALLOC : SROM_ERR_CUDA;
         }
-    cublasHandle_t cb = X.cbg.h;
     auto run = [&]() -> int {
         int kv = 0;  // columns of V so far
         std::vector<double> rdiag;
@@ -864,7 +880,8 @@ int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *
                     if (s) return s;
                 }
                 if (ip > 0 || order > 1) {
-                    s = reorthogonalize(cb, st, reinterpret_cast<const double2 *>(a.V), a.ldv, kv, Q, U, n, m, S, E);
+                    s = reorthogonalize(X.F, st, reinterpret_cast<const double2 *>(a.V), a.ldv, kv, Q, U, n, m, S,
+                                        X.d_nrm, E);
                     if (s) return s;
                 }
                 int rr = 0;

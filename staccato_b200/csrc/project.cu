@@ -20,6 +20,7 @@
 namespace srom {
 
 constexpr int PRJ_MAX_MATS = 3;
+constexpr int PRJ_WIN = 128;  // basis columns per SpMM pass and per side of a V^T Y window
 
 // ---- V (column-major, ldv) -> Vt (row-major N x k) --------------------------------------
 __global__ void transpose_kernel(const double *__restrict__ V, int64_t N, int k, int64_t ldv,
@@ -58,11 +59,13 @@ struct SpmmStage {
     double val[3 * PRJ_MAX_MATS][32];
 };
 
+// Column window: the k (<= 32 CPL) basis columns starting at Vt (row stride ldv) into Y (row
+// stride ldy); a basis wider than 128 columns is projected window by window.
 template <int CPL, int NMAT, int NR>
 __device__ __forceinline__ void spmm_rows(int64_t row, const int64_t *__restrict__ rowptr,
                                           const int *__restrict__ colind, int base, const ProjVals &vals,
-                                          const double *__restrict__ Vt, int k, double *__restrict__ Y,
-                                          int64_t y_stride, int lane, SpmmStage &st) {
+                                          const double *__restrict__ Vt, int k, int ldv, double *__restrict__ Y,
+                                          int ldy, int64_t y_stride, int lane, SpmmStage &st) {
     const int64_t e0 = rowptr[row] - base, e1 = rowptr[row + 1] - base;
     int64_t off[NR];
 #pragma unroll
@@ -90,7 +93,7 @@ __device__ __forceinline__ void spmm_rows(int64_t row, const int64_t *__restrict
             double v[SPMM_DEPTH][CPL];
 #pragma unroll
             for (int u = 0; u < SPMM_DEPTH; ++u) {
-                const double *vr = Vt + (int64_t)st.col[j + u] * k;
+                const double *vr = Vt + (int64_t)st.col[j + u] * ldv;
 #pragma unroll
                 for (int q = 0; q < CPL; ++q) {
                     const int c = lane + 32 * q;
@@ -109,7 +112,7 @@ __device__ __forceinline__ void spmm_rows(int64_t row, const int64_t *__restrict
                     }
         }
         for (; j < cnt; ++j) {
-            const double *vr = Vt + (int64_t)st.col[j] * k;
+            const double *vr = Vt + (int64_t)st.col[j] * ldv;
 #pragma unroll
             for (int q = 0; q < CPL; ++q) {
                 const int c = lane + 32 * q;
@@ -128,7 +131,7 @@ __device__ __forceinline__ void spmm_rows(int64_t row, const int64_t *__restrict
 #pragma unroll
             for (int q = 0; q < CPL; ++q) {
                 const int c = lane + 32 * q;
-                if (c < k) Y[m * y_stride + (row + r) * k + c] = acc[r][m][q];
+                if (c < k) Y[m * y_stride + (row + r) * ldy + c] = acc[r][m][q];
             }
 }
 
@@ -136,7 +139,8 @@ template <int CPL, int NMAT>
 __global__ void __launch_bounds__(SPMM_THREADS) spmm_full_kernel(int64_t N, const int64_t *__restrict__ rowptr,
                                                                  const int *__restrict__ colind, int base,
                                                                  ProjVals vals, const double *__restrict__ Vt, int k,
-                                                                 double *__restrict__ Y, int64_t y_stride) {
+                                                                 int ldv, double *__restrict__ Y, int ldy,
+                                                                 int64_t y_stride) {
     __shared__ SpmmStage stage[SPMM_WARPS];
     const int lane = threadIdx.x & 31;
     SpmmStage &st = stage[threadIdx.x >> 5];
@@ -161,10 +165,10 @@ __global__ void __launch_bounds__(SPMM_THREADS) spmm_full_kernel(int64_t N, cons
             }
         }
         if (same) {
-            spmm_rows<CPL, NMAT, 3>(r0, rowptr, colind, base, vals, Vt, k, Y, y_stride, lane, st);
+            spmm_rows<CPL, NMAT, 3>(r0, rowptr, colind, base, vals, Vt, k, ldv, Y, ldy, y_stride, lane, st);
         } else {
             for (int r = 0; r < nr; ++r)
-                spmm_rows<CPL, NMAT, 1>(r0 + r, rowptr, colind, base, vals, Vt, k, Y, y_stride, lane, st);
+                spmm_rows<CPL, NMAT, 1>(r0 + r, rowptr, colind, base, vals, Vt, k, ldv, Y, ldy, y_stride, lane, st);
         }
     }
 }
@@ -172,23 +176,25 @@ __global__ void __launch_bounds__(SPMM_THREADS) spmm_full_kernel(int64_t N, cons
 // grid = at most one wave of resident CTAs (the row loop is grid-strided)
 template <int CPL, int NMAT>
 static void spmm_full_launch(int grid, cudaStream_t st, int64_t N, const int64_t *rowptr, const int *colind,
-                             int base, const ProjVals &vals, const double *Vt, int k, double *Y, int64_t y_stride) {
+                             int base, const ProjVals &vals, const double *Vt, int k, int ldv, double *Y, int ldy,
+                             int64_t y_stride) {
     int per_sm = 0, dev = 0, sms = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmm_full_kernel<CPL, NMAT>, SPMM_THREADS, 0) ==
             cudaSuccess &&
         cudaGetDevice(&dev) == cudaSuccess &&
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && per_sm > 0)
         grid = std::min(grid, per_sm * sms);
-    spmm_full_kernel<CPL, NMAT><<<grid, SPMM_THREADS, 0, st>>>(N, rowptr, colind, base, vals, Vt, k, Y, y_stride);
+    spmm_full_kernel<CPL, NMAT><<<grid, SPMM_THREADS, 0, st>>>(N, rowptr, colind, base, vals, Vt, k, ldv, Y, ldy,
+                                                               y_stride);
 }
 
 template <int CPL>
 static void launch_spmm_full(int grid, cudaStream_t st, int64_t N, const int64_t *rowptr, const int *colind,
-                             int base, const ProjVals &vals, int n_mats, const double *Vt, int k, double *Y,
-                             int64_t y_stride) {
-    if (n_mats == 1) spmm_full_launch<CPL, 1>(grid, st, N, rowptr, colind, base, vals, Vt, k, Y, y_stride);
-    else if (n_mats == 2) spmm_full_launch<CPL, 2>(grid, st, N, rowptr, colind, base, vals, Vt, k, Y, y_stride);
-    else spmm_full_launch<CPL, 3>(grid, st, N, rowptr, colind, base, vals, Vt, k, Y, y_stride);
+                             int base, const ProjVals &vals, int n_mats, const double *Vt, int k, int ldv, double *Y,
+                             int ldy, int64_t y_stride) {
+    if (n_mats == 1) spmm_full_launch<CPL, 1>(grid, st, N, rowptr, colind, base, vals, Vt, k, ldv, Y, ldy, y_stride);
+    else if (n_mats == 2) spmm_full_launch<CPL, 2>(grid, st, N, rowptr, colind, base, vals, Vt, k, ldv, Y, ldy, y_stride);
+    else spmm_full_launch<CPL, 3>(grid, st, N, rowptr, colind, base, vals, Vt, k, ldv, Y, ldy, y_stride);
 }
 
 // Upper-triangle storage of a symmetric matrix (the reference's CSR,
@@ -196,8 +202,8 @@ static void launch_spmm_full(int grid, cudaStream_t st, int64_t N, const int64_t
 // FP64 atomics after the row pass above has written the stored half.
 __global__ void spmm_upper_mirror_kernel(int64_t N, const int64_t *__restrict__ rowptr,
                                          const int *__restrict__ colind, int base, ProjVals vals, int n_mats,
-                                         const double *__restrict__ Vt, int k, double *__restrict__ Y,
-                                         int64_t y_stride) {
+                                         const double *__restrict__ Vt, int k, int ldv, double *__restrict__ Y,
+                                         int ldy, int64_t y_stride) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -207,57 +213,71 @@ __global__ void spmm_upper_mirror_kernel(int64_t N, const int64_t *__restrict__ 
             const int64_t col = colind[e] - base;
             if (col == row) continue;
             for (int c = lane; c < k; c += 32) {
-                const double v = Vt[row * k + c];
-                for (int m = 0; m < n_mats; ++m) atomicAdd(&Y[m * y_stride + col * k + c], vals.v[m][e] * v);
+                const double v = Vt[row * ldv + c];
+                for (int m = 0; m < n_mats; ++m) atomicAdd(&Y[m * y_stride + col * ldy + c], vals.v[m][e] * v);
             }
         }
     }
 }
 
 // ---- R_m partial = Vt[rows]^T Y_m[rows] on FP64 tensor cores ------------------------------
-// One launch covers nm matrices.  Warp w owns matrix w / ntile and the 8-row band w % ntile
-// of its R (ntile = kp / 8 bands, 8x8 tiles across the band).  The rows of Vt and of the nm
-// Y's are staged 32 at a time in shared memory (leading dimension kp + 4 keeps the fragment
-// loads free of bank conflicts); the Vt chunk is staged once for all nm matrices, and the
-// chunks are double-buffered with cp.async so the loads of chunk c + 1 overlap the MMAs of
-// chunk c.  Each CTA takes a contiguous range of chunks and writes a private k x k partial.
+// One launch covers nm matrices and one window of R: ka rows (basis columns of Vt, row stride
+// ldv) by kb columns (columns of Y_m, row stride ldy), both <= 128.  Warp w owns matrix
+// w / nband and the 8-row band w % nband of the window (nband = kap / 8), 8x8 tiles across it.
+// The rows of Vt and of the nm Y's are staged 32 at a time in shared memory (leading
+// dimension padded by 4 keeps the fragment loads free of bank conflicts); the Vt chunk is
+// staged once for all nm matrices, and the chunks are double-buffered with cp.async so the
+// loads of chunk c + 1 overlap the MMAs of chunk c.  Each CTA takes a contiguous range of
+// chunks and writes a private kap x kbp partial.
 __device__ __forceinline__ void cp_async8(double *dst, const double *src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src));
 }
 
+struct VtyWindow {
+    const double *Vt;  // first basis column of the window's rows
+    int ka, ldv;
+    const double *Y;   // first column of the window's columns (matrix 0)
+    int kb, ldy;
+    int64_t y_stride;  // between matrices
+};
+
 template <int TMAX, int MAXT>
-__global__ void __launch_bounds__(MAXT) vty_partial_kernel(int64_t N, int k, const double *__restrict__ Vt,
-                                                           const double *__restrict__ Y, int64_t y_stride, int nm,
-                                                           int64_t chunks_per_cta, double *__restrict__ partial) {
+__global__ void __launch_bounds__(MAXT) vty_partial_kernel(int64_t N, VtyWindow w, int nm, int64_t chunks_per_cta,
+                                                           double *__restrict__ partial) {
     extern __shared__ double sh[];
-    const int kp = (k + 7) & ~7;
-    const int ld = kp + 4;
-    const int ntile = kp / 8;
-    const int stage = (1 + nm) * 32 * ld;
+    const int kap = (w.ka + 7) & ~7, kbp = (w.kb + 7) & ~7;
+    const int lda = kap + 4, ldb = kbp + 4;
+    const int nband = kap / 8, ntile = kbp / 8;
+    const int a_sz = 32 * lda, b_sz = 32 * ldb;
+    const int stage = a_sz + nm * b_sz;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int mloc = warp / ntile, band = warp % ntile;
+    const int mloc = warp / nband, band = warp % nband;
     const bool active = mloc < nm;
     const int64_t n_chunks = (N + 31) / 32;
     const int64_t c_begin = (int64_t)blockIdx.x * chunks_per_cta;
     const int64_t c_end = min(n_chunks, c_begin + chunks_per_cta);
-    const int per_mat = 32 * kp;
-    const int total = (1 + nm) * per_mat;
+    const int a_tot = 32 * kap, total = a_tot + nm * 32 * kbp;
 
     auto issue = [&](int64_t ch, int buf) {
         double *dst0 = sh + buf * stage;
         const int64_t r0 = ch * 32;
         const int nr = (int)min((int64_t)32, N - r0);
         for (int e = threadIdx.x; e < total; e += blockDim.x) {
-            const int mat = e / per_mat, rem = e - mat * per_mat;
-            const int rr = rem / kp, c = rem - rr * kp;
-            double *dst = dst0 + mat * 32 * ld + rr * ld + c;
-            if (rr < nr && c < k) {
-                const double *src = mat == 0 ? Vt + (r0 + rr) * k + c : Y + (mat - 1) * y_stride + (r0 + rr) * k + c;
-                cp_async8(dst, src);
+            double *dst;
+            const double *src = nullptr;
+            if (e < a_tot) {
+                const int rr = e / kap, c = e - rr * kap;
+                dst = dst0 + rr * lda + c;
+                if (rr < nr && c < w.ka) src = w.Vt + (r0 + rr) * w.ldv + c;
             } else {
-                *dst = 0.0;
+                const int eb = e - a_tot, mat = eb / (32 * kbp), rem = eb - mat * 32 * kbp;
+                const int rr = rem / kbp, c = rem - rr * kbp;
+                dst = dst0 + a_sz + mat * b_sz + rr * ldb + c;
+                if (rr < nr && c < w.kb) src = w.Y + mat * w.y_stride + (r0 + rr) * w.ldy + c;
             }
+            if (src) cp_async8(dst, src);
+            else *dst = 0.0;
         }
         asm volatile("cp.async.commit_group;");
     };
@@ -277,15 +297,15 @@ __global__ void __launch_bounds__(MAXT) vty_partial_kernel(int64_t N, int k, con
         __syncthreads();
         if (active) {
             const double *sV = sh + buf * stage;
-            const double *sY = sV + (1 + mloc) * 32 * ld;
+            const double *sY = sV + a_sz + mloc * b_sz;
 #pragma unroll
             for (int kk = 0; kk < 8; ++kk) {
                 const int rr = 4 * kk + (lane & 3);
-                const double a = sV[rr * ld + 8 * band + (lane >> 2)];
+                const double a = sV[rr * lda + 8 * band + (lane >> 2)];
 #pragma unroll
                 for (int t = 0; t < TMAX; ++t) {
                     if (t < ntile) {
-                        const double b = sY[rr * ld + 8 * t + (lane >> 2)];
+                        const double b = sY[rr * ldb + 8 * t + (lane >> 2)];
                         asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                                      : "+d"(acc[t][0]), "+d"(acc[t][1])
                                      : "d"(a), "d"(b));
@@ -298,28 +318,29 @@ __global__ void __launch_bounds__(MAXT) vty_partial_kernel(int64_t N, int k, con
     if (active) {
         // lane holds D[row = lane/4][col = 2*(lane%4) + {0,1}] of tile (band, t)
         const int ra = 8 * band + (lane >> 2);
-        double *P = partial + ((int64_t)mloc * gridDim.x + blockIdx.x) * kp * kp;
+        double *P = partial + ((int64_t)mloc * gridDim.x + blockIdx.x) * kap * kbp;
 #pragma unroll
         for (int t = 0; t < TMAX; ++t) {
             if (t < ntile) {
                 const int cb = 8 * t + 2 * (lane & 3);
-                P[ra + (int64_t)cb * kp] = acc[t][0];
-                P[ra + (int64_t)(cb + 1) * kp] = acc[t][1];
+                P[ra + (int64_t)cb * kap] = acc[t][0];
+                P[ra + (int64_t)(cb + 1) * kap] = acc[t][1];
             }
         }
     }
 }
 
-__global__ void reduce_partials_kernel(const double *__restrict__ partial, int nblk, int nmat, int k, int kp,
-                                       ProjOut out) {
-    const int64_t tot = (int64_t)nmat * k * k;
+// out.r[m][a + b * ldr] = sum over the CTA partials, in CTA order (deterministic)
+__global__ void reduce_partials_kernel(const double *__restrict__ partial, int nblk, int nmat, int ka, int kb,
+                                       int kap, int kbp, ProjOut out, int ldr) {
+    const int64_t tot = (int64_t)nmat * ka * kb;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-        const int m = (int)(e / ((int64_t)k * k));
-        const int rem = (int)(e % ((int64_t)k * k));
-        const int a = rem % k, b = rem / k;
+        const int m = (int)(e / ((int64_t)ka * kb));
+        const int rem = (int)(e % ((int64_t)ka * kb));
+        const int a = rem % ka, b = rem / ka;
         double s = 0.0;
-        for (int blk = 0; blk < nblk; ++blk) s += partial[((int64_t)m * nblk + blk) * kp * kp + a + (int64_t)b * kp];
-        out.r[m][a + (int64_t)b * k] = s;
+        for (int blk = 0; blk < nblk; ++blk) s += partial[((int64_t)m * nblk + blk) * kap * kbp + a + (int64_t)b * kap];
+        out.r[m][a + (int64_t)b * ldr] = s;
     }
 }
 
@@ -643,61 +664,84 @@ cudaError_t launch_spmm(int64_t N, const int64_t *rowptr, const int *colind, int
     const int threads = SPMM_THREADS;
     const int64_t warps_needed = (N + 2) / 3;
     int grid = (int)std::min<int64_t>((warps_needed * 32 + threads - 1) / threads, (int64_t)sms * 8);
-    if (k <= 32) launch_spmm_full<1>(grid, st, N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
-    else if (k <= 64) launch_spmm_full<2>(grid, st, N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
-    else if (k <= 96) launch_spmm_full<3>(grid, st, N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
-    else launch_spmm_full<4>(grid, st, N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || !upper) return e;
-    spmm_upper_mirror_kernel<<<grid, threads, 0, st>>>(N, rowptr, colind, base, vals, n_mats, Vt, k, Y, y_stride);
-    return cudaGetLastError();
+    // window by window (PRJ_WIN columns of the basis at a time), each into its columns of Y
+    for (int j0 = 0; j0 < k; j0 += PRJ_WIN) {
+        const int kw = std::min(PRJ_WIN, k - j0);
+        const double *Vw = Vt + j0;
+        double *Yw = Y + j0;
+        if (kw <= 32) launch_spmm_full<1>(grid, st, N, rowptr, colind, base, vals, n_mats, Vw, kw, k, Yw, k, y_stride);
+        else if (kw <= 64) launch_spmm_full<2>(grid, st, N, rowptr, colind, base, vals, n_mats, Vw, kw, k, Yw, k, y_stride);
+        else if (kw <= 96) launch_spmm_full<3>(grid, st, N, rowptr, colind, base, vals, n_mats, Vw, kw, k, Yw, k, y_stride);
+        else launch_spmm_full<4>(grid, st, N, rowptr, colind, base, vals, n_mats, Vw, kw, k, Yw, k, y_stride);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (upper) {
+            spmm_upper_mirror_kernel<<<grid, threads, 0, st>>>(N, rowptr, colind, base, vals, n_mats, Vw, kw, k, Yw, k,
+                                                               y_stride);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
 }
 
-// matrices per launch: 24 warps at most for up to 12 bands (<= 80 registers a thread),
-// one matrix of up to 16 bands (512 threads)
-static int vty_group(int k, int n_mats) {
-    const int ntile = ((k + 7) & ~7) / 8;
-    return ntile > 12 ? 1 : std::max(1, std::min(n_mats, 24 / ntile));
+// matrices per launch: 24 warps at most (768 threads, <= 85 registers a thread) for windows
+// up to 12 tiles wide, 16 warps (512 threads) for wider ones
+static int vty_group(int ka, int kb, int n_mats) {
+    const int nband = ((ka + 7) & ~7) / 8, ntile = ((kb + 7) & ~7) / 8;
+    return std::max(1, std::min(n_mats, (ntile > 12 ? 16 : 24) / nband));
 }
 
-size_t vty_smem_bytes(int k, int n_mats) {
-    const int kp = (k + 7) & ~7;
-    return sizeof(double) * (size_t)2 * (1 + vty_group(k, n_mats)) * 32 * (kp + 4);
+size_t vty_partial_doubles(int k, int n_mats, int nblk) {
+    const int kp = (std::min(k, PRJ_WIN) + 7) & ~7;
+    return (size_t)nblk * n_mats * kp * kp;
 }
 
 template <int TMAX, int MAXT>
-static cudaError_t vty_launch(int64_t N, int k, const double *Vt, const double *Y, int64_t y_stride, int nm,
-                              int nblk, double *partial, cudaStream_t st) {
-    const int kp = (k + 7) & ~7;
-    const int threads = 32 * nm * (kp / 8);
-    const size_t smem = sizeof(double) * (size_t)2 * (1 + nm) * 32 * (kp + 4);
+static cudaError_t vty_launch(int64_t N, const VtyWindow &w, int nm, int nblk, double *partial, cudaStream_t st) {
+    const int kap = (w.ka + 7) & ~7, kbp = (w.kb + 7) & ~7;
+    const int threads = 32 * nm * (kap / 8);
+    const size_t smem = sizeof(double) * (size_t)2 * 32 * ((kap + 4) + (size_t)nm * (kbp + 4));
     auto kf = vty_partial_kernel<TMAX, MAXT>;
     cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int64_t n_chunks = (N + 31) / 32;
     const int64_t per = (n_chunks + nblk - 1) / nblk;
-    kf<<<nblk, threads, smem, st>>>(N, k, Vt, Y, y_stride, nm, per, partial);
+    kf<<<nblk, threads, smem, st>>>(N, w, nm, per, partial);
     return cudaGetLastError();
 }
 
+// R_m = Vt^T Y_m (k x k, leading dimension k) window by window: PRJ_WIN x PRJ_WIN blocks of R,
+// each one DMMA pass over the rows plus a deterministic reduction into its block.
 cudaError_t launch_vty(int64_t N, int k, const double *Vt, const double *Y, int64_t y_stride, int n_mats,
                        int nblk, double *partial, ProjOut out, cudaStream_t st) {
-    const int kp = (k + 7) & ~7;
-    const int ntile = kp / 8;
-    const int group = vty_group(k, n_mats);
-    for (int m0 = 0; m0 < n_mats; m0 += group) {
-        const int nm = std::min(group, n_mats - m0);
-        const double *Ym = Y + m0 * y_stride;
-        double *Pm = partial + (int64_t)m0 * nblk * kp * kp;
-        cudaError_t e;
-        if (ntile <= 4) e = vty_launch<4, 768>(N, k, Vt, Ym, y_stride, nm, nblk, Pm, st);
-        else if (ntile <= 8) e = vty_launch<8, 768>(N, k, Vt, Ym, y_stride, nm, nblk, Pm, st);
-        else if (ntile <= 12) e = vty_launch<12, 768>(N, k, Vt, Ym, y_stride, nm, nblk, Pm, st);
-        else e = vty_launch<16, 512>(N, k, Vt, Ym, y_stride, nm, nblk, Pm, st);
-        if (e != cudaSuccess) return e;
+    for (int i0 = 0; i0 < k; i0 += PRJ_WIN) {
+        const int ka = std::min(PRJ_WIN, k - i0);
+        const int kap = (ka + 7) & ~7;
+        for (int j0 = 0; j0 < k; j0 += PRJ_WIN) {
+            const int kb = std::min(PRJ_WIN, k - j0);
+            const int kbp = (kb + 7) & ~7, ntile = kbp / 8;
+            const int group = vty_group(ka, kb, n_mats);
+            for (int m0 = 0; m0 < n_mats; m0 += group) {
+                const int nm = std::min(group, n_mats - m0);
+                const VtyWindow w{Vt + i0, ka, k, Y + m0 * y_stride + j0, kb, k, y_stride};
+                double *Pm = partial + (int64_t)m0 * nblk * kap * kbp;
+                cudaError_t e;
+                if (ntile <= 4) e = vty_launch<4, 768>(N, w, nm, nblk, Pm, st);
+                else if (ntile <= 8) e = vty_launch<8, 768>(N, w, nm, nblk, Pm, st);
+                else if (ntile <= 12) e = vty_launch<12, 768>(N, w, nm, nblk, Pm, st);
+                else e = vty_launch<16, 512>(N, w, nm, nblk, Pm, st);
+                if (e != cudaSuccess) return e;
+            }
+            ProjOut o{};
+            for (int m = 0; m < n_mats; ++m) o.r[m] = out.r[m] + i0 + (int64_t)j0 * k;
+            const int64_t tot = (int64_t)n_mats * ka * kb;
+            reduce_partials_kernel<<<(int)((tot + 255) / 256), 256, 0, st>>>(partial, nblk, n_mats, ka, kb, kap, kbp,
+                                                                               o, k);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+        }
     }
-    reduce_partials_kernel<<<(n_mats * k * k + 255) / 256, 256, 0, st>>>(partial, nblk, n_mats, k, kp, out);
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 size_t gs_workspace_doubles(int k, int nblk) {

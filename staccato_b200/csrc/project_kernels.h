@@ -15,10 +15,14 @@ struct ProjOut {
     double *r[3];
 };
 
+// widest basis of the projection (real form; the complex form projects 2k real columns)
+constexpr int PRJ_MAX_K = 4096;
+
 cudaError_t launch_transpose(const double *V, int64_t N, int k, int64_t ldv, double *Vt, cudaStream_t st);
 cudaError_t launch_spmm(int64_t N, const int64_t *rowptr, const int *colind, int base, int upper, ProjVals vals,
                         int n_mats, const double *Vt, int k, double *Y, int64_t y_stride, int sms, cudaStream_t st);
-size_t vty_smem_bytes(int k, int n_mats);
+// doubles of the V^T Y partials buffer (one window of at most 128 x 128 per matrix and CTA)
+size_t vty_partial_doubles(int k, int n_mats, int nblk);
 cudaError_t launch_vty(int64_t N, int k, const double *Vt, const double *Y, int64_t y_stride, int n_mats, int nblk,
                        double *partial, ProjOut out, cudaStream_t st);
 cudaError_t launch_transpose_split(const double2 *V, int64_t N, int k, int64_t ldv, double *Wt, cudaStream_t st);

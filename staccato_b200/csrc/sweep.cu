@@ -570,21 +570,25 @@ __device__ void trailing_update(T *A, int64_t lda, int n, int j0, int nbc, const
 // The u and panel regions come last: during the mixed form's refinement neither is in use, and
 // together with whatever dynamic shared memory lies beyond `total` they form the staging ring
 // of the correction solves (ring = [u, end of the dynamic allocation)).
+// big: the large-order FP64 instances (orders whose panel does not fit shared memory): the
+// panel lives in global scratch, the panel region holds the solve's 32 x 33 diagonal tile
+// instead, and the mixed form's regions (work32, pos, dinv) are empty.
 struct GlobalSmem {
     size_t work64, work32, perm, ptot, pos, ipiv, moved, dinv, u, panel, total;
     static __host__ __device__ size_t up(size_t b) { return (b + 255) / 256 * 256; }
-    __host__ __device__ GlobalSmem(int ldp, int n_max, int r_max) {
+    __host__ __device__ GlobalSmem(int ldp, int n_max, int r_max, bool big = false) {
         work64 = 0;
         work32 = work64 + up((size_t)n_max * r_max * 16);
-        perm = work32 + up((size_t)n_max * r_max * 8);
+        perm = work32 + (big ? 0 : up((size_t)n_max * r_max * 8));
         ptot = perm + up((size_t)ldp * 4);
         pos = ptot + up((size_t)ldp * 4);
-        ipiv = pos + up((size_t)ldp * 4);
+        ipiv = pos + (big ? 0 : up((size_t)ldp * 4));
         moved = ipiv + up((size_t)ldp * 4);
         dinv = moved + up((size_t)2 * 2 * NB32 * 4);
-        u = dinv + up((size_t)ldp * 16);                  // reciprocals of diag(U), mixed form
+        u = dinv + (big ? 0 : up((size_t)ldp * 16));      // reciprocals of diag(U), mixed form
         panel = u + up((size_t)NW * 2048);                // per warp NB x CWG complex
-        total = panel + up((size_t)ldp * 256);            // ldp x 16 double2 == ldp x 32 float2
+        total = panel + (big ? up((size_t)32 * 33 * 16)   // the solve's diagonal tile
+                             : up((size_t)ldp * 256));    // ldp x 16 double2 == ldp x 32 float2
     }
 };
 
@@ -594,8 +598,9 @@ struct GlobalSmem {
 template <typename T, int NB, int RPT>
 __device__ void factor_global(T *A, int64_t lda, int n, int ldp, unsigned char *sm, const GlobalSmem &L,
                               T *B, int nrhs, PanelLists &PL, PivotXchg<typename CT<T>::R> &X,
-                              int *s_pivlg) {
-    T *P = reinterpret_cast<T *>(sm + L.panel);
+                              int *s_pivlg, T *P_global = nullptr) {
+    // the panel: shared memory, or (large orders) the CTA's global scratch, L2-resident
+    T *P = P_global ? P_global : reinterpret_cast<T *>(sm + L.panel);
     T *s_u = reinterpret_cast<T *>(sm + L.u);
     int *s_perm = reinterpret_cast<int *>(sm + L.perm);
     int *s_ptot = reinterpret_cast<int *>(sm + L.ptot);
@@ -644,8 +649,12 @@ __device__ void factor_global(T *A, int64_t lda, int n, int ldp, unsigned char *
 // Global-class kernel.  MIXED: complex-FP32 factors + FP64 refinement; systems that do not
 // converge are appended to a.fb_items (when given) for the FP64 kernel launched after it.
 // FP64: the bit-exact path; a.n_items_dev (when given) holds the item count (fallback list).
-template <bool MIXED, int RPT>
+// BIG (FP64 only): the panel in global scratch (a.panel_off into the CTA's slot) and the
+// tile-staged blocked solve (lu_solve), for orders up to NT * RPT whose panel does not fit
+// shared memory.
+template <bool MIXED, int RPT, bool BIG = false>
 __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
+    static_assert(!(MIXED && BIG), "large orders are FP64 only");
     extern __shared__ __align__(256) unsigned char sm[];
     __shared__ int s_item;
     __shared__ int s_pivlg[NB32];
@@ -653,7 +662,7 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
     __shared__ PivotXchg<typename CT<typename std::conditional<MIXED, float2, double2>::type>::R> Xx;
     __shared__ double s_dx[RMAX_MIXED];
     using T = typename std::conditional<MIXED, float2, double2>::type;
-    const GlobalSmem L(a.ldp, a.n_max, a.r_max);
+    const GlobalSmem L(a.ldp, a.n_max, a.r_max, BIG);
     const int tid = threadIdx.x;
     const int n_items = a.n_items_dev ? *a.n_items_dev : a.n_items;
     int *s_ipiv = reinterpret_cast<int *>(sm + L.ipiv);
@@ -689,9 +698,16 @@ __global__ void __launch_bounds__(NT) sweep_global_kernel(GlobalArgs a) {
             assemble_into<double2>(A64, n, R, w, wi.f);
             load_rhs(B, n, R);
             __syncthreads();
-            factor_global<double2, NB64, RPT>(A64, n, n, a.ldp, sm, L, B, R.r, PL, Xx, s_pivlg);
-            info = PL.info;
-            lu_solve_strips<double2, 8>(A64, n, n, B, n, R.r, reinterpret_cast<double2 *>(sm + L.panel));
+            if constexpr (BIG) {
+                double2 *Pg = reinterpret_cast<double2 *>(a.scratch + (int64_t)blockIdx.x * a.slot_bytes + a.panel_off);
+                factor_global<double2, NB64, RPT>(A64, n, n, a.ldp, sm, L, B, R.r, PL, Xx, s_pivlg, Pg);
+                info = PL.info;
+                lu_solve<double2>(A64, n, n, B, n, R.r, reinterpret_cast<double2 *>(sm + L.panel));
+            } else {
+                factor_global<double2, NB64, RPT>(A64, n, n, a.ldp, sm, L, B, R.r, PL, Xx, s_pivlg);
+                info = PL.info;
+                lu_solve_strips<double2, 8>(A64, n, n, B, n, R.r, reinterpret_cast<double2 *>(sm + L.panel));
+            }
             store_solution(B, n, R, wi.f);
             steps = a.steps_value;
             if (R.ipiv)
@@ -714,9 +730,18 @@ size_t fp64_smem_bytes(int n, int r) {
     return sizeof(double2) * (lda * n + (size_t)n * r) + sizeof(int) * (size_t)n;
 }
 
-size_t global_smem_bytes(int n_max, int r_max) { return GlobalSmem(n_max | 1, n_max, r_max).total; }
+size_t global_smem_bytes(int n_max, int r_max, bool big) { return GlobalSmem(n_max | 1, n_max, r_max, big).total; }
 
-size_t fp64_global_smem_bytes(int n_max, int r_max) { return global_smem_bytes(n_max, r_max); }
+bool global_panel_fits(int n_max, int r_max, int smem_optin) {
+    return global_rpt(n_max) <= GLOBAL_MAX_RPT &&
+           global_smem_bytes(n_max, r_max, false) + GLOBAL_STATIC_SMEM <= (size_t)smem_optin;
+}
+
+int64_t big_panel_offset(int n_max) { return ((int64_t)n_max * n_max * 16 + 255) / 256 * 256; }
+
+int64_t big_slot_bytes(int n_max) { return big_panel_offset(n_max) + (int64_t)(n_max | 1) * NB64 * 16; }
+
+size_t fp64_global_smem_bytes(int n_max, int r_max) { return global_smem_bytes(n_max, r_max, false); }
 
 int global_rpt(int n_max) { return (n_max + NT - 1) / NT; }
 
@@ -739,11 +764,11 @@ int fp64_smem_blocks_per_sm(size_t smem) {
 
 // The mixed kernel takes all the shared memory a CTA may have (one CTA per SM either way, by
 // registers): what lies beyond its fixed regions deepens the correction solves' staging ring.
-template <bool MIXED, int RPT>
+template <bool MIXED, int RPT, bool BIG = false>
 static cudaError_t launch_global_t(const GlobalArgs &a0, int grid, cudaStream_t st) {
-    auto k = sweep_global_kernel<MIXED, RPT>;
+    auto k = sweep_global_kernel<MIXED, RPT, BIG>;
     GlobalArgs a = a0;
-    size_t smem = global_smem_bytes(a.n_max, a.r_max);
+    size_t smem = global_smem_bytes(a.n_max, a.r_max, BIG);
     if (MIXED) {
         int dev = 0, optin = 0;
         cudaFuncAttributes fa{};
@@ -778,6 +803,18 @@ cudaError_t launch_global(bool mixed, const GlobalArgs &a0, int grid, cudaStream
         if (rpt == 2) return launch_global_t<false, 2>(a, grid, st);
         if (rpt == 3) return launch_global_t<false, 3>(a, grid, st);
     }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_global_big(const GlobalArgs &a0, int grid, cudaStream_t st) {
+    GlobalArgs a = a0;
+    a.ldp = a.n_max | 1;
+    if (a.slot_bytes < big_slot_bytes(a.n_max)) return cudaErrorInvalidValue;
+    a.panel_off = big_panel_offset(a.n_max);
+    const int rpt = global_rpt(a.n_max);
+    if (rpt <= 3) return launch_global_t<false, 3, true>(a, grid, st);
+    if (rpt <= 6) return launch_global_t<false, 6, true>(a, grid, st);
+    if (rpt <= BIG_RPT) return launch_global_t<false, BIG_RPT, true>(a, grid, st);
     return cudaErrorInvalidValue;
 }
 

@@ -336,7 +336,9 @@ __device__ void residual64(const RomDev &R, double w, const double2 *X64, float2
 }
 
 // x += d (FP32 correction) and, per right-hand side, the relative correction size
-// ||d||_inf / ||x||_inf (|re|+|im| norms) into s_dx; one warp per right-hand side.
+// ||d||_2 / ||x||_2 into s_dx; one warp per right-hand side.  The 2-norm is the norm of the
+// accuracy criterion (relative 2-norm error per system): with max norms the estimate missed
+// errors spread over many entries of a solution dominated by a few (near resonance).
 static __device__ void apply_correction(double2 *X, const float2 *B32, int n, int nrhs, double *s_dx) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int c = warp; c < nrhs; c += NW) {
@@ -346,15 +348,15 @@ static __device__ void apply_correction(double2 *X, const float2 *B32, int n, in
             double2 &x = X[i + (int64_t)c * n];
             x.x += (double)d.x;
             x.y += (double)d.y;
-            dm = fmax(dm, fabs((double)d.x) + fabs((double)d.y));
-            xm = fmax(xm, fabs(x.x) + fabs(x.y));
+            dm = fma((double)d.x, (double)d.x, fma((double)d.y, (double)d.y, dm));
+            xm = fma(x.x, x.x, fma(x.y, x.y, xm));
         }
 #pragma unroll
         for (int off = 16; off; off >>= 1) {
-            dm = fmax(dm, __shfl_xor_sync(FULL_MASK, dm, off));
-            xm = fmax(xm, __shfl_xor_sync(FULL_MASK, xm, off));
+            dm += __shfl_xor_sync(FULL_MASK, dm, off);
+            xm += __shfl_xor_sync(FULL_MASK, xm, off);
         }
-        if (lane == 0) s_dx[c] = xm > 0.0 ? dm / xm : (dm > 0.0 ? INFINITY : 0.0);
+        if (lane == 0) s_dx[c] = xm > 0.0 ? sqrt(dm / xm) : (dm > 0.0 ? INFINITY : 0.0);
     }
     __syncthreads();
 }
@@ -537,11 +539,13 @@ __device__ void mixed_refine(const GlobalArgs &a, const RomDev &R, const Item &w
         apply_correction(W.X, W.B32, n, R.r, W.s_dx);
         if (s > 0) {
             // error left after this correction ~ rho * ||d||, rho ~ ||d_s|| / ||d_{s-1}||
-            // (the contraction of the iteration), taken twice for safety
+            // (the contraction of the iteration), taken twice for safety.  After the first
+            // correction the ratio is ||d_1|| / ||x||, the relative error of the first solve,
+            // a weaker stand-in for the contraction: it is taken four times.
             double worst = 0.0;
             for (int c = 0; c < R.r; ++c) worst = fmax(worst, W.s_dx[c]);
             const double ratio = worst / prev;
-            const double rho = fmin(1.0, 2.0 * ratio);
+            const double rho = fmin(1.0, (s == 1 ? 4.0 : 2.0) * ratio);
             berr = worst * rho;
             conv = berr <= tol_x;
             prev = worst;

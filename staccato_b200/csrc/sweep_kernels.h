@@ -21,9 +21,17 @@ size_t fp64_global_smem_bytes(int n_max, int r_max);
 int fp64_smem_blocks_per_sm(size_t smem);
 cudaError_t launch_fp64_smem(const RomDev *roms, const Item *items, int n_items, int *counter,
                              size_t smem, int grid, cudaStream_t st);
-size_t global_smem_bytes(int n_max, int r_max);
+// dynamic shared memory of the global kernels; big: the large-order FP64 instances
+size_t global_smem_bytes(int n_max, int r_max, bool big = false);
+// the shared-memory-panel instances (launch_global) can run (n_max, r_max)
+bool global_panel_fits(int n_max, int r_max, int smem_optin);
 int global_rpt(int n_max);
-constexpr int GLOBAL_MAX_RPT = 3;
+constexpr int GLOBAL_MAX_RPT = 3;   // rows per thread of the shared-memory-panel instances
+constexpr int BIG_RPT = 10;         // the largest large-order FP64 instance: n <= NT * BIG_RPT = 2560
+constexpr int BIG_MAX_N = 256 * BIG_RPT;
+// large-order FP64 instance: global scratch per CTA (the matrix, then the 16-column panel)
+int64_t big_panel_offset(int n_max);
+int64_t big_slot_bytes(int n_max);
 constexpr int MIXED_MAX_R = 16;
 constexpr size_t GLOBAL_STATIC_SMEM = 4096;
 // Arguments of the global-storage kernels.
@@ -43,9 +51,13 @@ struct GlobalArgs {
     int steps_value;  // FP64: value stored in steps (0; -1 when re-solving mixed fallbacks)
     int smem_dyn;     // dynamic shared memory of the launch (set by launch_global)
     int *err_flag;    // tensor-core kernel: set to 1 when a bounded device-side wait ran out
+    int64_t panel_off;  // large-order FP64 instances: offset of the panel in a slot (set by launch_global_big)
 };
 // Global-storage kernel, FP64 (mixed = false) or complex-FP32 factors + FP64 refinement.
 cudaError_t launch_global(bool mixed, const GlobalArgs &a, int grid, cudaStream_t st);
+// FP64 sweep of orders up to BIG_MAX_N with the panel in global scratch (slot_bytes >=
+// big_slot_bytes(n_max)); 3, 6 or 10 rows per thread by n_max
+cudaError_t launch_global_big(const GlobalArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_fp64_global(const RomDev *roms, const Item *items, int n_items, int *counter,
                                double2 *scratch, int64_t slot_elems, int n_max, int r_max,
                                int grid, cudaStream_t st);

@@ -30,6 +30,7 @@ from typing import List, Optional, Sequence, Union
 import numpy as np
 
 from . import _capi
+from .linalg import OP_N, OP_T, zgemm
 from .sweep import DeviceRom, solve_batched, sweep
 
 
@@ -111,22 +112,42 @@ def couple(handle: _capi.Handle, models: Sequence[Model], dRdY: Sequence[np.ndar
         ys.append(y)
     ps = [int(H.shape[1]) for H in Hs]
     G = sum(ps)
-    dY = [torch.as_tensor(a, dtype=torch.complex128, device=dev) for a in dRdY]
-    dU = [torch.as_tensor(a, dtype=torch.complex128, device=dev) for a in dRdU]
+    dY = [torch.as_tensor(a, dtype=torch.complex128, device=dev).contiguous() for a in dRdY]
+    dU = [torch.as_tensor(a, dtype=torch.complex128, device=dev).contiguous() for a in dRdU]
+    Hs = [H.contiguous() for H in Hs]
+    ys = [y.contiguous() for y in ys]
     for s, p in enumerate(ps):
         if tuple(dY[s].shape) != (G, p) or tuple(dU[s].shape) != (G, p):
             raise ValueError(f"dRdY[{s}] and dRdU[{s}] must be {G} x {p}")
     U = [torch.zeros((nf, p), dtype=torch.complex128, device=dev) if U0 is None
          else torch.as_tensor(U0[s], dtype=torch.complex128, device=dev).expand(nf, p).clone()
          for s, p in enumerate(ps)]
-    # interface Jacobian: column block s = dR/dY_s H_s + dR/dU_s   (constant in U)
-    J = torch.cat([dY[s] @ Hs[s] + dU[s] for s in range(len(ps))], dim=2)  # (nf, G, G)
     offs = np.cumsum([0] + ps)
+    # Products on the library's batched complex GEMM, in column-major terms (a row-major
+    # (a, b) tensor is the column-major b x a matrix, its transpose).
+    # Interface Jacobian J (nf, G, G), column block s = dR/dY_s H_s + dR/dU_s (constant in U):
+    # J_s^T = H_s^T dY_s^T + dU_s^T per frequency.
+    J = torch.empty((nf, G, G), dtype=torch.complex128, device=dev)
+    for s, p in enumerate(ps):
+        J[:, :, offs[s]:offs[s + 1]] = dU[s]
+        zgemm(handle, OP_N, OP_N, p, G, p, Hs[s], p, p * p, dY[s], p, 0, J[:, :, offs[s]:], G, G * G,
+              batch=nf, beta=1.0)
 
     def outputs_and_residual():
-        Y = [torch.einsum("fij,fj->fi", Hs[s], U[s]) + ys[s] for s in range(len(ps))]
-        R = sum(torch.einsum("gi,fi->fg", dY[s], Y[s]) + torch.einsum("gi,fi->fg", dU[s], U[s])
-                for s in range(len(ps)))
+        # Y_s[f] = H_s[f] U_s[f] + y_s[f]   (y^T = U^T H^T: op T on the column-major H^T)
+        Y = []
+        for s, p in enumerate(ps):
+            Ys = ys[s].clone()
+            zgemm(handle, OP_T, OP_N, p, 1, p, Hs[s], p, p * p, U[s], p, p, Ys, p, p, batch=nf, beta=1.0)
+            Y.append(Ys)
+        # R[f] = sum_s dY_s Y_s[f] + dU_s U_s[f], all frequencies at once: R^T = dY_s Y_s^T + ...
+        R = torch.empty((nf, G), dtype=torch.complex128, device=dev)
+        first = True
+        for s, p in enumerate(ps):
+            for Dm, X in ((dY[s], Y[s]), (dU[s], U[s])):
+                zgemm(handle, OP_T, OP_N, G, nf, p, Dm, p, 0, X.contiguous(), p, 0, R, G, 0,
+                      beta=0.0 if first else 1.0)
+                first = False
         return Y, R
 
     Y, R = outputs_and_residual()

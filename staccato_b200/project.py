@@ -65,7 +65,7 @@ def project(handle: _capi.Handle, csr: DeviceCsr, values: Sequence, V) -> List:
 
 def project_complex(handle: _capi.Handle, csr: DeviceCsr, values: Sequence, V, Z=None) -> List:
     """R_m = Z^H A_m V (Z = V by default) for complex values sharing one CSR pattern
-    (``srom_project_complex``, k <= 64).  values: complex128 tensors (nnz each); V, Z:
+    (``srom_project_complex``, k <= 2048).  values: complex128 tensors (nnz each); V, Z:
     contiguous (k, n_rows) complex128 tensors = n_rows x k column-major bases.  Returns k x k
     complex128 tensors."""
     import torch

@@ -65,8 +65,8 @@ class KrylovROMSubstructure:
         (KrylovROMSubstructure.cpp:709-765): K_r = V^H K V, M_r = V^H M V, D_r = V^H D V,
         B_r = V^H B, C_r = C V.
 
-        V: (k, n) tensor = n x k column-major basis, float64 (real form, k <= 128) or
-        complex128 (complex form, k <= 64; complex values are used as given, real values are
+        V: (k, n) tensor = n x k column-major basis, float64 (real form, k <= 4096) or
+        complex128 (complex form, k <= 2048; complex values are used as given, real values are
         promoted).  B: n x n_in, C: n_out x n."""
         import torch
 

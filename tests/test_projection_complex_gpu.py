@@ -33,7 +33,8 @@ def _csym(n, density, seed):
     return A, vals
 
 
-@pytest.mark.parametrize("k", [1, 13, 64])
+# k > 64: the 2k real columns take several windows of 128
+@pytest.mark.parametrize("k", [1, 13, 64, 65, 100, 150])
 @pytest.mark.parametrize("base,upper,two_sided", [(0, False, False), (1, True, False), (0, False, True)])
 def test_complex_projection(handle, k, base, upper, two_sided):
     n = 1200
@@ -84,7 +85,7 @@ def test_complex_projection_rejects_wide_basis(handle):
 
     A, vals = _csym(100, 0.05, 1)
     csr = DeviceCsr.from_host(A.indptr, A.indices)
-    V = torch.zeros((65, 100), dtype=torch.complex128, device="cuda")
+    V = torch.zeros((2049, 100), dtype=torch.complex128, device="cuda")
     with pytest.raises(_capi.SromError) as e:
         project_complex(handle, csr, [_dev(vals[0])], V)
     assert e.value.status == _capi.SROM_ERR_UNSUPPORTED

@@ -32,7 +32,8 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-@pytest.mark.parametrize("k", [1, 8, 33, 96, 128])
+# k > 128: several SpMM passes and V^T Y windows (128 columns each), ragged last window
+@pytest.mark.parametrize("k", [1, 8, 33, 96, 128, 129, 200, 300])
 @pytest.mark.parametrize("base,upper", [(0, False), (1, False), (1, True)])
 def test_projection_random(handle, k, base, upper):
     n = 1500
