@@ -167,10 +167,15 @@ SROM_API int srom_graph_launch(srom_graph *graph, void *cuda_stream);
 SROM_API int srom_graph_destroy(srom_graph *graph);
 
 /*
- * Autotune the FP64 kernel choice (whole system in shared memory vs. blocked LU in global
- * scratch) for each order in n_values with r right-hand sides: both are timed on a synthetic
- * system and the faster is used by later sweeps on this handle.  cache_path (or NULL) is a
- * JSON file of earlier choices for this device, read first and rewritten with new entries.
+ * Autotune the kernel choices for each order in n_values with r right-hand sides, timed on a
+ * synthetic system (2 x SMs frequencies) and used by later sweeps on this handle:
+ *   - FP64: the whole system in shared memory vs. the blocked LU in global scratch;
+ *   - mixed forms, where the FP64 choice is the shared-memory kernel: solving such systems in
+ *     FP64 outright (steps = 0) vs. complex-FP32 factors in the mixed global kernel plus
+ *     refinement (without a measurement the rule is: FP64 when two systems fit an SM).
+ * Panel width, tile shapes and threads per system are fixed per kernel by its register and
+ * shared-memory budget (compile-time).  cache_path (or NULL) is a JSON file of earlier choices
+ * for this device, read first and rewritten with new entries.
  */
 SROM_API int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char *cache_path);
 
@@ -304,6 +309,18 @@ SROM_API int srom_fom_sweep(srom_handle *h, int64_t n_rows, int64_t nnz, const i
                             int base, int upper, const srom_complex *K, const srom_complex *M, const srom_complex *D,
                             const srom_complex *F, int r, int64_t ldf, const double *freq_hz, int n_freq,
                             srom_complex *X, int64_t ldx);
+
+/*
+ * Pivots of the band L D L^T factorisations made by the last srom_krylov_basis or
+ * srom_fom_sweep call on this handle.  The factorisation does not pivot; like PARDISO with the
+ * reference's iparm[9] = 13 (KrylovROMSubstructure.cpp:621) it replaces a pivot d with
+ * |d| < 1e-13 ||A||_inf by the value of the same phase and modulus 1e-13 ||A||_inf and goes on
+ * (an exactly zero pivot still fails the call).  factorisations, perturbed: counts;
+ * min_pivot_ratio: the smallest |d| / ||A||_inf before perturbation (a small value warns of a
+ * shift close to an eigenvalue).  Any output pointer may be NULL.
+ */
+SROM_API int srom_band_pivot_report(const srom_handle *h, int64_t *factorisations, int64_t *perturbed,
+                                    double *min_pivot_ratio);
 
 /*
  * Host-only: the reverse Cuthill-McKee ordering srom_krylov_basis uses for a pattern (HOST

@@ -37,7 +37,7 @@ EXPORTS = [
     "srom_sweep_backward",
     "srom_graph_create", "srom_graph_launch", "srom_graph_destroy", "srom_tune",
     "srom_mtx_read_dense", "srom_mtx_write_dense", "srom_write_solution",
-    "srom_krylov_basis", "srom_band_order", "srom_fom_sweep", "srom_zgemm_batched",
+    "srom_krylov_basis", "srom_band_order", "srom_fom_sweep", "srom_zgemm_batched", "srom_band_pivot_report",
 ]
 
 SROM_OP_N = 0
@@ -130,6 +130,8 @@ def lib() -> C.CDLL:
         L.srom_zgemm_batched.argtypes = [vp, i, i, i, i, i, Complex, vp, C.c_int64, C.c_int64, vp, C.c_int64,
                                          C.c_int64, Complex, vp, C.c_int64, C.c_int64, i]
         L.srom_zgemm_batched.restype = i
+        L.srom_band_pivot_report.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+        L.srom_band_pivot_report.restype = i
         L.srom_orthonormalize.argtypes = [vp, vp, C.c_int64, i, C.c_int64, i]
         L.srom_orthonormalize.restype = i
         L.srom_graph_create.argtypes = [vp, C.POINTER(RomDesc), i, C.POINTER(SweepOpts), pp]

@@ -53,6 +53,8 @@ struct srom_handle {
     // split-k partials of srom_zgemm_batched
     void *d_zwork = nullptr;
     size_t d_zwork_bytes = 0;
+    // pivots of the band factorisations of the last srom_krylov_basis / srom_fom_sweep call
+    srom::kry::PivotStats band_stats;
     // per-launch profiling
     struct ProfRec {
         std::string name;
@@ -64,6 +66,9 @@ struct srom_handle {
     std::vector<ProfRec> recs;
     // FP64 storage class chosen by srom_tune per (n << 16 | r): 0 smem kernel, 1 global kernel
     std::map<long long, int> tune_fp64;
+    // mixed-form routing chosen by srom_tune per (n << 16 | r) where the FP64 smem kernel is
+    // the FP64 choice: 0 solve in FP64 outright, 1 mixed global kernel
+    std::map<long long, int> tune_mixed;
     std::vector<cudaEvent_t> event_pool;
     // error word of the last tensor-core sweep (device, inside d_meta) and its pinned host copy
     int *tc_flag_dev = nullptr;
@@ -405,6 +410,8 @@ int mixed_class(const srom_handle *h, int n, int r, int flags) {
     if (large_order(h, n, r)) return 2;
     if (flags & SROM_FLAG_MIXED_EVERY) return 1;
     if (fp64_class(h, n, r) != 0) return 1;
+    auto it = h->tune_mixed.find(((long long)n << 16) | r);  // srom_tune's measurement, if any
+    if (it != h->tune_mixed.end()) return it->second;
     return srom::fp64_smem_blocks_per_sm(srom::fp64_smem_bytes(n, r)) >= 2 ? 0 : 1;
 }
 
@@ -743,6 +750,15 @@ int srom_graph_destroy(srom_graph *G) {
     return SROM_OK;
 }
 
+int srom_band_pivot_report(const srom_handle *h, int64_t *factorisations, int64_t *perturbed,
+                           double *min_pivot_ratio) {
+    if (!h) return SROM_ERR_INVALID;
+    if (factorisations) *factorisations = h->band_stats.factorisations;
+    if (perturbed) *perturbed = h->band_stats.perturbed;
+    if (min_pivot_ratio) *min_pivot_ratio = h->band_stats.min_pivot_ratio;
+    return SROM_OK;
+}
+
 int srom_zgemm_batched(srom_handle *h, int opa, int opb, int m, int n, int k, srom_complex alpha, const srom_complex *A,
                        int64_t lda, int64_t stride_a, const srom_complex *B, int64_t ldb, int64_t stride_b,
                        srom_complex beta, srom_complex *C, int64_t ldc, int64_t stride_c, int batch) {
@@ -1049,6 +1065,8 @@ int srom_krylov_basis(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t
     a.V = V;
     a.ldv = ldv;
     a.max_cols = max_cols;
+    h->band_stats = srom::kry::PivotStats{};
+    a.stats = &h->band_stats;
     std::string msg;
     ProfScope ps(h, "krylov_basis", n_points, 0.0, 0.0);
     const int s = srom::kry::krylov_basis(a, &msg, n_cols, nullptr);
@@ -1093,6 +1111,8 @@ int srom_fom_sweep(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t *r
     a.n_freq = n_freq;
     a.X = X;
     a.ldx = ldx;
+    h->band_stats = srom::kry::PivotStats{};
+    a.stats = &h->band_stats;
     std::string msg;
     ProfScope ps(h, "fom_sweep", n_freq, 0.0, 0.0);
     const int s = srom::kry::fom_sweep(a, &msg);
@@ -1258,6 +1278,9 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
                 if (same_dev && sscanf(line, " {\"precision\": \"fp64\", \"n\": %d, \"r\": %d, \"kernel\": \"%31[^\"]\"",
                                        &n, &rr, kern) == 3)
                     h->tune_fp64[((long long)n << 16) | rr] = strcmp(kern, "smem") == 0 ? 0 : 1;
+                if (same_dev && sscanf(line, " {\"precision\": \"mixed\", \"n\": %d, \"r\": %d, \"kernel\": \"%31[^\"]\"",
+                                       &n, &rr, kern) == 3)
+                    h->tune_mixed[((long long)n << 16) | rr] = strcmp(kern, "fp64_smem") == 0 ? 0 : 1;
             }
             fclose(fp);
         }
@@ -1266,6 +1289,8 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
     struct Entry {
         int n, r, cls;
         float ms[2];
+        int mcls;      // mixed routing (-1: not measured)
+        float mms[2];  // mixed sweep: FP64 outright, mixed global kernel
     };
     std::vector<Entry> measured;
     for (int q = 0; q < count; ++q) {
@@ -1315,21 +1340,44 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
         for (int k = 0; k < 4 && rc == SROM_OK; ++k)
             if ((e = cudaMemcpy(dst[k], src[k], bytes[k], cudaMemcpyHostToDevice)) != cudaSuccess)
                 rc = set_err(h, SROM_ERR_CUDA, "tuning input copy: %s", cudaGetErrorString(e));
-        Entry ent{n, r, 0, {0.f, 0.f}};
+        Entry ent{n, r, 0, {0.f, 0.f}, -1, {0.f, 0.f}};
         cudaEvent_t a = nullptr, b = nullptr;
         if (rc == SROM_OK && ((e = cudaEventCreate(&a)) != cudaSuccess || (e = cudaEventCreate(&b)) != cudaSuccess))
             rc = set_err(h, SROM_ERR_CUDA, "tuning events: %s", cudaGetErrorString(e));
+        // one warm-up sweep, then three timed ones
+        auto time_sweep = [&](const srom_sweep_opts &o, float *ms) {
+            int q = srom_sweep(h, &d, 1, &o);
+            if (q == SROM_OK && (e = cudaEventRecord(a, h->stream)) != cudaSuccess)
+                q = set_err(h, SROM_ERR_CUDA, "tuning timer: %s", cudaGetErrorString(e));
+            for (int rep = 0; rep < 3 && q == SROM_OK; ++rep) q = srom_sweep(h, &d, 1, &o);
+            if (q == SROM_OK && ((e = cudaEventRecord(b, h->stream)) != cudaSuccess ||
+                                 (e = cudaEventSynchronize(b)) != cudaSuccess ||
+                                 (e = cudaEventElapsedTime(ms, a, b)) != cudaSuccess))
+                q = set_err(h, SROM_ERR_CUDA, "tuning timer: %s", cudaGetErrorString(e));
+            return q;
+        };
+        const srom_sweep_opts o64{SROM_FP64, 5, 0.0, 0};
         for (int c = 0; c < 2 && rc == SROM_OK; ++c) {
             h->tune_fp64[key] = c;
-            srom_sweep_opts o{SROM_FP64, 5, 0.0, 0};
-            rc = srom_sweep(h, &d, 1, &o);  // warm-up
-            if (rc == SROM_OK && (e = cudaEventRecord(a, h->stream)) != cudaSuccess)
-                rc = set_err(h, SROM_ERR_CUDA, "tuning timer: %s", cudaGetErrorString(e));
-            for (int rep = 0; rep < 3 && rc == SROM_OK; ++rep) rc = srom_sweep(h, &d, 1, &o);
-            if (rc == SROM_OK && ((e = cudaEventRecord(b, h->stream)) != cudaSuccess ||
-                                  (e = cudaEventSynchronize(b)) != cudaSuccess ||
-                                  (e = cudaEventElapsedTime(&ent.ms[c], a, b)) != cudaSuccess))
-                rc = set_err(h, SROM_ERR_CUDA, "tuning timer: %s", cudaGetErrorString(e));
+            rc = time_sweep(o64, &ent.ms[c]);
+        }
+        if (rc == SROM_OK) {
+            ent.cls = ent.ms[1] < ent.ms[0] ? 1 : 0;
+            h->tune_fp64[key] = ent.cls;
+        }
+        // the mixed form's routing of such a system: the FP64 shared-memory kernel outright, or
+        // complex-FP32 factors in the mixed global kernel plus refinement (only a choice when the
+        // FP64 choice is the shared-memory kernel)
+        if (rc == SROM_OK && ent.cls == 0 && r <= srom::MIXED_MAX_R) {
+            const srom_sweep_opts om{SROM_MIXED_FP32, 5, 0.0, SROM_FLAG_FALLBACK_FP64};
+            for (int c = 0; c < 2 && rc == SROM_OK; ++c) {
+                h->tune_mixed[key] = c;
+                rc = time_sweep(om, &ent.mms[c]);
+            }
+            if (rc == SROM_OK) {
+                ent.mcls = ent.mms[1] < ent.mms[0] ? 1 : 0;
+                h->tune_mixed[key] = ent.mcls;
+            }
         }
         if (a) cudaEventDestroy(a);
         if (b) cudaEventDestroy(b);
@@ -1337,10 +1385,9 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
         cudaFree(buf);
         if (rc != SROM_OK) {
             h->tune_fp64.erase(key);
+            h->tune_mixed.erase(key);
             return rc;
         }
-        ent.cls = ent.ms[1] < ent.ms[0] ? 1 : 0;
-        h->tune_fp64[key] = ent.cls;
         measured.push_back(ent);
     }
     // 3) rewrite the cache with every entry the handle knows
@@ -1348,6 +1395,7 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
         FILE *fp = fopen(cache_path, "w");
         if (!fp) return set_err(h, SROM_ERR_INVALID, "cannot write %s", cache_path);
         fprintf(fp, "{\n  \"device\": \"%s\",\n  \"entries\": [\n", prop.name);
+        const size_t total = h->tune_fp64.size() + h->tune_mixed.size();
         size_t k = 0;
         for (const auto &kv : h->tune_fp64) {
             const int n = (int)(kv.first >> 16), rr = (int)(kv.first & 0xffff);
@@ -1358,7 +1406,18 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
                     ms1 = m.ms[1];
                 }
             fprintf(fp, "    {\"precision\": \"fp64\", \"n\": %d, \"r\": %d, \"kernel\": \"%s\", \"ms_smem\": %.4f, \"ms_global\": %.4f}%s\n",
-                    n, rr, kv.second == 0 ? "smem" : "global", ms0, ms1, ++k < h->tune_fp64.size() ? "," : "");
+                    n, rr, kv.second == 0 ? "smem" : "global", ms0, ms1, ++k < total ? "," : "");
+        }
+        for (const auto &kv : h->tune_mixed) {
+            const int n = (int)(kv.first >> 16), rr = (int)(kv.first & 0xffff);
+            float ms0 = -1.f, ms1 = -1.f;
+            for (const auto &m : measured)
+                if (m.n == n && m.r == rr && m.mcls >= 0) {
+                    ms0 = m.mms[0];
+                    ms1 = m.mms[1];
+                }
+            fprintf(fp, "    {\"precision\": \"mixed\", \"n\": %d, \"r\": %d, \"kernel\": \"%s\", \"ms_fp64_smem\": %.4f, \"ms_mixed_global\": %.4f}%s\n",
+                    n, rr, kv.second == 0 ? "fp64_smem" : "mixed_global", ms0, ms1, ++k < total ? "," : "");
         }
         fprintf(fp, "  ]\n}\n");
         fclose(fp);

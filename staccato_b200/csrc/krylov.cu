@@ -41,6 +41,7 @@ namespace kry {
 constexpr int NB = 64;   // columns per elimination step (and rows of band headroom)
 constexpr int KT = 256;  // threads per CTA
 constexpr int SLD = NB + 1;
+constexpr double PIVOT_EPS = 1e-13;  // small-pivot threshold relative to ||A||_inf (PARDISO iparm[9] = 13)
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -72,19 +73,21 @@ __device__ __forceinline__ double2 shfl2(double2 v, int src) {
 // value arrays.  Entry (i, j) lands at (pi, pj) = (iperm[i], iperm[j]) when pi >= pj, so every
 // unordered pair is written once.  Value sign * (K - w^2 M + i w D): sign = -1 gives the Krylov
 // process's K~, +1 the full-order dynamic stiffness.  One warp per row.
+// Also the infinity norm of the matrix (largest row sum of |a_ij| over the full pattern) into
+// anorm_bits, as the bits of a non-negative double (their unsigned order is the numeric order).
 __global__ void scatter_band_kernel(int64_t n, const int64_t *__restrict__ rp, const int *__restrict__ ci,
                                     const int64_t *__restrict__ vmap, const double2 *__restrict__ K,
                                     const double2 *__restrict__ M, const double2 *__restrict__ D, double w,
                                     double sign, const int *__restrict__ iperm, double2 *__restrict__ band,
-                                    int64_t ldab) {
+                                    int64_t ldab, unsigned long long *__restrict__ anorm_bits) {
     const int lane = threadIdx.x & 31;
     const double w2 = w * w;
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < n;
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int pi = iperm[i];
+        double rs = 0.0;
         for (int64_t e = rp[i] + lane; e < rp[i + 1]; e += 32) {
             const int pj = iperm[ci[e]];
-            if (pi < pj) continue;
             const int64_t v = vmap[e];
             const double2 k = K[v], m = M[v];
             double re = k.x - w2 * m.x, im = k.y - w2 * m.y;
@@ -93,8 +96,13 @@ __global__ void scatter_band_kernel(int64_t n, const int64_t *__restrict__ rp, c
                 re -= w * d.y;
                 im += w * d.x;
             }
+            rs += hypot(re, im);
+            if (pi < pj) continue;
             band[(int64_t)pj * ldab + (pi - pj + NB)] = make_double2(sign * re, sign * im);
         }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, off);
+        if (lane == 0) atomicMax(anorm_bits, (unsigned long long)__double_as_longlong(rs));
     }
 }
 
@@ -105,11 +113,29 @@ __global__ void scatter_band_kernel(int64_t n, const int64_t *__restrict__ rp, c
 // entries are contiguous across the warp) and every fourth row, so a step needs one barrier.
 // The columns are scaled by 1/d_k once at the end.  The first exactly-zero pivot is recorded
 // 1-based in *info.
+// Small pivots are perturbed as PARDISO does with the reference's setting iparm[9] = 13
+// (KrylovROMSubstructure.cpp:621): a pivot d with |d| < 1e-13 ||A||_inf is replaced by the value
+// of the same phase and modulus 1e-13 ||A||_inf, and counted in *perturbed; *min_ratio_bits
+// keeps the smallest |d| / ||A||_inf (bits of a non-negative double).  An exactly zero pivot
+// is still reported in *info (the matrix is singular, not merely ill-conditioned).
+__device__ __forceinline__ double2 perturb_pivot(double2 d, double tau) {
+    const double a = hypot(d.x, d.y);
+    if (a >= tau) return d;
+    if (a == 0.0) return make_double2(tau, 0.0);
+    const double s = tau / a;
+    return make_double2(d.x * s, d.y * s);
+}
+
 __global__ void __launch_bounds__(KT) ldlt_diag_kernel(double2 *__restrict__ band, int64_t ldab, int64_t j0, int nb,
-                                                       int *__restrict__ info) {
+                                                       int *__restrict__ info,
+                                                       const unsigned long long *__restrict__ anorm_bits,
+                                                       int *__restrict__ perturbed,
+                                                       unsigned long long *__restrict__ min_ratio_bits) {
     extern __shared__ double2 S[];  // S[i * SLD + j], full symmetric block
     constexpr int RS = KT / NB;     // row stride of a thread
     const int t = threadIdx.x;
+    const double anorm = __longlong_as_double((long long)*anorm_bits);
+    const double tau = PIVOT_EPS * anorm;
     for (int e = t; e < nb * nb; e += KT) {
         const int i = e / nb, j = e % nb;
         const int r = max(i, j), c = min(i, j);
@@ -118,8 +144,14 @@ __global__ void __launch_bounds__(KT) ldlt_diag_kernel(double2 *__restrict__ ban
     __syncthreads();
     const int j = t % NB, ir = t / NB;
     for (int k = 0; k < nb; ++k) {
-        const double2 d = S[k * SLD + k];
-        if (t == 0 && d.x == 0.0 && d.y == 0.0) atomicCAS(info, 0, (int)(j0 + k + 1));
+        const double2 d0 = S[k * SLD + k];
+        const double2 d = perturb_pivot(d0, tau);  // the same value in every thread
+        if (t == 0) {
+            if (d0.x == 0.0 && d0.y == 0.0) atomicCAS(info, 0, (int)(j0 + k + 1));
+            const double a = hypot(d0.x, d0.y);
+            if (a < tau) atomicAdd(perturbed, 1);
+            if (anorm > 0.0) atomicMin(min_ratio_bits, (unsigned long long)__double_as_longlong(a / anorm));
+        }
         if (j > k && j < nb) {
             const double2 cj = cmul(S[k * SLD + j], crecip(d));
             for (int i = k + 1 + ((ir - (k + 1)) % RS + RS) % RS; i < nb; i += RS)
@@ -129,10 +161,11 @@ __global__ void __launch_bounds__(KT) ldlt_diag_kernel(double2 *__restrict__ ban
     }
     for (int e = t; e < nb * nb; e += KT) {
         const int i = e % nb, c = e / nb;
+        const double2 dc = perturb_pivot(S[c * SLD + c], tau);  // step c never changes S[c][c]
         if (i > c)
-            band[(j0 + c) * ldab + (i - c + NB)] = cmul(S[i * SLD + c], crecip(S[c * SLD + c]));
+            band[(j0 + c) * ldab + (i - c + NB)] = cmul(S[i * SLD + c], crecip(dc));
         else if (i == c)
-            band[(j0 + c) * ldab + NB] = S[c * SLD + c];
+            band[(j0 + c) * ldab + NB] = dc;
     }
 }
 
@@ -567,6 +600,10 @@ struct BandLDLT {
     double2 *zwork = nullptr;  // split-k partials of the complex GEMMs
     int64_t zwork_elems = 0;
     int sms = 148;
+    // ||A||_inf of the assembled matrix, perturbed-pivot count, smallest |d| / ||A||_inf (device)
+    unsigned long long *d_anorm = nullptr, *d_minr = nullptr;
+    int *d_pert = nullptr;
+    PivotStats *stats = nullptr;  // accumulated over the factorisations of a call (may be null)
 
     // complex GEMM C -= op(A) op(B) (beta = 1) on this factor's stream and workspace
     Zgemm gemm(int opa, int opb, int m, int nn, int k, const double2 *A, int64_t lda, const double2 *Bm, int64_t ldb,
@@ -593,11 +630,14 @@ struct BandLDLT {
 
     int factor(Err &E) {
         const size_t smem = sizeof(double2) * NB * SLD;
+        const unsigned long long inf_bits = 0x7FF0000000000000ull;
         KCU(cudaMemsetAsync(d_info, 0, sizeof(int), st));
+        KCU(cudaMemsetAsync(d_pert, 0, sizeof(int), st));
+        KCU(cudaMemcpyAsync(d_minr, &inf_bits, sizeof inf_bits, cudaMemcpyHostToDevice, st));
         int prev_rows = ldw;
         for (int64_t j0 = 0; j0 < n; j0 += NB) {
             const int nb = (int)std::min<int64_t>(NB, n - j0);
-            ldlt_diag_kernel<<<1, KT, smem, st>>>(band, ldab, j0, nb, d_info);
+            ldlt_diag_kernel<<<1, KT, smem, st>>>(band, ldab, j0, nb, d_info, d_anorm, d_pert, d_minr);
             const int rows = (int)std::min<int64_t>(bw, n - j0 - nb);
             if (rows <= 0) continue;
             const int zero_to = std::max(rows, prev_rows);
@@ -616,9 +656,19 @@ struct BandLDLT {
             KCU(zgemm(z, st));
         }
         KCU(cudaGetLastError());
-        int info = 0;
+        int info = 0, pert = 0;
+        unsigned long long minr = inf_bits;
         KCU(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st));
+        KCU(cudaMemcpyAsync(&pert, d_pert, sizeof(int), cudaMemcpyDeviceToHost, st));
+        KCU(cudaMemcpyAsync(&minr, d_minr, sizeof minr, cudaMemcpyDeviceToHost, st));
         KCU(cudaStreamSynchronize(st));
+        if (stats) {
+            double r;
+            std::memcpy(&r, &minr, sizeof r);
+            stats->factorisations += 1;
+            stats->perturbed += pert;
+            stats->min_pivot_ratio = std::min(stats->min_pivot_ratio, r);
+        }
         if (info != 0)
             return E.set(SROM_ERR_INVALID, "K~ has an exactly zero pivot at (permuted) row " + std::to_string(info) +
                                                ": the shifted matrix is singular");
@@ -798,7 +848,9 @@ struct BandContext {
         // split-k partials: at most (2 SMs' worth + the tiles) 64 x 64 blocks
         F.zwork_elems = (int64_t)(4 * F.sms + 64) * 64 * 64;
         if (!need(B.alloc(&F.zwork, (size_t)F.zwork_elems), "the GEMM workspace") ||
-            !need(B.alloc(&d_nrm, znorm2_work_doubles() + 2), "the norm workspace"))
+            !need(B.alloc(&d_nrm, znorm2_work_doubles() + 2), "the norm workspace") ||
+            !need(B.alloc(&F.d_anorm, 1), "the pivot statistics") || !need(B.alloc(&F.d_minr, 1), "the pivot statistics") ||
+            !need(B.alloc(&F.d_pert, 1), "the pivot statistics"))
             return E.code;
         const size_t smem = sizeof(double2) * NB * SLD;
         KCU(cudaFuncSetAttribute(ldlt_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -817,9 +869,10 @@ struct BandContext {
     // sign * (K - w^2 M + i w D) into the band, then L D L^T
     int assemble_factor(const void *K, const void *M, const void *D, double w, double sign, Err &E) {
         KCU(cudaMemsetAsync(F.band, 0, sizeof(double2) * (size_t)(n + 2 * NB) * F.ldab, st));
+        KCU(cudaMemsetAsync(F.d_anorm, 0, sizeof(unsigned long long), st));
         scatter_band_kernel<<<grid_for(n * 32, KT), KT, 0, st>>>(
             n, d_frp, d_fci, d_fmap, reinterpret_cast<const double2 *>(K), reinterpret_cast<const double2 *>(M),
-            reinterpret_cast<const double2 *>(D), w, sign, d_iperm, F.band, F.ldab);
+            reinterpret_cast<const double2 *>(D), w, sign, d_iperm, F.band, F.ldab, F.d_anorm);
         KCU(cudaGetLastError());
         return F.factor(E);
     }
@@ -848,6 +901,7 @@ int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *
         return E.code;
     }
     if (log) log->bandwidth = X.F.bw;
+    X.F.stats = a.stats;
     cudaStream_t st = a.stream;
     const int64_t n = a.n_rows;
     const int mmax = std::max(a.n_in, 1);
@@ -915,6 +969,7 @@ int fom_sweep(const FomArgs &a, std::string *msg) {
         *msg = E.msg;
         return E.code;
     }
+    X.F.stats = a.stats;
     double2 *work = nullptr;
     cudaError_t e = X.B.alloc(&work, (size_t)a.n_rows * a.r);
     if (e != cudaSuccess) {

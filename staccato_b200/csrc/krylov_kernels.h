@@ -10,6 +10,14 @@
 namespace srom {
 namespace kry {
 
+// Pivots of the band LDL^T factorisations of one call: how many were below 1e-13 ||A||_inf and
+// were perturbed (PARDISO iparm[9] = 13), and the smallest |d| / ||A||_inf seen.
+struct PivotStats {
+    int64_t factorisations = 0;
+    int64_t perturbed = 0;
+    double min_pivot_ratio = 1.0 / 0.0;
+};
+
 struct KrylovArgs {
     cudaStream_t stream;
     int64_t n_rows, nnz;
@@ -26,6 +34,7 @@ struct KrylovArgs {
     void *V;  // device n_rows x max_cols output, leading dimension ldv
     int64_t ldv;
     int max_cols;
+    PivotStats *stats;  // may be null
 };
 
 struct KrylovBlock {
@@ -55,6 +64,7 @@ struct FomArgs {
     int n_freq;
     void *X;  // device: n_freq blocks of n_rows x r (leading dimension ldx, block stride ldx * r)
     int64_t ldx;
+    PivotStats *stats;  // may be null
 };
 
 // (K - w^2 M + i w D) X_f = F for every frequency: band LDL^T per frequency.

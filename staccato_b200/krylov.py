@@ -69,6 +69,14 @@ def fom_sweep(handle: _capi.Handle, csr: DeviceCsr, K, M, D, F, freq_hz: Sequenc
     return X
 
 
+def band_pivot_report(handle: _capi.Handle):
+    """(factorisations, perturbed, min_pivot_ratio) of the band L D L^T factorisations of the
+    handle's last krylov_basis / fom_sweep call (``srom_band_pivot_report``)."""
+    nf, npert, mr = C.c_int64(0), C.c_int64(0), C.c_double(0.0)
+    check(handle.ptr, _capi.lib().srom_band_pivot_report(handle.ptr, C.byref(nf), C.byref(npert), C.byref(mr)))
+    return int(nf.value), int(npert.value), float(mr.value)
+
+
 def band_order(indptr, indices, base: int = 0, upper: bool = False):
     """(perm, bandwidth, band_bytes) of the reverse Cuthill-McKee ordering of a host CSR pattern:
     perm[k] = original row of row k."""

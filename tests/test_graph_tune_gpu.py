@@ -46,13 +46,31 @@ def test_tune_writes_cache_and_keeps_results_exact(handle, tmp_path):
     cache = tmp_path / "tune.json"
     tune(handle, [24, 64, 100], r=1, cache_path=str(cache))
     data = json.loads(cache.read_text())
-    assert data["device"] and {e["n"] for e in data["entries"]} >= {24, 64, 100}
-    assert all(e["kernel"] in ("smem", "global") for e in data["entries"])
+    fp64 = [e for e in data["entries"] if e["precision"] == "fp64"]
+    mixed = [e for e in data["entries"] if e["precision"] == "mixed"]
+    assert data["device"] and {e["n"] for e in fp64} >= {24, 64, 100}
+    assert all(e["kernel"] in ("smem", "global") for e in fp64)
+    # the mixed routing is measured wherever the FP64 choice is the shared-memory kernel
+    smem_n = {e["n"] for e in fp64 if e["kernel"] == "smem"}
+    assert {e["n"] for e in mixed} == smem_n
+    assert all(e["kernel"] in ("fp64_smem", "mixed_global") and e["ms_fp64_smem"] > 0 and e["ms_mixed_global"] > 0
+               for e in mixed)
     rom = W.plain_rom(F=30)
     d = DeviceRom.from_host(rom.K, rom.M, None, rom.rhs, rom.omega)
     sweep(handle, [d])
     torch.cuda.synchronize()
     Xo, _ = O.sweep(rom.K, rom.M, None, 0.0, rom.rhs, rom.omega)
     assert np.array_equal(d.solutions().view(np.uint64), Xo.view(np.uint64))
+    # the mixed form follows the tuned routing and stays within 1e-10 of x_ref (n = 64)
+    dm = DeviceRom.from_host(rom.K, rom.M, None, rom.rhs, rom.omega)
+    sweep(handle, [dm], precision=_capi.SROM_MIXED_FP32, flags=_capi.SROM_FLAG_FALLBACK_FP64)
+    steps = dm.steps.cpu().numpy()
+    routed = {e["n"]: e["kernel"] for e in mixed}.get(64)
+    if routed == "fp64_smem":
+        assert (steps == 0).all()
+    elif routed == "mixed_global":
+        assert (steps != 0).all()
+    xr = O.x_ref(rom.K, rom.M, None, 0.0, rom.rhs, rom.omega)
+    assert O.rel_err(dm.solutions(), xr).max() <= 1e-10
     # a second tune call reads the cache instead of timing again
     tune(handle, [24, 64, 100], r=1, cache_path=str(cache))

@@ -214,3 +214,47 @@ def test_fom_sweep_matches_sparse_direct_solve(handle, problem):
             ref = spla.spsolve(sp.csc_matrix(A), F)
             err = np.linalg.norm(X[i].T - ref) / np.linalg.norm(ref)
             assert err <= 1e-9, (f / f1, upper, Dm is None, err)
+
+
+def test_band_small_pivot_perturbed_like_pardiso(handle):
+    """A pivot below 1e-13 ||A||_inf is replaced by the value of the same phase and modulus
+    1e-13 ||A||_inf (PARDISO with the reference's iparm[9] = 13) and counted; a regular
+    problem perturbs nothing and reports its smallest pivot ratio."""
+    import torch
+
+    from staccato_b200.krylov import band_pivot_report, fom_sweep
+
+    n = 300
+    rng = np.random.default_rng(3)
+    main = 4.0 + rng.uniform(0, 1, n) + 0.1j
+    off = -1.0 + 0.05j * rng.standard_normal(n - 1)
+    A = sp.diags([off, main, off], [-1, 0, 1], format="lil").astype(complex)
+    # DOF 150 decoupled, with a diagonal 1e-20 of the matrix norm
+    A[150, 149] = A[149, 150] = A[150, 151] = A[151, 150] = 0.0
+    A[150, 150] = 1e-20 * (1 + 1j)
+    A = A.tocsr()
+    A.eliminate_zeros()
+    A.sort_indices()
+    anorm = abs(A).sum(axis=1).max()
+    csr = DeviceCsr.from_host(A.indptr, A.indices)
+    Kv = torch.from_numpy(A.data.astype(np.complex128)).cuda()
+    Mv = torch.zeros_like(Kv)
+    F = torch.ones((1, n), dtype=torch.complex128, device="cuda")
+    X = fom_sweep(handle, csr, Kv, Mv, None, F, [10.0, 20.0]).cpu().numpy()
+    nf, npert, ratio = band_pivot_report(handle)
+    assert nf == 2 and npert == 2
+    assert ratio == pytest.approx(abs(1e-20 * (1 + 1j)) / anorm, rel=1e-12)
+    d = 1e-13 * anorm * (1 + 1j) / abs(1 + 1j)
+    assert np.allclose(X[:, 0, 150], 1.0 / d, rtol=1e-12)
+    # the rest of the solution is the exact solve of the coupled part
+    keep = np.r_[0:150, 151:n]
+    ref = spla.spsolve(A[keep][:, keep].tocsc(), np.ones(n - 1))
+    assert np.abs(X[0, 0, keep] - ref).max() <= 1e-12 * np.abs(ref).max()
+    # a regular matrix: no perturbation
+    B = sp.diags([off, main, off], [-1, 0, 1], format="csr").astype(complex)
+    B.sort_indices()
+    csr = DeviceCsr.from_host(B.indptr, B.indices)
+    Kv = torch.from_numpy(B.data.astype(np.complex128)).cuda()
+    fom_sweep(handle, csr, Kv, torch.zeros_like(Kv), None, F, [10.0])
+    nf, npert, ratio = band_pivot_report(handle)
+    assert nf == 1 and npert == 0 and 0.0 < ratio <= 1.0
