@@ -111,9 +111,9 @@ typedef struct {
 typedef struct {
     int precision;   /* SROM_FP64 / SROM_MIXED_FP32 / SROM_MIXED_TC                  */
     int max_refine;  /* refinement steps for the mixed forms (default 5 when <= 0)   */
-    double tol;      /* stop refining when the error estimate c (||d_s||/||d_s-1||) ||d_s||/||x|| <= tol
-                        (2-norms per right-hand side; c = 2, after the first correction c = 4
-                        with d_0 = x); 0 = 2^-34 */
+    double tol;      /* a right-hand side stops refining when its error estimate
+                        c (||d_s||/||d_s-1||) ||d_s||/||x|| <= tol (2-norms; c = 2, after the first
+                        correction c = 4 with d_0 = x); 0 = 2^-34 */
     int flags;       /* SROM_FLAG_*                                                  */
 } srom_sweep_opts;
 

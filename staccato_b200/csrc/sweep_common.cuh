@@ -255,23 +255,29 @@ __device__ void panel_factor_par(T *P, int ldp, int m, int ncols, int *s_perm, i
 // written permuted and rounded to FP32 into B32 (B32[pos[i]] = r[i]) for the next correction.
 // Thread t owns rows t + k*NT; right-hand sides are processed four at a time; the column
 // batches are taken cyclically from batch sweep_start(f).
+// Only the right-hand sides still refined: column act[c] of x and b gives column c of B32
+// (c < ra).
 template <int RPT>
-__device__ void residual64(const RomDev &R, double w, const double2 *X64, float2 *B32, const int *s_pos, int f) {
+__device__ void residual64(const RomDev &R, double w, const double2 *X64, float2 *B32, const int *s_pos, int f,
+                           const int *act, int ra) {
     constexpr int JB = RPT >= 3 ? 1 : 4 / RPT;  // columns of K, M, D loaded per batch
     const int tid = threadIdx.x;
     const int n = R.n;
     const int nbat = (n + JB - 1) / JB, b0 = sweep_start(f, nbat);
     const double s = -__dmul_rn(w, w);
     const uint64_t pol = l2_keep_policy();
-    for (int c0 = 0; c0 < R.r; c0 += 4) {
-        const int nc = min(4, R.r - c0);
+    for (int c0 = 0; c0 < ra; c0 += 4) {
+        const int nc = min(4, ra - c0);
+        int col[4];
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) col[cc] = cc < nc ? act[c0 + cc] : 0;
         double2 acc[RPT][4];
 #pragma unroll
         for (int k = 0; k < RPT; ++k) {
             const int i = tid + k * NT;
 #pragma unroll
             for (int cc = 0; cc < 4; ++cc)
-                acc[k][cc] = (i < n && cc < nc) ? R.rhs[i + (int64_t)(c0 + cc) * R.ldb] : make_double2(0.0, 0.0);
+                acc[k][cc] = (i < n && cc < nc) ? R.rhs[i + (int64_t)col[cc] * R.ldb] : make_double2(0.0, 0.0);
         }
         for (int bt = 0; bt < nbat; ++bt) {
             const int bb = b0 + bt, j0 = (bb < nbat ? bb : bb - nbat) * JB;
@@ -296,7 +302,7 @@ __device__ void residual64(const RomDev &R, double w, const double2 *X64, float2
                 double2 xj[4];
 #pragma unroll
                 for (int cc = 0; cc < 4; ++cc)
-                    xj[cc] = cc < nc ? X64[j + (int64_t)(c0 + cc) * n] : make_double2(0.0, 0.0);
+                    xj[cc] = cc < nc ? X64[j + (int64_t)col[cc] * n] : make_double2(0.0, 0.0);
 #pragma unroll
                 for (int k = 0; k < RPT; ++k) {
                     const int i = tid + k * NT;
@@ -339,13 +345,15 @@ __device__ void residual64(const RomDev &R, double w, const double2 *X64, float2
 // ||d||_2 / ||x||_2 into s_dx; one warp per right-hand side.  The 2-norm is the norm of the
 // accuracy criterion (relative 2-norm error per system): with max norms the estimate missed
 // errors spread over many entries of a solution dominated by a few (near resonance).
-static __device__ void apply_correction(double2 *X, const float2 *B32, int n, int nrhs, double *s_dx) {
+// Column c of B32 (c < ra) corrects column act[c] of X.
+static __device__ void apply_correction(double2 *X, const float2 *B32, int n, const int *act, int ra, double *s_dx) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int c = warp; c < nrhs; c += NW) {
+    for (int c = warp; c < ra; c += NW) {
         double dm = 0.0, xm = 0.0;
+        const int col = act[c];
         for (int i = lane; i < n; i += 32) {
             const float2 d = B32[i + (int64_t)c * n];
-            double2 &x = X[i + (int64_t)c * n];
+            double2 &x = X[i + (int64_t)col * n];
             x.x += (double)d.x;
             x.y += (double)d.y;
             dm = fma((double)d.x, (double)d.x, fma((double)d.y, (double)d.y, dm));
@@ -507,20 +515,35 @@ struct RingSolve {
 
 // Refinement of one system after its complex-FP32 factorisation (A32, ld n, LAPACK layout with
 // rows in the factor's order; info = the factorisation's zero-pivot report): x_0 from the FP32
-// factors, then r = b - A(w) x in FP64 and x += LU \ r (solve(B32, r) replaces the right-hand
-// sides in B32 by the correction) until the predicted error
-// rho * ||d_s|| / ||x||, rho = 2 ||d_s|| / ||d_s-1||, is at most tol for every right-hand side
-// (default 2^-34), at most max_refine corrections.  Non-converged systems are appended to the
-// FP64 fallback list when one is given (write_status = false: that launch writes the results).
+// factors, then r = b - A(w) x in FP64 and x += LU \ r (solve(B32, k) replaces the k right-hand
+// sides in B32 by their corrections).  Each right-hand side stops on its own once its predicted
+// error c rho ||d_s|| / ||x||, rho = ||d_s|| / ||d_s-1|| (c = 2; after the first correction,
+// where d_0 = x, c = 4), is at most tol (default 2^-34): later residuals and solves carry only
+// the columns still refined.  At most max_refine corrections.  Non-converged systems are
+// appended to the FP64 fallback list when one is given (write_status = false: that launch
+// writes the results).
 template <int RPT, class Solve>
 __device__ void mixed_refine(const GlobalArgs &a, const RomDev &R, const Item &wi, double w, const float2 *A32,
                              const MixedWork &W, const Solve &solve, int &info, int &steps, double &berr,
                              bool &write_status) {
+    __shared__ int s_act[RMAX_MIXED];       // right-hand sides still refined
+    __shared__ double s_prev[RMAX_MIXED];   // their previous relative correction size
+    __shared__ double s_be[RMAX_MIXED];     // latest error estimate of every right-hand side
+    __shared__ int s_ra, s_state;           // active count; 1 converged, 2 hopeless
     const int tid = threadIdx.x;
     const int n = R.n;
     for (int l = tid; l < n; l += NT) {
         W.s_pos[W.s_ptot[l]] = l;
         W.s_dinv[l] = CT<float2>::recip(A32[l + (int64_t)l * W.lda]);
+    }
+    if (tid < R.r) {
+        s_act[tid] = tid;
+        s_prev[tid] = 1.0;  // the first correction is x itself
+        s_be[tid] = 0.0;
+    }
+    if (tid == 0) {
+        s_ra = R.r;
+        s_state = 0;
     }
     __syncthreads();
     for (int e = tid; e < n * R.r; e += NT) {
@@ -531,36 +554,44 @@ __device__ void mixed_refine(const GlobalArgs &a, const RomDev &R, const Item &w
     }
     __syncthreads();
     const double tol_x = a.tol > 0.0 ? a.tol : 5.820766091346741e-11;  // 2^-34
-    bool conv = false, hopeless = false;
-    double prev = 1.0;  // relative size of the previous correction (the first is x itself)
     for (int s = 0;; ++s) {
-        if (s > 0) residual64<RPT>(R, w, W.X, W.B32, W.s_pos, wi.f);
-        solve(W.B32, R.r);
-        apply_correction(W.X, W.B32, n, R.r, W.s_dx);
-        if (s > 0) {
-            // error left after this correction ~ rho * ||d||, rho ~ ||d_s|| / ||d_{s-1}||
-            // (the contraction of the iteration), taken twice for safety.  After the first
-            // correction the ratio is ||d_1|| / ||x||, the relative error of the first solve,
-            // a weaker stand-in for the contraction: it is taken four times.
-            double worst = 0.0;
-            for (int c = 0; c < R.r; ++c) worst = fmax(worst, W.s_dx[c]);
-            const double ratio = worst / prev;
-            const double rho = fmin(1.0, (s == 1 ? 4.0 : 2.0) * ratio);
-            berr = worst * rho;
-            conv = berr <= tol_x;
-            prev = worst;
-            // With the FP64 fallback on, stop as soon as even the measured contraction
-            // (no safety factor) cannot reach tol in the steps left: those corrections
-            // would be discarded by the re-solve anyway.
-            if (!conv && a.fb_items && s >= 2 && s < a.max_refine) {
-                double pred = worst * ratio;
-                for (int k = s; k < a.max_refine && pred > tol_x; ++k) pred *= ratio;
-                hopeless = ratio >= 1.0 || pred > tol_x;
+        const int ra = s_ra;
+        if (s > 0) residual64<RPT>(R, w, W.X, W.B32, W.s_pos, wi.f, s_act, ra);
+        solve(W.B32, ra);
+        apply_correction(W.X, W.B32, n, s_act, ra, W.s_dx);
+        if (s > 0 && tid == 0) {
+            // error left after this correction ~ rho ||d||, rho ~ ||d_s|| / ||d_s-1|| (the
+            // contraction), taken twice for safety; after the first correction the ratio is
+            // ||d_1|| / ||x||, the relative error of the first solve, a weaker stand-in for
+            // the contraction: taken four times.  With the FP64 fallback on, a column whose
+            // measured contraction (no safety factor) cannot reach tol in the steps left makes
+            // the system hopeless: its corrections would be discarded by the re-solve anyway.
+            int keep = 0;
+            bool hopeless = false;
+            for (int c = 0; c < ra; ++c) {
+                const int col = s_act[c];
+                const double dx = W.s_dx[c], ratio = dx / s_prev[col];
+                const double be = dx * fmin(1.0, (s == 1 ? 4.0 : 2.0) * ratio);
+                s_be[col] = be;
+                s_prev[col] = dx;
+                if (be <= tol_x) continue;
+                if (a.fb_items && s >= 2 && s < a.max_refine) {
+                    double pred = dx * ratio;
+                    for (int k = s; k < a.max_refine && pred > tol_x; ++k) pred *= ratio;
+                    hopeless = hopeless || ratio >= 1.0 || pred > tol_x;
+                }
+                s_act[keep++] = col;  // keep < = c: compaction in place
             }
+            s_ra = keep;
+            s_state = keep == 0 ? 1 : (hopeless ? 2 : 0);
         }
+        __syncthreads();
         steps = s;
-        if (conv || hopeless || s >= a.max_refine) break;
+        if (s_state != 0 || s >= a.max_refine) break;
     }
+    const bool conv = s_state == 1;
+    berr = 0.0;
+    for (int c = 0; c < R.r; ++c) berr = fmax(berr, s_be[c]);
     if (!conv && a.fb_items) {
         // re-solved by the FP64 kernel that runs after this one; it writes X and status
         if (tid == 0) a.fb_items[atomicAdd(a.fb_count, 1)] = wi;
