@@ -301,51 +301,13 @@ __device__ void drain(const Bars &B, const TcState &S) {
 
 // ---------------------------------------------------------------------------- assembly
 // A(w) = (1 + i eta) K + (-w^2) M + (i w) D rounded to complex FP32 into A (ld lda), with the
-// FP64 arithmetic of assemble_entry.  Thread t converts the column-major entries t, t + NT, ...
-// of each batch of NT * 8, eight at a time, every load of a batch issued before any of them is
-// used; the batches are taken cyclically from batch sweep_start(f).
+// FP64 arithmetic of assemble_entry: the mixed kernel's column sweep (a warp a column, column
+// sweep_start(f) first), in a function of its own so that its registers do not weigh on the
+// factorisation's.  (A batched form, eight entries of NT-strided column-major positions per
+// thread with their loads issued together, measured 1.8x slower at n = 512: two integer
+// divisions an entry and spills.)
 __device__ __noinline__ void assemble_fp32(float2 *A, int lda, const RomDev &R, double w, int f) {
-    constexpr int U = 8;
-    const int n = R.n, total = n * n;
-    const int nbat = (total + NT * U - 1) / (NT * U), b0 = sweep_start(f, nbat);
-    const double s = -__dmul_rn(w, w);
-    const uint64_t pol = l2_keep_policy();
-    for (int bt = 0; bt < nbat; ++bt) {
-        const int bb = b0 + bt, base = (bb < nbat ? bb : bb - nbat) * NT * U + threadIdx.x;
-        double2 kv[U], mv[U], dv[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int idx = base + u * NT;
-            if (idx < total) {
-                const int j = idx / n, i = idx - j * n;
-                const int64_t e = i + (int64_t)j * R.ldk;
-                kv[u] = ld_keep(R.K + e, pol);
-                mv[u] = ld_keep(R.M + e, pol);
-                dv[u] = R.D ? ld_keep(R.D + e, pol) : make_double2(0.0, 0.0);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int idx = base + u * NT;
-            if (idx < total) {
-                double2 k = kv[u];
-                if (R.eta != 0.0) {
-                    const double t1 = __dmul_rn(R.eta, k.y), t2 = __dmul_rn(R.eta, k.x);
-                    k.x = __dsub_rn(k.x, t1);
-                    k.y = __dadd_rn(k.y, t2);
-                }
-                double2 v;
-                v.x = __dadd_rn(k.x, __dmul_rn(s, mv[u].x));
-                v.y = __dadd_rn(k.y, __dmul_rn(s, mv[u].y));
-                if (R.D) {
-                    v.x = __dsub_rn(v.x, __dmul_rn(w, dv[u].y));
-                    v.y = __dadd_rn(v.y, __dmul_rn(w, dv[u].x));
-                }
-                const int j = idx / n, i = idx - j * n;
-                A[i + (int64_t)j * lda] = make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
-            }
-        }
-    }
+    assemble_into<float2>(A, lda, R, w, f);
 }
 
 // ---------------------------------------------------------------------------- phase A helpers
