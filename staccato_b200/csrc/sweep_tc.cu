@@ -40,7 +40,7 @@
 //      the result; producer and epilogue hand over through mbarriers only (schur_tc).
 // The row interchanges of a panel are applied to the columns left of it once, after the last
 // panel (unswap_left), and the correction solves use inverse diagonal blocks built per panel.
-// No cluster, no multicast: every copy reads this GPU's own memory into this CTA.
+// No thread-block clusters: every copy reads this GPU's own memory into this CTA alone.
 //
 // Every mbarrier wait is bounded (about 2 s of device time); a wait that runs out marks the
 // system (info = -2), sets the launch's error word, drains the copies and MMAs this CTA has in

@@ -42,12 +42,13 @@ def _padded(a, ld):
     return torch.from_numpy(buf.ravel()).cuda()
 
 
+# n = 700 (r = 3) runs on the large-order kernel, in the mixed form too (FP64 there)
 @pytest.mark.parametrize("form", [0, 1], ids=["fp64", "mixed"])
-@pytest.mark.parametrize("n", [50, 200])
+@pytest.mark.parametrize("n", [50, 200, 700])
 def test_padded_leading_dimensions(handle, form, n):
     import torch
 
-    r, F, ldk, ldb = 3, 9, n + 5, n + 3
+    r, F, ldk, ldb = 3, (9 if n < 500 else 3), n + 5, n + 3
     K, M, D, rhs, omega = _system(n, n, r, F, with_d=True)
     dK, dM, dD, dB = _padded(K, ldk), _padded(M, ldk), _padded(D, ldk), _padded(rhs, ldb)
     dw = torch.from_numpy(omega).cuda()
@@ -69,7 +70,7 @@ def test_padded_leading_dimensions(handle, form, n):
         assert O.rel_err(Xg, Xr).max() <= 1e-10
 
 
-@pytest.mark.parametrize("n", [20, 150])
+@pytest.mark.parametrize("n", [20, 150, 800])
 def test_nonfinite_entries_follow_the_oracle(handle, n):
     """A NaN at the top of a column is taken as that column's pivot (IZAMAX's first entry);
     an Inf elsewhere spreads through the factors.  info, the positions of NaN and every
