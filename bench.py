@@ -39,9 +39,10 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--precision", choices=["both", "mixed", "mixed_tc", "fp64"], default="both",
-                   help="both: headline = mixed+refine (CUDA-core FP32 LU), plain FP64 and the "
-                        "tensor-core mixed form measured beside it")
+    p.add_argument("--precision", choices=["both", "mixed", "mixed_tc", "mixed_fp32", "fp64"], default="both",
+                   help="both: headline = mixed+refine with each system on the faster mixed kernel "
+                        "(SROM_MIXED_AUTO), plain FP64, and the tensor-core and CUDA-core mixed "
+                        "kernels on every system measured beside it")
     p.add_argument("--cpu-sample-stride", type=int, default=16,
                    help="CPU baseline sweeps every k-th frequency of every ROM")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -384,11 +385,11 @@ def adjoint_leg(torch, dev, h):
 
 
 def workloads_leg(torch, dev, h, reps=3):
-    """All three forms on the single-ROM workloads beside the batching one: plain (n = 64, 500
+    """Every form on the single-ROM workloads beside the batching one: plain (n = 64, 500
     frequencies, r = 1) and precision (n = 256, 4096 frequencies, 60 % within 0.1 % of an
-    eigenfrequency, r = 8, damping D).  Device time per sweep (median of reps), freq-solves/s,
-    and for the mixed form the error against the oracle's refined x_ref on every 16th
-    frequency."""
+    eigenfrequency, r = 8, damping D); mixed = SROM_MIXED_AUTO (untuned for these orders: the
+    CUDA-core kernel below n = 320).  Device time per sweep (median of reps), freq-solves/s, and
+    for the mixed forms the error against the oracle's refined x_ref on every 16th frequency."""
     from oracle import oracle as O
     from staccato_b200 import _capi, workloads as W
     from staccato_b200.sweep import DeviceRom, sweep
@@ -400,7 +401,8 @@ def workloads_leg(torch, dev, h, reps=3):
         res = {"n": rom.n, "F": rom.F, "r": int(rom.rhs.shape[1])}
         for form, prec, flags in (("fp64", _capi.SROM_FP64, 0),
                                   ("mixed_tc", _capi.SROM_MIXED_TC, _capi.SROM_FLAG_FALLBACK_FP64),
-                                  ("mixed", _capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)):
+                                  ("mixed_fp32", _capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64),
+                                  ("mixed", _capi.SROM_MIXED_AUTO, _capi.SROM_FLAG_FALLBACK_FP64)):
             sweep(h, [d], precision=prec, flags=flags)
             ts = []
             for _ in range(reps):
@@ -420,8 +422,8 @@ def workloads_leg(torch, dev, h, reps=3):
                 res[form]["max_rel_err"] = float(err.max())
                 st = d.steps.cpu().numpy()
                 res[form]["refine_steps_hist"] = {str(k): int(v) for k, v in zip(*np.unique(st, return_counts=True))}
-        res["mixed_vs_plain"] = res["mixed"]["freq_solves_per_s"] / res["fp64"]["freq_solves_per_s"]
-        res["mixed_tc_vs_plain"] = res["mixed_tc"]["freq_solves_per_s"] / res["fp64"]["freq_solves_per_s"]
+        for form in ("mixed", "mixed_tc", "mixed_fp32"):
+            res[form + "_vs_plain"] = res[form]["freq_solves_per_s"] / res["fp64"]["freq_solves_per_s"]
         out[name] = res
     return out
 
@@ -451,7 +453,7 @@ def reference_orders_leg(torch, dev, h, reps=2):
         d = DeviceRom.from_host(rom.K, rom.M, rom.D, rom.rhs, rom.omega, device=dev)
         res = {"n": n, "F": F, "r": 1, "reference": REFERENCE_PER_OMEGA_MS[n]}
         for form, prec, flags in (("fp64", _capi.SROM_FP64, 0),
-                                  ("mixed", _capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)):
+                                  ("mixed", _capi.SROM_MIXED_AUTO, _capi.SROM_FLAG_FALLBACK_FP64)):
             sweep(h, [d], precision=prec, flags=flags)
             ts = []
             for _ in range(reps):
@@ -608,9 +610,10 @@ def run_ours(args):
     tune_s = time.time() - t_tune
     FORMS = {"fp64": (_capi.SROM_FP64, 0),
              "mixed_tc": (_capi.SROM_MIXED_TC, _capi.SROM_FLAG_FALLBACK_FP64),
-             "mixed": (_capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64)}
-    forms = {"both": ["fp64", "mixed_tc", "mixed"], "mixed": ["mixed"], "mixed_tc": ["mixed_tc"],
-             "fp64": ["fp64"]}[args.precision]
+             "mixed_fp32": (_capi.SROM_MIXED_FP32, _capi.SROM_FLAG_FALLBACK_FP64),
+             "mixed": (_capi.SROM_MIXED_AUTO, _capi.SROM_FLAG_FALLBACK_FP64)}
+    forms = {"both": ["fp64", "mixed_tc", "mixed_fp32", "mixed"], "mixed": ["mixed"], "mixed_tc": ["mixed_tc"],
+             "mixed_fp32": ["mixed_fp32"], "fp64": ["fp64"]}[args.precision]
     headline = forms[-1]
     x64 = None  # FP64 solutions of every system (device), the comparator of the mixed forms
 
@@ -696,17 +699,17 @@ def run_ours(args):
         tpeak, tsrc = ((float(bf16), "MEASURED_PEAKS.json bf16_tflops_sustained (dense bf16 tensor rate under "
                                      "the power cap)") if bf16 else
                        (1400.0, "fallback: 1.4 PFLOP/s sustained dense bf16 (no MEASURED_PEAKS.json)"))
-        if "mixed" in results:
-            # Headline kernel: the CUDA-core mixed form, against the GPU's compute ceiling (its
-            # tensor cores, sustained dense bf16: the launch lasts over a second); its FP32
-            # arithmetic runs on the CUDA cores, so the fraction of the FP32 rate (cuBLAS SGEMM
-            # measured in this run) is given beside it.
-            p32 = gemm_peak_tflops(torch, dev, torch.float32)
-            rm = roofline("mixed", tpeak, tsrc)
-            rm["peak_fp32_cuda_cores"] = p32
-            rm["frac_of_fp32_cuda_cores"] = rm["achieved"] / p32
-            rm["peak_fp32_cuda_cores_source"] = "cuBLAS SGEMM 8192^3, TF32 off, measured in this run"
-            info["roofline_mixed"] = rm
+        p32 = gemm_peak_tflops(torch, dev, torch.float32) if ("mixed" in results or "mixed_fp32" in results) else None
+        for form in ("mixed", "mixed_fp32"):
+            if form in results:
+                # Against the GPU's compute ceiling (its tensor cores, sustained dense bf16: the
+                # launch lasts over a second); the CUDA-core kernel's FP32 arithmetic is compared
+                # with the FP32 rate (cuBLAS SGEMM measured in this run) as well.
+                rm = roofline(form, tpeak, tsrc)
+                rm["peak_fp32_cuda_cores"] = p32
+                rm["frac_of_fp32_cuda_cores"] = rm["achieved"] / p32
+                rm["peak_fp32_cuda_cores_source"] = "cuBLAS SGEMM 8192^3, TF32 off, measured in this run"
+                info["roofline_" + form] = rm
         if "mixed_tc" in results:
             # Tensor-core form: Schur updates as tcgen05 MMAs; achieved counts algorithmic flops
             # (8/3 n^3 + 8 n^2 r), the tensor pipe executes six bf16 piece products per FP32
@@ -802,17 +805,20 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": "freq-solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ("c64 LU + c128 refinement" if headline == "mixed" else
-                      "c64 LU (tensor-core Schur updates on bf16 piece splits) + c128 refinement"
-                      if headline == "mixed_tc" else "c128"),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": ({"mixed": "c64 LU (Schur updates on the tensor cores, bf16 piece splits, where that kernel is "
+                                "the faster; CUDA-core FP32 elsewhere) + c128 refinement",
+                      "mixed_fp32": "c64 LU + c128 refinement",
+                      "mixed_tc": "c64 LU (tensor-core Schur updates on bf16 piece splits) + c128 refinement"}
+                     .get(headline, "c128")),
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "systems_per_gpu": systems,
                        "tflop_per_step_per_gpu": flops / 1e12, "precision": headline,
-                       "refine": "complex-FP32 LU on CUDA cores (the tensor-core form, Schur updates as tcgen05 MMAs on three-piece bf16 splits, is measured beside it as mixed_tc), FP64 residuals, <=5 corrections, stop when the predicted error rho*||d||/||x|| (2-norms) <= 2^-34 (or early once the measured contraction cannot reach it), correction solves streamed through a shared-memory strip ring, back substitution by reciprocals of diag(U), FP64 fallback; systems the FP64 shared-memory kernel holds are routed by the autotuner (FP64 outright or the mixed kernel)",
+                       "refine": "complex-FP32 LU, each system on the faster of the two mixed kernels for its (n, r) as the autotuner measured (SROM_MIXED_AUTO: the tensor-core kernel, Schur updates as tcgen05 MMAs on three-piece bf16 splits, or the CUDA-core kernel; each measured on every system beside it as mixed_tc and mixed_fp32), FP64 residuals, <=5 corrections, each right-hand side stopping once its predicted error rho*||d||/||x|| (2-norms) <= 2^-34 (or the system early once the measured contraction cannot reach it), correction solves streamed through a shared-memory strip ring, back substitution by reciprocals of diag(U), FP64 fallback; systems the FP64 shared-memory kernel holds are routed by the autotuner (FP64 outright or a mixed kernel)",
                        "l2": "inputs 167 MB + outputs 1.6 GB per step exceed L2; no flush",
                        "autotune": "srom_tune over every (n, r) of the batch before warm-up (%.1f s): FP64 smem/global "
-                                   "kernel and the mixed form's FP64-outright/mixed-kernel routing of the orders the "
-                                   "FP64 smem kernel holds" % tune_s,
+                                   "kernel, the mixed form's FP64-outright/mixed-kernel routing of the orders the "
+                                   "FP64 smem kernel holds, and tensor-core vs CUDA-core mixed kernel for n in "
+                                   "96..512" % tune_s,
                        "parallelism": f"independent batch per GPU x{world} (seed 3 + 1000003*rank)"},
             "roofline": info.get("roofline"),
             "roofline_fp64": info.get("roofline_fp64"),
@@ -821,14 +827,14 @@ def run_ours(args):
             "mixed_vs_plain": (results["mixed"]["value"] / results["fp64"]["value"]
                                if "mixed" in results and "fp64" in results else None),
             "refine_steps_hist": results.get("mixed", {}).get("steps"),
-            "mixed_tc": ({"value": results["mixed_tc"]["value"], "unit": "freq-solves/s",
-                          "ms_per_step": results["mixed_tc"]["ms"],
-                          "vs_plain": (results["mixed_tc"]["value"] / results["fp64"]["value"]
-                                       if "fp64" in results else None),
-                          "refine_steps_hist": results["mixed_tc"]["steps"],
-                          "accuracy_vs_fp64_all_systems": (results["mixed_tc"]["accuracy_all"] or {}).get("summary"),
-                          "roofline": info.get("roofline_mixed_tc")}
-                         if "mixed_tc" in results else None),
+            **{form: ({"value": results[form]["value"], "unit": "freq-solves/s",
+                       "ms_per_step": results[form]["ms"],
+                       "vs_plain": (results[form]["value"] / results["fp64"]["value"]
+                                    if "fp64" in results else None),
+                       "refine_steps_hist": results[form]["steps"],
+                       "accuracy_vs_fp64_all_systems": (results[form]["accuracy_all"] or {}).get("summary"),
+                       "roofline": info.get("roofline_" + form)}
+                      if form in results else None) for form in ("mixed_tc", "mixed_fp32")},
             "cpu_baseline": cpu,
             "accuracy": acc,
             "accuracy_vs_fp64_all_systems": (acc_all or {}).get("summary"),

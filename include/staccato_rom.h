@@ -61,6 +61,9 @@ typedef struct {
                               with every Schur update run on the tensor cores (tcgen05 MMAs on
                               three-piece bf16 splits of the FP32 operands, FP32 accumulation);
                               systems up to n = 512 (larger ones use the SROM_MIXED_FP32 kernel) */
+#define SROM_MIXED_AUTO 3  /* each system on the faster of the two mixed kernels for its order and
+                              right-hand sides: as srom_tune measured, else the tensor-core kernel
+                              from n = 320 to 512 and the CUDA-core kernel elsewhere            */
 
 /* ---- sweep flags ---------------------------------------------------------------------- */
 #define SROM_FLAG_FALLBACK_FP64 1 /* re-solve non-converged frequencies in FP64 (steps = -1);
@@ -109,7 +112,7 @@ typedef struct {
 } srom_rom_desc;
 
 typedef struct {
-    int precision;   /* SROM_FP64 / SROM_MIXED_FP32 / SROM_MIXED_TC                  */
+    int precision;   /* SROM_FP64 / SROM_MIXED_FP32 / SROM_MIXED_TC / SROM_MIXED_AUTO */
     int max_refine;  /* refinement steps for the mixed forms (default 5 when <= 0)   */
     double tol;      /* a right-hand side stops refining when its error estimate
                         c (||d_s||/||d_s-1||) ||d_s||/||x|| <= tol (2-norms; c = 2, after the first

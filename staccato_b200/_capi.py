@@ -22,6 +22,7 @@ SROM_ERR_UNSUPPORTED = 5
 SROM_FP64 = 0
 SROM_MIXED_FP32 = 1
 SROM_MIXED_TC = 2
+SROM_MIXED_AUTO = 3
 
 SROM_FLAG_FALLBACK_FP64 = 1
 SROM_FLAG_KEEP_FACTORS = 2

@@ -69,6 +69,8 @@ struct srom_handle {
     // mixed-form routing chosen by srom_tune per (n << 16 | r) where the FP64 smem kernel is
     // the FP64 choice: 0 solve in FP64 outright, 1 mixed global kernel
     std::map<long long, int> tune_mixed;
+    // SROM_MIXED_AUTO's kernel chosen by srom_tune per (n << 16 | r): 0 CUDA-core, 1 tensor-core
+    std::map<long long, int> tune_tc;
     std::vector<cudaEvent_t> event_pool;
     // error word of the last tensor-core sweep (device, inside d_meta) and its pinned host copy
     int *tc_flag_dev = nullptr;
@@ -355,19 +357,25 @@ namespace {
 
 // A validated, classified and ordered sweep: the host image of the device metadata
 // (descriptors, cost-ordered work lists, fallback list, zeroed counters) plus launch shapes.
+// Storage classes of a plan: 0 FP64 shared-memory kernel, 1 global kernel (FP64, or the
+// CUDA-core mixed kernel), 2 large-order FP64 kernel, 3 tensor-core mixed kernel.
+constexpr int NCLS = 4;
+
 struct SweepPlan {
     bool mixed = false;
-    bool tc = false;  // the mixed systems of class 1 run on the tensor-core kernel
     srom_sweep_opts o{};
     std::vector<char> meta;
-    size_t off_items0 = 0, off_items1 = 0, off_items2 = 0, off_fb = 0, off_ctr = 0;
-    long long n_items[3] = {0, 0, 0};
-    double flops[3] = {0.0, 0.0, 0.0};
+    size_t off_items[NCLS] = {0, 0, 0, 0};
+    size_t off_fb = 0, off_ctr = 0;
+    long long n_items[NCLS] = {0, 0, 0, 0};
+    double flops[NCLS] = {0.0, 0.0, 0.0, 0.0};
     size_t smem_max = 0;
     int g_nmax = 0, g_rmax = 0;    // class 1: the global kernels' largest order and RHS count
     int b_nmax = 0, b_rmax = 0;    // class 2: the large-order FP64 kernel's
-    long long grid0 = 0, grid1 = 0, grid2 = 0;
-    int64_t slot_bytes = 0, slot2_bytes = 0;
+    int t_nmax = 0, t_rmax = 0;    // class 3: the tensor-core kernel's
+    int f_nmax = 0, f_rmax = 0;    // the FP64 re-solve of non-converged mixed systems (classes 1, 3)
+    long long grid0 = 0, grid1 = 0, grid2 = 0, grid3 = 0;
+    int64_t slot_bytes = 0, slot2_bytes = 0, slot3_bytes = 0, slotf_bytes = 0;
     bool need_scratch = false;
     std::vector<srom::BackProj> backproj;  // ROMs whose solutions are projected onto outputs
     // ROMs without a mass matrix.  Their descriptors point M at a zero matrix instead: for any
@@ -415,10 +423,27 @@ int mixed_class(const srom_handle *h, int n, int r, int flags) {
     return srom::fp64_smem_blocks_per_sm(srom::fp64_smem_bytes(n, r)) >= 2 ? 0 : 1;
 }
 
+// SROM_MIXED_AUTO: the tensor-core kernel from this order up (without a measurement).  On the
+// batching shapes it is 2-8 % faster than the CUDA-core kernel from n = 384 on and 8 % slower at
+// n = 256 (r = 8); the factorisation's panel, inverse blocks and per-column work weigh more at
+// smaller orders.
+constexpr int TC_AUTO_MIN_N = 320;
+
+// Whether a mixed system of the global class runs on the tensor-core kernel.
+bool use_tc(const srom_handle *h, int n, int r, int precision) {
+    if (n > srom::TC_MAX_N) return false;
+    if (precision == SROM_MIXED_TC) return true;
+    if (precision != SROM_MIXED_AUTO) return false;
+    auto it = h->tune_tc.find(((long long)n << 16) | r);
+    if (it != h->tune_tc.end()) return it->second != 0;
+    return n >= TC_AUTO_MIN_N;
+}
+
 int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_sweep_opts *opts, SweepPlan &P) {
     if (n_roms < 0 || (n_roms > 0 && !roms)) return set_err(h, SROM_ERR_INVALID, "roms is null");
     srom_sweep_opts o = opts ? *opts : srom_sweep_opts{SROM_FP64, 5, 0.0, 0};
-    if (o.precision != SROM_FP64 && o.precision != SROM_MIXED_FP32 && o.precision != SROM_MIXED_TC)
+    if (o.precision != SROM_FP64 && o.precision != SROM_MIXED_FP32 && o.precision != SROM_MIXED_TC &&
+        o.precision != SROM_MIXED_AUTO)
         return set_err(h, SROM_ERR_UNSUPPORTED, "precision %d not available in this build", o.precision);
     const bool mixed = o.precision != SROM_FP64;
     if (o.max_refine <= 0) o.max_refine = 5;
@@ -465,6 +490,21 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
         if (big < 0 || srom::global_panel_fits(gn, gr, h->max_smem_optin)) break;
         cls[big] = 2;
     }
+    // mixed systems of the global class that the tensor-core kernel takes (SROM_MIXED_TC: every
+    // one it can; SROM_MIXED_AUTO: where it is the faster); if the kernel cannot run their
+    // largest order and RHS count together, they stay on the CUDA-core kernel
+    if (mixed) {
+        int tn = 0, tr = 0;
+        for (int i = 0; i < n_roms; ++i)
+            if (cls[i] == 1 && use_tc(h, roms[i].n, roms[i].r, o.precision)) {
+                cls[i] = 3;
+                tn = std::max(tn, roms[i].n);
+                tr = std::max(tr, roms[i].r);
+            }
+        if (tn > 0 && !srom::tc_supported(tn, tr, h->max_smem_optin, nullptr))
+            for (int i = 0; i < n_roms; ++i)
+                if (cls[i] == 3) cls[i] = 1;
+    }
     for (int i = 0; i < n_roms; ++i) {
         const srom_rom_desc &d = roms[i];
         if (cls[i] < 0) continue;
@@ -473,9 +513,12 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
         } else if (cls[i] == 1) {
             P.g_nmax = std::max(P.g_nmax, d.n);
             P.g_rmax = std::max(P.g_rmax, d.r);
-        } else {
+        } else if (cls[i] == 2) {
             P.b_nmax = std::max(P.b_nmax, d.n);
             P.b_rmax = std::max(P.b_rmax, d.r);
+        } else {
+            P.t_nmax = std::max(P.t_nmax, d.n);
+            P.t_rmax = std::max(P.t_rmax, d.r);
         }
         P.n_items[cls[i]] += d.F;
         P.flops[cls[i]] += lu_flops(d.n, d.r) * d.F;
@@ -487,7 +530,7 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
         return set_err(h, SROM_ERR_UNSUPPORTED,
                        "n=%d with r=%d: the right-hand sides (n*r*16 bytes) exceed shared memory", P.b_nmax,
                        P.b_rmax);
-    if (P.n_items[0] + P.n_items[1] + P.n_items[2] > INT32_MAX)
+    if (P.n_items[0] + P.n_items[1] + P.n_items[2] + P.n_items[3] > INT32_MAX)
         return set_err(h, SROM_ERR_UNSUPPORTED, "too many systems");
     if (P.n_items[0] > 0) {
         const int bps = srom::fp64_smem_blocks_per_sm(P.smem_max);
@@ -497,13 +540,22 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
     if (P.n_items[1] > 0) {
         P.grid1 = std::min<long long>(P.n_items[1], h->sm_count);
         P.slot_bytes = (int64_t)P.g_nmax * P.g_nmax * (int64_t)sizeof(double2);
-        // SROM_MIXED_TC: the tensor-core kernel takes class 1 when its limits allow (n <= 512 and
-        // the refinement's work areas fit); otherwise the CUDA-core FP32 kernel does.
-        P.tc = o.precision == SROM_MIXED_TC && srom::tc_supported(P.g_nmax, P.g_rmax, h->max_smem_optin, nullptr);
-        if (P.tc) P.slot_bytes = std::max<int64_t>(P.slot_bytes, (int64_t)srom::tc_slot_bytes(P.g_nmax));
         P.need_scratch = mixed;
         for (int i = 0; i < n_roms; ++i)
             if (cls[i] == 1 && !roms[i].LU) P.need_scratch = true;
+    }
+    if (P.n_items[3] > 0) {
+        P.grid3 = std::min<long long>(P.n_items[3], h->sm_count);
+        P.slot3_bytes = (int64_t)srom::tc_slot_bytes(P.t_nmax);
+        P.need_scratch = true;
+    }
+    if (mixed && (o.flags & SROM_FLAG_FALLBACK_FP64) && P.n_items[1] + P.n_items[3] > 0) {
+        // the FP64 re-solve covers the systems of both mixed kernels, one CTA per SM
+        P.f_nmax = std::max(P.g_nmax, P.t_nmax);
+        P.f_rmax = std::max(P.g_rmax, P.t_rmax);
+        P.slotf_bytes = srom::global_panel_fits(P.f_nmax, P.f_rmax, h->max_smem_optin)
+                            ? (int64_t)P.f_nmax * P.f_nmax * (int64_t)sizeof(double2)
+                            : srom::big_slot_bytes(P.f_nmax);
     }
     if (P.n_items[2] > 0) {
         // one system per CTA: matrix (or the caller's LU buffer) and the panel in the CTA's slot;
@@ -516,17 +568,17 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
     std::vector<int> order(n_roms);
     for (int i = 0; i < n_roms; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return roms[a].n > roms[b].n; });
-    P.off_items0 = align_up(sizeof(RomDev) * std::max(n_roms, 1), 256);
-    P.off_items1 = P.off_items0 + align_up(sizeof(Item) * (size_t)P.n_items[0] + 1, 256);
-    P.off_items2 = P.off_items1 + align_up(sizeof(Item) * (size_t)P.n_items[1] + 1, 256);
-    P.off_fb = P.off_items2 + align_up(sizeof(Item) * (size_t)P.n_items[2] + 1, 256);
-    P.off_ctr = P.off_fb + (mixed ? align_up(sizeof(Item) * (size_t)P.n_items[1] + 1, 256) : 0);
+    P.off_items[0] = align_up(sizeof(RomDev) * std::max(n_roms, 1), 256);
+    for (int c = 1; c < NCLS; ++c)
+        P.off_items[c] = P.off_items[c - 1] + align_up(sizeof(Item) * (size_t)P.n_items[c - 1] + 1, 256);
+    P.off_fb = P.off_items[NCLS - 1] + align_up(sizeof(Item) * (size_t)P.n_items[NCLS - 1] + 1, 256);
+    P.off_ctr = P.off_fb + (mixed ? align_up(sizeof(Item) * (size_t)(P.n_items[1] + P.n_items[3]) + 1, 256) : 0);
     P.meta.assign(P.off_ctr + 256, 0);
     char *hm = P.meta.data();
     if (n_roms) memcpy(hm, dev.data(), sizeof(RomDev) * n_roms);
-    Item *it0 = reinterpret_cast<Item *>(hm + P.off_items0);
-    Item *its[3] = {it0, reinterpret_cast<Item *>(hm + P.off_items1), reinterpret_cast<Item *>(hm + P.off_items2)};
-    long long k[3] = {0, 0, 0};
+    Item *its[NCLS];
+    for (int c = 0; c < NCLS; ++c) its[c] = reinterpret_cast<Item *>(hm + P.off_items[c]);
+    long long k[NCLS] = {0, 0, 0, 0};
     for (int oi = 0; oi < n_roms; ++oi) {
         const int i = order[oi];
         if (cls[i] < 0) continue;
@@ -535,18 +587,21 @@ int make_plan(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom_
     return SROM_OK;
 }
 
-// Scratch bytes of a plan: classes 1 and 2 run one after the other on one stream and share it.
+// Scratch bytes of a plan: the global, tensor-core, FP64 re-solve and large-order launches run
+// one after the other on one stream and share it.
 size_t plan_scratch_bytes(const SweepPlan &P) {
-    return std::max((size_t)P.slot_bytes * P.grid1, (size_t)P.slot2_bytes * P.grid2);
+    size_t b = std::max<size_t>((size_t)P.slot_bytes * P.grid1, (size_t)P.slot2_bytes * P.grid2);
+    b = std::max<size_t>(b, (size_t)P.slot3_bytes * P.grid3);
+    return std::max<size_t>(b, (size_t)P.slotf_bytes * std::max(P.grid1, P.grid3));
 }
 
-// Counters (smem, global, fallback count, fallback work) live at off_ctr and must be zero
-// when the launches start: the metadata copy zeroes them, or zero_counters does.
+// Counters live at off_ctr and must be zero when the launches start (the metadata copy zeroes
+// them, or zero_counters does): 0 smem kernel, 1 global kernel, 2 fallback count, 3 fallback
+// work, 4 tensor-core error word, 5 large-order kernel, 6 tensor-core kernel.
 int enqueue_plan(srom_handle *h, const SweepPlan &P, char *dm, void *scratch, cudaStream_t st, bool zero_counters,
                  bool profile) {
     const RomDev *d_roms = reinterpret_cast<const RomDev *>(dm);
-    const Item *d_it0 = reinterpret_cast<const Item *>(dm + P.off_items0);
-    const Item *d_it1 = reinterpret_cast<const Item *>(dm + P.off_items1);
+    auto items = [&](int c) { return reinterpret_cast<const Item *>(dm + P.off_items[c]); };
     int *d_ctr = reinterpret_cast<int *>(dm + P.off_ctr);
     if (zero_counters) SROM_CUDA(h, cudaMemsetAsync(d_ctr, 0, 8 * sizeof(int), st));
     const bool prof_prev = h->prof;
@@ -554,55 +609,69 @@ int enqueue_plan(srom_handle *h, const SweepPlan &P, char *dm, void *scratch, cu
     int rc = SROM_OK;
     if (P.n_items[0] > 0) {
         ProfScope ps(h, "fp64_smem", P.n_items[0], P.flops[0], 0.0);
-        cudaError_t e = srom::launch_fp64_smem(d_roms, d_it0, (int)P.n_items[0], d_ctr, P.smem_max, (int)P.grid0, st);
+        cudaError_t e = srom::launch_fp64_smem(d_roms, items(0), (int)P.n_items[0], d_ctr, P.smem_max, (int)P.grid0, st);
         if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "fp64 smem launch: %s", cudaGetErrorString(e));
     }
-    if (rc == SROM_OK && P.n_items[1] > 0) {
+    Item *fb_items = nullptr;
+    int *fb_count = nullptr;
+    if (P.mixed && (P.o.flags & SROM_FLAG_FALLBACK_FP64)) {
+        fb_items = reinterpret_cast<Item *>(dm + P.off_fb);
+        fb_count = d_ctr + 2;
+    }
+    auto mixed_args = [&](int c, int *counter, int64_t slot, int n_max, int r_max) {
         srom::GlobalArgs a{};
         a.roms = d_roms;
-        a.items = d_it1;
-        a.n_items = (int)P.n_items[1];
-        a.counter = d_ctr + 1;
+        a.items = items(c);
+        a.n_items = (int)P.n_items[c];
+        a.counter = counter;
         a.scratch = static_cast<unsigned char *>(scratch);
-        a.slot_bytes = P.slot_bytes;
-        a.n_max = P.g_nmax;
-        a.r_max = P.g_rmax;
+        a.slot_bytes = slot;
+        a.n_max = n_max;
+        a.r_max = r_max;
         a.max_refine = P.o.max_refine;
         a.tol = P.o.tol;
-        if (P.mixed && (P.o.flags & SROM_FLAG_FALLBACK_FP64)) {
-            a.fb_items = reinterpret_cast<Item *>(dm + P.off_fb);
-            a.fb_count = d_ctr + 2;
-        }
-        if (P.tc) {
-            a.err_flag = d_ctr + 4;
-            ProfScope ps(h, "mixed_tc", P.n_items[1], P.flops[1], 0.0);
-            cudaError_t e = srom::launch_tc(a, (int)P.grid1, st);
-            if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "tensor-core launch: %s", cudaGetErrorString(e));
-        } else {
-            ProfScope ps(h, P.mixed ? "mixed_global" : "fp64_global", P.n_items[1], P.flops[1], 0.0);
-            cudaError_t e = srom::launch_global(P.mixed, a, (int)P.grid1, st);
-            if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "global launch: %s", cudaGetErrorString(e));
-        }
-        if (rc == SROM_OK && a.fb_items) {
-            // FP64 re-solve of the systems the mixed kernel could not refine; the item count
-            // stays on the device, so the launch needs no host synchronisation.
-            srom::GlobalArgs b = a;
-            b.items = a.fb_items;
-            b.n_items_dev = a.fb_count;
-            b.counter = d_ctr + 3;
-            b.fb_items = nullptr;
-            b.fb_count = nullptr;
-            b.err_flag = nullptr;
-            b.steps_value = -1;
-            ProfScope ps(h, "fp64_fallback", 0, 0.0, 0.0);
-            cudaError_t e = srom::launch_global(false, b, (int)P.grid1, st);
-            if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "fallback launch: %s", cudaGetErrorString(e));
-        }
+        a.fb_items = fb_items;
+        a.fb_count = fb_count;
+        return a;
+    };
+    if (rc == SROM_OK && P.n_items[1] > 0) {
+        srom::GlobalArgs a = mixed_args(1, d_ctr + 1, P.slot_bytes, P.g_nmax, P.g_rmax);
+        if (!P.mixed) a.fb_items = nullptr, a.fb_count = nullptr;
+        ProfScope ps(h, P.mixed ? "mixed_global" : "fp64_global", P.n_items[1], P.flops[1], 0.0);
+        cudaError_t e = srom::launch_global(P.mixed, a, (int)P.grid1, st);
+        if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "global launch: %s", cudaGetErrorString(e));
+    }
+    if (rc == SROM_OK && P.n_items[3] > 0) {
+        srom::GlobalArgs a = mixed_args(3, d_ctr + 6, P.slot3_bytes, P.t_nmax, P.t_rmax);
+        a.err_flag = d_ctr + 4;
+        ProfScope ps(h, "mixed_tc", P.n_items[3], P.flops[3], 0.0);
+        cudaError_t e = srom::launch_tc(a, (int)P.grid3, st);
+        if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "tensor-core launch: %s", cudaGetErrorString(e));
+    }
+    if (rc == SROM_OK && fb_items && P.n_items[1] + P.n_items[3] > 0) {
+        // FP64 re-solve of the systems the mixed kernels could not refine; the item count stays
+        // on the device, so the launch needs no host synchronisation
+        srom::GlobalArgs b{};
+        b.roms = d_roms;
+        b.items = fb_items;
+        b.n_items_dev = fb_count;
+        b.counter = d_ctr + 3;
+        b.scratch = static_cast<unsigned char *>(scratch);
+        b.slot_bytes = P.slotf_bytes;
+        b.n_max = P.f_nmax;
+        b.r_max = P.f_rmax;
+        b.steps_value = -1;
+        const int grid = (int)std::max(P.grid1, P.grid3);
+        ProfScope ps(h, "fp64_fallback", 0, 0.0, 0.0);
+        cudaError_t e = srom::global_panel_fits(P.f_nmax, P.f_rmax, h->max_smem_optin)
+                            ? srom::launch_global(false, b, grid, st)
+                            : srom::launch_global_big(b, grid, st);
+        if (e != cudaSuccess) rc = set_err(h, SROM_ERR_CUDA, "fallback launch: %s", cudaGetErrorString(e));
     }
     if (rc == SROM_OK && P.n_items[2] > 0) {
         srom::GlobalArgs a{};
         a.roms = d_roms;
-        a.items = reinterpret_cast<const Item *>(dm + P.off_items2);
+        a.items = items(2);
         a.n_items = (int)P.n_items[2];
         a.counter = d_ctr + 5;
         a.scratch = static_cast<unsigned char *>(scratch);
@@ -668,7 +737,7 @@ int srom_sweep(srom_handle *h, const srom_rom_desc *roms, int n_roms, const srom
     SROM_CUDA(h, cudaMemcpyAsync(h->d_meta, h->h_meta, P.meta.size(), cudaMemcpyHostToDevice, h->stream));
     SROM_CUDA(h, cudaEventRecord(h->meta_done, h->stream));
     h->meta_pending = true;
-    h->tc_flag_dev = P.tc ? reinterpret_cast<int *>(static_cast<char *>(h->d_meta) + P.off_ctr) + 4 : nullptr;
+    h->tc_flag_dev = P.n_items[3] > 0 ? reinterpret_cast<int *>(static_cast<char *>(h->d_meta) + P.off_ctr) + 4 : nullptr;
     return enqueue_plan(h, P, static_cast<char *>(h->d_meta), scr, h->stream, false, true);
 }
 
@@ -1281,6 +1350,9 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
                 if (same_dev && sscanf(line, " {\"precision\": \"mixed\", \"n\": %d, \"r\": %d, \"kernel\": \"%31[^\"]\"",
                                        &n, &rr, kern) == 3)
                     h->tune_mixed[((long long)n << 16) | rr] = strcmp(kern, "fp64_smem") == 0 ? 0 : 1;
+                if (same_dev && sscanf(line, " {\"precision\": \"auto\", \"n\": %d, \"r\": %d, \"kernel\": \"%31[^\"]\"",
+                                       &n, &rr, kern) == 3)
+                    h->tune_tc[((long long)n << 16) | rr] = strcmp(kern, "tensor_core") == 0 ? 1 : 0;
             }
             fclose(fp);
         }
@@ -1291,14 +1363,21 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
         float ms[2];
         int mcls;      // mixed routing (-1: not measured)
         float mms[2];  // mixed sweep: FP64 outright, mixed global kernel
+        int tcls;      // SROM_MIXED_AUTO's kernel (-1: not measured)
+        float tms[2];  // mixed sweep on every system: CUDA-core kernel, tensor-core kernel
     };
     std::vector<Entry> measured;
     for (int q = 0; q < count; ++q) {
         const int n = n_values[q];
         if (n <= 0) continue;
         const long long key = ((long long)n << 16) | r;
-        if (h->tune_fp64.count(key)) continue;
-        if (srom::fp64_smem_bytes(n, r) > (size_t)h->max_smem_optin) continue;  // only the global kernel fits
+        // FP64: only a choice where the shared-memory kernel fits; the mixed kernels: orders
+        // from 96 up to the tensor-core kernel's limit
+        const bool need_fp64 = !h->tune_fp64.count(key) && srom::fp64_smem_bytes(n, r) <= (size_t)h->max_smem_optin;
+        const bool need_tc = !h->tune_tc.count(key) && n >= 96 && n <= srom::TC_MAX_N && r <= srom::MIXED_MAX_R &&
+                             srom::tc_supported(n, r, h->max_smem_optin, nullptr) &&
+                             srom::global_panel_fits(n, r, h->max_smem_optin);
+        if (!need_fp64 && !need_tc) continue;
         const int F = 2 * h->sm_count;
         std::vector<srom_complex> K((size_t)n * n), M((size_t)n * n), B((size_t)n * r);
         std::vector<double> om(F);
@@ -1340,7 +1419,7 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
         for (int k = 0; k < 4 && rc == SROM_OK; ++k)
             if ((e = cudaMemcpy(dst[k], src[k], bytes[k], cudaMemcpyHostToDevice)) != cudaSuccess)
                 rc = set_err(h, SROM_ERR_CUDA, "tuning input copy: %s", cudaGetErrorString(e));
-        Entry ent{n, r, 0, {0.f, 0.f}, -1, {0.f, 0.f}};
+        Entry ent{n, r, -1, {0.f, 0.f}, -1, {0.f, 0.f}, -1, {0.f, 0.f}};
         cudaEvent_t a = nullptr, b = nullptr;
         if (rc == SROM_OK && ((e = cudaEventCreate(&a)) != cudaSuccess || (e = cudaEventCreate(&b)) != cudaSuccess))
             rc = set_err(h, SROM_ERR_CUDA, "tuning events: %s", cudaGetErrorString(e));
@@ -1357,18 +1436,29 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
             return q;
         };
         const srom_sweep_opts o64{SROM_FP64, 5, 0.0, 0};
-        for (int c = 0; c < 2 && rc == SROM_OK; ++c) {
+        for (int c = 0; c < 2 && rc == SROM_OK && need_fp64; ++c) {
             h->tune_fp64[key] = c;
             rc = time_sweep(o64, &ent.ms[c]);
         }
-        if (rc == SROM_OK) {
+        if (rc == SROM_OK && need_fp64) {
             ent.cls = ent.ms[1] < ent.ms[0] ? 1 : 0;
             h->tune_fp64[key] = ent.cls;
+        }
+        // SROM_MIXED_AUTO's kernel: every system on the CUDA-core, then on the tensor-core kernel
+        if (rc == SROM_OK && need_tc) {
+            const int fl = SROM_FLAG_FALLBACK_FP64 | SROM_FLAG_MIXED_EVERY;
+            const srom_sweep_opts occ{SROM_MIXED_FP32, 5, 0.0, fl}, otc{SROM_MIXED_TC, 5, 0.0, fl};
+            rc = time_sweep(occ, &ent.tms[0]);
+            if (rc == SROM_OK) rc = time_sweep(otc, &ent.tms[1]);
+            if (rc == SROM_OK) {
+                ent.tcls = ent.tms[1] < ent.tms[0] ? 1 : 0;
+                h->tune_tc[key] = ent.tcls;
+            }
         }
         // the mixed form's routing of such a system: the FP64 shared-memory kernel outright, or
         // complex-FP32 factors in the mixed global kernel plus refinement (only a choice when the
         // FP64 choice is the shared-memory kernel)
-        if (rc == SROM_OK && ent.cls == 0 && r <= srom::MIXED_MAX_R) {
+        if (rc == SROM_OK && need_fp64 && ent.cls == 0 && r <= srom::MIXED_MAX_R) {
             const srom_sweep_opts om{SROM_MIXED_FP32, 5, 0.0, SROM_FLAG_FALLBACK_FP64};
             for (int c = 0; c < 2 && rc == SROM_OK; ++c) {
                 h->tune_mixed[key] = c;
@@ -1384,8 +1474,11 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
         cudaStreamSynchronize(h->stream);
         cudaFree(buf);
         if (rc != SROM_OK) {
-            h->tune_fp64.erase(key);
-            h->tune_mixed.erase(key);
+            if (need_fp64) {
+                h->tune_fp64.erase(key);
+                h->tune_mixed.erase(key);
+            }
+            if (need_tc) h->tune_tc.erase(key);
             return rc;
         }
         measured.push_back(ent);
@@ -1395,13 +1488,13 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
         FILE *fp = fopen(cache_path, "w");
         if (!fp) return set_err(h, SROM_ERR_INVALID, "cannot write %s", cache_path);
         fprintf(fp, "{\n  \"device\": \"%s\",\n  \"entries\": [\n", prop.name);
-        const size_t total = h->tune_fp64.size() + h->tune_mixed.size();
+        const size_t total = h->tune_fp64.size() + h->tune_mixed.size() + h->tune_tc.size();
         size_t k = 0;
         for (const auto &kv : h->tune_fp64) {
             const int n = (int)(kv.first >> 16), rr = (int)(kv.first & 0xffff);
             float ms0 = -1.f, ms1 = -1.f;
             for (const auto &m : measured)
-                if (m.n == n && m.r == rr) {
+                if (m.n == n && m.r == rr && m.cls >= 0) {
                     ms0 = m.ms[0];
                     ms1 = m.ms[1];
                 }
@@ -1418,6 +1511,17 @@ int srom_tune(srom_handle *h, const int *n_values, int count, int r, const char 
                 }
             fprintf(fp, "    {\"precision\": \"mixed\", \"n\": %d, \"r\": %d, \"kernel\": \"%s\", \"ms_fp64_smem\": %.4f, \"ms_mixed_global\": %.4f}%s\n",
                     n, rr, kv.second == 0 ? "fp64_smem" : "mixed_global", ms0, ms1, ++k < total ? "," : "");
+        }
+        for (const auto &kv : h->tune_tc) {
+            const int n = (int)(kv.first >> 16), rr = (int)(kv.first & 0xffff);
+            float ms0 = -1.f, ms1 = -1.f;
+            for (const auto &m : measured)
+                if (m.n == n && m.r == rr && m.tcls >= 0) {
+                    ms0 = m.tms[0];
+                    ms1 = m.tms[1];
+                }
+            fprintf(fp, "    {\"precision\": \"auto\", \"n\": %d, \"r\": %d, \"kernel\": \"%s\", \"ms_cuda_core\": %.4f, \"ms_tensor_core\": %.4f}%s\n",
+                    n, rr, kv.second ? "tensor_core" : "cuda_core", ms0, ms1, ++k < total ? "," : "");
         }
         fprintf(fp, "  ]\n}\n");
         fclose(fp);

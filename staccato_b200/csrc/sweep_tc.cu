@@ -755,7 +755,7 @@ __device__ __forceinline__ bool df_wait(const int *flag, int target) {
 }
 
 template <int RC>
-__device__ __noinline__ void solve_df(const float2 *A, int n, int lda, float2 *B, int nrhs, const float2 *ginv,
+__device__ __forceinline__ void solve_df(const float2 *A, int n, int lda, float2 *B, int nrhs, const float2 *ginv,
                                       float2 *stage, int ns, int *s_flag, int phase, int *s_abort, int *err_flag) {
     using C = CT<float2>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -891,7 +891,7 @@ struct TcSolve {
 // (LAPACK layout, rows in final order, s_ptot the composite permutation, s_ipiv the pivots,
 // PL.info the first zero pivot), with the Schur updates on the tensor cores.
 template <int RPT>
-__device__ __noinline__ void factor_tc(float2 *A, int n, int lda, int ldp, unsigned char *sm, const TcSmem &L,
+__device__ __forceinline__ void factor_tc(float2 *A, int n, int lda, int ldp, unsigned char *sm, const TcSmem &L,
                                        unsigned char *abuf, unsigned char *bbuf, float2 *ginv, int *moves, PanelLists &PL,
                                        PivotXchg<float> &X, int *s_pivlg, uint32_t tmem, const Bars &B, TcState &S,
                                        int *s_abort, int *err_flag) {

@@ -105,7 +105,7 @@ def test_all_three_fp64_kernels_in_one_call(handle):
         _assert_bitexact(d.solutions(), xo, f"n={s[0]}")
 
 
-@pytest.mark.parametrize("precision", [_capi.SROM_MIXED_FP32, _capi.SROM_MIXED_TC])
+@pytest.mark.parametrize("precision", [_capi.SROM_MIXED_FP32, _capi.SROM_MIXED_TC, _capi.SROM_MIXED_AUTO])
 def test_mixed_precisions_solve_large_orders_in_fp64(handle, precision):
     n = 1024
     K, M, D, rhs, omega = _rand_rom(11, n, 2, 2)

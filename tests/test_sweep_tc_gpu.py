@@ -138,3 +138,79 @@ def test_tc_larger_orders_use_the_fp32_kernel(handle):
     assert "mixed_global" in names and "mixed_tc" not in names
     xr = O.x_ref(rom.K, rom.M, rom.D, 0.0, rom.rhs, rom.omega)
     assert O.rel_err(d.solutions(), xr).max() <= 1e-10
+
+
+def _kernels(h, fn):
+    h.profile(True)
+    h.read_profile()
+    fn()
+    recs, _ = h.read_profile()
+    h.profile(False)
+    return [rec[0] for rec in recs]
+
+
+def test_auto_routes_each_system_to_its_kernel():
+    """SROM_MIXED_AUTO without measurements: the tensor-core kernel from n = 320 up, the
+    CUDA-core kernel below, both in one call; every system within 1e-10 of x_ref."""
+    from staccato_b200 import _capi as CA
+
+    h = CA.Handle(0)
+    try:
+        roms = [_random_rom(200, 2, 41, F=4), _random_rom(400, 3, 42, F=3), _random_rom(130, 1, 43, F=5)]
+        devs = [DeviceRom.from_host(r.K, r.M, r.D, r.rhs, r.omega) for r in roms]
+        names = _kernels(h, lambda: sweep(h, devs, precision=CA.SROM_MIXED_AUTO, flags=FALLBACK))
+        assert "mixed_tc" in names and "mixed_global" in names, names
+        for r, d in zip(roms, devs):
+            xr = O.x_ref(r.K, r.M, r.D, 0.0, r.rhs, r.omega)
+            assert O.rel_err(d.solutions(), xr).max() <= 1e-10
+            assert (d.steps.cpu().numpy() >= 1).all()
+    finally:
+        h.close()
+
+
+def test_auto_shared_fallback_is_the_fp64_solve():
+    """With a tolerance no correction can meet, every system of both mixed kernels goes to the
+    shared FP64 re-solve list: the results are the FP64 form's, bit for bit, steps = -1."""
+    from staccato_b200 import _capi as CA
+
+    h = CA.Handle(0)
+    try:
+        roms = [_random_rom(150, 2, 51, F=3), _random_rom(420, 2, 52, F=2)]
+        devs = [DeviceRom.from_host(r.K, r.M, r.D, r.rhs, r.omega) for r in roms]
+        names = _kernels(h, lambda: sweep(h, devs, precision=CA.SROM_MIXED_AUTO, max_refine=1, tol=1e-300,
+                                          flags=FALLBACK))
+        assert {"mixed_tc", "mixed_global", "fp64_fallback"} <= set(names), names
+        for r, d in zip(roms, devs):
+            Xo, _ = O.sweep(r.K, r.M, r.D, 0.0, r.rhs, r.omega)
+            assert np.array_equal(np.ascontiguousarray(d.solutions()).view(np.uint64),
+                                  np.ascontiguousarray(Xo).view(np.uint64))
+            assert (d.steps.cpu().numpy() == -1).all()
+    finally:
+        h.close()
+
+
+def test_auto_follows_the_tuner(tmp_path):
+    """srom_tune records the faster mixed kernel per (n, r) (JSON entries of precision "auto")
+    and SROM_MIXED_AUTO uses that choice."""
+    import json
+
+    from staccato_b200 import _capi as CA
+    from staccato_b200.sweep import tune
+
+    h = CA.Handle(0)
+    try:
+        cache = tmp_path / "tune.json"
+        tune(h, [128, 448], r=2, cache_path=str(cache))
+        auto = {e["n"]: e for e in json.loads(cache.read_text())["entries"] if e["precision"] == "auto"}
+        assert set(auto) == {128, 448}
+        for n, e in auto.items():
+            assert e["kernel"] in ("tensor_core", "cuda_core") and e["ms_cuda_core"] > 0 and e["ms_tensor_core"] > 0
+            assert (e["kernel"] == "tensor_core") == (e["ms_tensor_core"] < e["ms_cuda_core"])
+            rom = _random_rom(n, 2, 60 + n, F=3)
+            d = DeviceRom.from_host(rom.K, rom.M, rom.D, rom.rhs, rom.omega)
+            names = _kernels(h, lambda: sweep(h, [d], precision=CA.SROM_MIXED_AUTO, flags=FALLBACK))
+            assert ("mixed_tc" in names) == (e["kernel"] == "tensor_core"), (n, names)
+            xr = O.x_ref(rom.K, rom.M, rom.D, 0.0, rom.rhs, rom.omega)
+            assert O.rel_err(d.solutions(), xr).max() <= 1e-10
+    finally:
+        h.close()
