@@ -318,7 +318,7 @@ __device__ __noinline__ void assemble_fp32(float2 *A, int lda, const RomDev &R, 
 // L or U and the pivot's reciprocal of each step shared by the four columns.  L11^-1 goes to
 // shared memory (phase B) and both to the CTA's global inverse buffer (the correction solves),
 // 32 x 32 column-major with zeros outside bs x bs.
-__device__ void build_inverses(const float2 *P, int ldp, const int *s_perm, int bs, float2 *s_linv,
+__device__ __forceinline__ void build_inverses(const float2 *P, int ldp, const int *s_perm, int bs, float2 *s_linv,
                                float2 *ginv) {
     using C = CT<float2>;
     constexpr int Q = NB / NW;  // columns per warp
@@ -373,7 +373,7 @@ __device__ void build_inverses(const float2 *P, int ldp, const int *s_perm, int 
 // bf16 pieces per tile.  Rows past the last (to the tile's 128) are zero.  One thread per
 // (8-row group, 8-deep chunk pair): two 16-byte stores per piece, consecutive threads on
 // consecutive 16-byte rows of a core matrix.
-__device__ void build_abuf(const float2 *P, int ldp, const int *s_perm, int mt, unsigned char *abuf) {
+__device__ __forceinline__ void build_abuf(const float2 *P, int ldp, const int *s_perm, int mt, unsigned char *abuf) {
     const int nrt = (mt + TM - 1) / TM;
     const int total = nrt * (TM / 8) * 32;
     for (int e = threadIdx.x; e < total; e += NT) {
@@ -432,7 +432,7 @@ __device__ void build_abuf(const float2 *P, int ldp, const int *s_perm, int mt, 
 // q, else q; after panel k = p+1 is folded in, block column p's rows f >= 32 (p + 1) are
 // gathered from rows idx[f], eight columns at a time (all reads, a barrier, all writes).
 // moves: the panels' records (count, dst[], src[] relative to the panel's first row).
-__device__ void unswap_left(float2 *A, int n, int lda, const int *moves, int *idx, int *map) {
+__device__ __forceinline__ void unswap_left(float2 *A, int n, int lda, const int *moves, int *idx, int *map) {
     constexpr int CG = 8;
     constexpr int MAXR = (512 + NT - 1) / NT;  // rows per thread (TC_MAX_N)
     const int tid = threadIdx.x;
@@ -485,7 +485,7 @@ __device__ void unswap_left(float2 *A, int n, int lda, const int *moves, int *id
 // U12 = L11^-1 x written to the matrix, and the column's 4M entries (Ur, Ui; -Ui, Ur) as three
 // bf16 pieces into the B-operand tiles.  After this phase rows j0+32.. of the trailing matrix
 // are in the factor's (logical) order.
-__device__ void trailing_rows(float2 *A, int n, int lda, int j0, const int *s_perm, const int *s_mdst,
+__device__ __forceinline__ void trailing_rows(float2 *A, int n, int lda, int j0, const int *s_perm, const int *s_mdst,
                               const int *s_msrc, int nmoved, const float2 *s_linv, unsigned char *bbuf) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int c0 = j0 + NB;
@@ -596,7 +596,7 @@ __device__ void load_c_rows(const float2 *A, int n, int lda, int r0q, int c0, ui
 //                 C rows, subtract the accumulator from the old values and store the results to the
 //                 matrix, arrive on bar_free, and then load their rows of tile g + 2 into the buffer;
 //   warps 1..3    wait at the closing barrier.
-__device__ void schur_tc(float2 *A, int n, int lda, int j0, unsigned char *op, const unsigned char *abuf,
+__device__ __forceinline__ void schur_tc(float2 *A, int n, int lda, int j0, unsigned char *op, const unsigned char *abuf,
                          const unsigned char *bbuf, uint32_t tmem, const Bars &B, TcState &S, int *s_abort,
                          int *err_flag) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
