@@ -741,7 +741,11 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
         gms = g0.elapsed_time(g1) / args.steps
         gph.close()
-        graph = {"value": systems / (gms * 1e-3), "unit": "freq-solves/s", "ms_per_step": gms,
+        if pg is not None:  # every rank replays its own graph; the step is the slowest rank's
+            t = torch.tensor([gms], dtype=torch.float64, device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            gms = float(t.item())
+        graph = {"value": systems * world / (gms * 1e-3), "unit": "freq-solves/s", "ms_per_step": gms,
                  "api": "srom_graph_launch of the captured sweep (plan and metadata built once)"}
 
     # the oracle's x_ref on the systems farthest from the FP64 solution (and one per ROM)
