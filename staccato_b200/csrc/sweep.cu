@@ -45,7 +45,7 @@ namespace srom {
 // ====================================================================================
 // smem class (FP64)
 // ====================================================================================
-__device__ void panel_factor_smem(double2 *P, int ldp, int m, int ncols, int *ipiv, int *s_info,
+__device__ __forceinline__ void panel_factor_smem(double2 *P, int ldp, int m, int ncols, int *ipiv, int *s_info,
                                   double2 *Bs, int ldbs, int nrhs, int *s_bc) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int jj = 0; jj < ncols; ++jj) {
