@@ -36,8 +36,9 @@
 //      completion; the A tile once per row tile, the B tiles through a 3-deep ring), one thread
 //      issues a tile's 24 MMAs into one of two TMEM accumulators, and while the tensor cores
 //      work on tile t four epilogue warps take tile t-1's accumulator (tcgen05.ld), subtract it
-//      from the tile's old values (bulk-copied into shared memory two tiles ahead) and store
-//      the result; producer and epilogue hand over through mbarriers only (schur_tc).
+//      from the tile's old values (copied into shared memory two tiles ahead, each lane its own
+//      row, by cp.async) and store the result; producer and epilogue hand over through mbarriers
+//      only (schur_tc).
 // The row interchanges of a panel are applied to the columns left of it once, after the last
 // panel (unswap_left), and the correction solves use inverse diagonal blocks built per panel.
 // No thread-block clusters: every copy reads this GPU's own memory into this CTA alone.
@@ -74,7 +75,7 @@ constexpr int OP_B = A_TILE;                        // B ring offset in the oper
 constexpr int OP_C = OP_B + STAGES * B_TILE;        // C tiles (two) offset
 constexpr int OP_BYTES = OP_C + 2 * C_TILE;         // A tile + B ring + two C tiles
 constexpr int TMEM_COLS = 2 * TN;                   // two accumulator buffers
-constexpr int NBARS = 6 + STAGES + 8;               // mbarriers of the pipeline (see Bars)
+constexpr int NBARS = 6 + STAGES;                   // mbarriers of the pipeline (see Bars)
 constexpr int EPI_WARP0 = 4;                        // warps 4..7 run the Schur epilogue
 constexpr int LDL = 33;                             // leading dimension of L11^-1 in smem
 constexpr int CPW = 4;                              // trailing columns per warp pass (phase B)
@@ -255,16 +256,14 @@ __device__ __forceinline__ float2 cfma(float2 u, float2 a, float2 b) {
 // ---------------------------------------------------------------------------- pipeline state
 // Barrier words: bar_a (A tile), bar_full[s] (ring slot s), bar_mma[b] (accumulator b holds a
 // finished tile), bar_free[b] (the four epilogue warps are done with accumulator b and C buffer
-// b), bar_c[b][q] (epilogue warp q's rows of C buffer b have landed), bar_panel (the panel's
-// columns have landed in shared memory).
+// b), bar_panel (the panel's columns have landed in shared memory).
 struct Bars {
     uint32_t base;
     __device__ uint32_t a() const { return base; }
     __device__ uint32_t full(int s) const { return base + 8u * (uint32_t)(1 + s); }
     __device__ uint32_t mma(int b) const { return base + 8u * (uint32_t)(1 + STAGES + b); }
     __device__ uint32_t free(int b) const { return base + 8u * (uint32_t)(3 + STAGES + b); }
-    __device__ uint32_t c(int b, int q) const { return base + 8u * (uint32_t)(5 + STAGES + 4 * b + q); }
-    __device__ uint32_t panel() const { return base + 8u * (uint32_t)(13 + STAGES); }
+    __device__ uint32_t panel() const { return base + 8u * (uint32_t)(5 + STAGES); }
 };
 
 // Counters that give every barrier wait its parity.  Tiles are numbered over the CTA's life
@@ -571,20 +570,16 @@ __device__ __forceinline__ void trailing_rows(float2 *A, int n, int lda, int j0,
 }
 
 // ---------------------------------------------------------------------------- phase C
-// Rows r0q .. r0q + 31 (one epilogue warp's quarter of a tile) of complex columns c0 .. c0 + 31
-// into the warp's quarter of a C buffer (column-major, 128 rows): one bulk copy per column,
-// issued by the warp's lanes and counted on the warp's barrier.  A column's row count is rounded
-// up to even (bulk sizes are multiples of 16 bytes); the row past n of an odd order is the
-// scratch matrix's padding row.  A quarter below the matrix copies nothing (the arrive alone
-// completes the barrier phase).
-__device__ void load_c_rows(const float2 *A, int n, int lda, int r0q, int c0, uint32_t dst, uint32_t bar) {
-    const int lane = threadIdx.x & 31;
-    const int rows = max(0, min(32, n - r0q)), rows_copy = (rows + 1) & ~1;
+// Row r0q + lane (this lane's row of one epilogue warp's quarter of a tile) of complex columns
+// c0 .. c0 + 31 into the warp's quarter of a C buffer (column-major, 128 rows) with cp.async, one
+// group per tile.  For a column the warp's 32 copies are 256 contiguous bytes; a lane reads back
+// only the row it copied, so its own wait_group is the whole handoff (no barrier, no proxy fence).
+__device__ __forceinline__ void load_c_row(const float2 *A, int n, int lda, int r0q, int c0, float2 *dst) {
+    const int lane = threadIdx.x & 31, gr = r0q + lane;
     const int cols = min(TNC, n - c0);
-    if (lane == 0) mbar_expect_tx(bar, (uint32_t)(rows_copy > 0 ? cols * rows_copy * 8 : 0));
-    __syncwarp();
-    if (rows_copy > 0 && lane < cols)
-        bulk_load(dst + (uint32_t)(lane * TM * 8), A + r0q + (int64_t)(c0 + lane) * lda, (uint32_t)(rows_copy * 8), bar);
+    if (gr < n)
+        for (int c = 0; c < cols; ++c) cp_async_elem(dst + lane + c * TM, A + gr + (int64_t)(c0 + c) * lda);
+    cp_async_commit();
 }
 
 // Schur update of rows and columns [j0 + 32, n) from the operand buffers (see the file header),
@@ -593,8 +588,9 @@ __device__ void load_c_rows(const float2 *A, int n, int lda, int r0q, int c0, ui
 //                 be free (bar_free of tile g - 2), issues tile g's MMAs into it and commits to
 //                 bar_mma; once tile g - 1's MMAs are done its ring slot takes tile g - 1 + STAGES;
 //   warps 4..7    (warp 4 + q owns TMEM lanes and tile rows 32 q .. +31) wait for bar_mma and their
-//                 C rows, subtract the accumulator from the old values and store the results to the
-//                 matrix, arrive on bar_free, and then load their rows of tile g + 2 into the buffer;
+//                 C rows (cp.async, two tiles ahead), subtract the accumulator from the old values
+//                 and store the results to the matrix, arrive on bar_free, and then load their rows
+//                 of tile g + 2 into the buffer;
 //   warps 1..3    wait at the closing barrier.
 __device__ __forceinline__ void schur_tc(float2 *A, int n, int lda, int j0, unsigned char *op, const unsigned char *abuf,
                          const unsigned char *bbuf, uint32_t tmem, const Bars &B, TcState &S, int *s_abort,
@@ -670,22 +666,23 @@ __device__ __forceinline__ void schur_tc(float2 *A, int n, int lda, int j0, unsi
         }
     } else if (warp >= EPI_WARP0) {
         const int q = warp - EPI_WARP0;
-        const uint32_t cb0 = opa + (uint32_t)OP_C;
-        const float2 *cs = reinterpret_cast<const float2 *>(op + OP_C);
-        int issued = 0;  // C loads of this warp (tiles g0 .. g0 + issued - 1)
+        float2 *cs = reinterpret_cast<float2 *>(op + OP_C);
+        auto cq = [&](int g) { return cs + (size_t)(g & 1) * (C_TILE / 8) + 32 * q; };
         bool ok = !aborted(s_abort);
-        for (int i = 0; i < 2 && i < T && ok; ++i, ++issued) {
-            const int g = g0 + i;
-            load_c_rows(A, n, lda, tile_r0(i) + 32 * q, tile_c0(i), cb0 + (uint32_t)((g & 1) * C_TILE + 32 * q * 8),
-                        B.c(g & 1, q));
+        // one cp.async group per tile, committed even when empty: before tile t's use exactly the
+        // group of tile t + 1 may still be pending
+        for (int i = 0; i < 2; ++i) {
+            if (i < T) load_c_row(A, n, lda, tile_r0(i) + 32 * q, tile_c0(i), cq(g0 + i));
+            else cp_async_commit();
         }
         for (int t = 0; t < T && ok; ++t) {
             const int g = g0 + t, b = g & 1;
             const uint32_t par = (uint32_t)(g >> 1) & 1u;
-            ok = !aborted(s_abort) && mbar_wait(B.mma(b), par) && mbar_wait(B.c(b, q), par);
+            ok = !aborted(s_abort) && mbar_wait(B.mma(b), par);
             ok = __all_sync(FULL_MASK, ok);
             if (!ok) break;
             tc_fence_after();
+            cp_async_wait<1>();
             const int row = 32 * q + lane, gr = tile_r0(t) + row, c0 = tile_c0(t);
             const uint32_t tb = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * TN);
             const float2 *cbuf = cs + (size_t)b * (C_TILE / 8);
@@ -706,23 +703,13 @@ __device__ __forceinline__ void schur_tc(float2 *A, int n, int lda, int j0, unsi
                 }
             }
             tc_fence_before();
-            fence_proxy_async();  // this warp's reads of its C rows before the next copy into them
             __syncwarp();
             if (lane == 0) mbar_arrive(B.free(b));
-            if (t + 2 < T) {
-                load_c_rows(A, n, lda, tile_r0(t + 2) + 32 * q, tile_c0(t + 2),
-                            cb0 + (uint32_t)(b * C_TILE + 32 * q * 8), B.c(b, q));
-                ++issued;
-            }
+            if (t + 2 < T) load_c_row(A, n, lda, tile_r0(t + 2) + 32 * q, tile_c0(t + 2), cq(g + 2));
+            else cp_async_commit();
         }
-        if (!ok) {
-            set_abort(s_abort, err_flag);
-            if (lane == 0)
-                for (int k = 1; k <= 2 && issued - k >= 0; ++k) {
-                    const int g = g0 + issued - k;
-                    mbar_wait(B.c(g & 1, q), (uint32_t)(g >> 1) & 1u);
-                }
-        }
+        cp_async_wait<0>();  // also after a timeout: no copy lands after the CTA moves on
+        if (!ok) set_abort(s_abort, err_flag);
     }
     __syncthreads();
     if (!aborted(s_abort)) S.g = g0 + T;  // after a timeout thread 0 keeps its count of issued tiles
@@ -998,7 +985,6 @@ __global__ void __launch_bounds__(NT, 1) sweep_tc_kernel(GlobalArgs a) {
         for (int b = 0; b < 2; ++b) {
             mbar_init(B.mma(b), 1);
             mbar_init(B.free(b), NW - EPI_WARP0);
-            for (int q = 0; q < 4; ++q) mbar_init(B.c(b, q), 1);
         }
         mbar_init(B.panel(), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
