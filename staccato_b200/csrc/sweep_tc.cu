@@ -89,11 +89,13 @@ static_assert(TN % 16 == 0 && TN >= 16 && TN <= 256, "N of an M = 128 MMA");
 static_assert(TMEM_COLS >= 32 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "TMEM allocations are powers of two >= 32");
 static_assert(OP_BYTES >= (512 | 1) * NB * 8, "the panel of an n = 512 system fits the operand region");
 
-// Byte offset of element (row, k) in one operand piece: K-major core matrices of 8 rows x 16
-// bytes (8 bf16), the K-adjacent ones 128 bytes apart (LBO), the 8-row groups 1024 bytes apart
-// (SBO = 8 core matrices of the 64-deep row).  A pieces have 128 rows, B pieces 64.
+// Byte offset of element (row, k) in one operand piece: K-major with the 128-byte swizzle.  A
+// row's 64 bf16 fill one 128-byte line, 8-row groups are 1024 bytes apart (SBO), and the 16-byte
+// chunk c of row r sits at chunk c ^ (r & 7) of its line, so that the tensor cores' reads of
+// eight rows at one K position fall in different shared-memory banks.  A pieces have 128 rows,
+// B pieces 64; every piece starts on a 1024-byte boundary (the swizzle uses address bits 4-9).
 __host__ __device__ constexpr int op_off(int row, int k) {
-    return (row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
+    return (row >> 3) * 1024 + (row & 7) * 128 + ((((k >> 3) ^ row) & 7) << 4) + (k & 7) * 2;
 }
 
 // Shared-memory layout (offsets from a 1024-byte aligned base).  The operand region holds the
@@ -202,11 +204,12 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Shared-memory matrix descriptor: no swizzle, K-major core matrices, LBO 128 B, SBO 1024 B,
-// descriptor version 1 (sm_100).
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle (layout type 2), SBO 1024 B (LBO
+// unused: a K step of 16 bf16 stays inside the 128-byte line), descriptor version 1 (sm_100),
+// base offset 0 (1024-byte aligned pieces).  The K steps of a piece start 32 bytes apart.
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
-           (1ull << 46);
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
@@ -643,8 +646,8 @@ __device__ __forceinline__ void schur_tc(float2 *A, int n, int lda, int j0, unsi
             for (int p = 0; p < NPROD; ++p)
 #pragma unroll
                 for (int ks = 0; ks < KSTEPS; ++ks) {
-                    const uint64_t ad = sdesc(opa + (uint32_t)(PA[p] * A_PIECE + ks * 256));
-                    const uint64_t bd = sdesc(bsl + (uint32_t)(PB[p] * B_PIECE + ks * 256));
+                    const uint64_t ad = sdesc(opa + (uint32_t)(PA[p] * A_PIECE + ks * 32));
+                    const uint64_t bd = sdesc(bsl + (uint32_t)(PB[p] * B_PIECE + ks * 32));
                     mma_bf16(d, ad, bd, (uint32_t)(p | ks));
                 }
             mma_commit(B.mma(g & 1));
