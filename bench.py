@@ -118,14 +118,23 @@ class ClockSampler:
 
 # ----------------------------------------------------------------------------- peaks
 
-# DRAM bytes (read + write) per launch of the dominant kernels on this bench's default
-# workload (the 64-ROM batching draw of rank 0), from a one-pass ncu capture of
-# dram__bytes_read.sum + dram__bytes_write.sum over
-# `bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-e2e --no-extras` (mean of 4 launches).
-MEASURED_TRAFFIC = {"mixed_global": 574.5e9 + 460.1e9, "fp64_global": 1757.4e9 + 1803.5e9}
+# DRAM bytes (read + write) per launch of the dominant kernel of a form on this bench's default
+# workload (the 64-ROM batching draw of rank 0), keyed by (form, kernel).  The CUDA-core and FP64
+# global kernels: a one-pass ncu capture of dram__bytes_read.sum + dram__bytes_write.sum over
+# `bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-e2e --no-extras` (mean of 4 launches;
+# the CUDA-core kernel then took every system of the mixed form, as it does in mixed_fp32).
+MEASURED_TRAFFIC = {("mixed_fp32", "mixed_global"): 574.5e9 + 460.1e9, ("fp64", "fp64_global"): 1757.4e9 + 1803.5e9}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, one-pass capture of this "
-                  "workload with the current kernels; compare with the bytes the matrices alone need "
-                  "(8 n^2 B per FP32 system, 16 n^2 B per FP64 system)")
+                  "workload; compare with the bytes the matrices alone need (8 n^2 B per FP32 system, "
+                  "16 n^2 B per FP64 system)")
+# The tensor-core kernel of the headline (SROM_MIXED_AUTO) sweep: the same metrics captured on a
+# small case, every 16th frequency of every ROM of the same batch (same n / r mix, autotuned the
+# same way; one launch of 5,271 systems and 0.717 TFLOP), scaled to a full launch by its flops.
+TC_SAMPLE_BYTES = 42724239616 + 42177227776
+TC_SAMPLE_FLOPS = 716926045381.0
+TC_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the tensor-core launch on every 16th "
+                     "frequency of the same batch (84.9 GB for 0.717 TFLOP), scaled to this launch by its flops; "
+                     "compare with 8 n^2 B per FP32 system")
 
 
 # DRAM bytes (read + write) of one projection of the Tet10 block (K and M, k = 96): transpose,
@@ -681,9 +690,12 @@ def run_ours(args):
         kms, kitems, kfl, kl = per[dom]
         achieved = kfl / (kms * 1e-3) / 1e12
         tot = sum(x[0] for x in per.values())
+        traffic, tsource = MEASURED_TRAFFIC.get((form, dom)), TRAFFIC_SOURCE
+        if form == "mixed" and dom == "mixed_tc" and kl > 0:
+            traffic, tsource = TC_SAMPLE_BYTES * (kfl / kl) / TC_SAMPLE_FLOPS, TC_TRAFFIC_SOURCE
         return {"bound": "tensor", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": MEASURED_TRAFFIC.get(dom),
-                "traffic_source": TRAFFIC_SOURCE, "kernel": dom,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                "traffic_source": tsource, "kernel": dom,
                 "peak_source": peak_source,
                 "algorithmic": "8/3 n^3 + 8 n^2 r real flops per system (LU + solve, both forms)",
                 "kernels": {k: {"ms_per_launch": v[0] / v[3], "launches": v[3],
