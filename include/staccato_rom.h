@@ -326,6 +326,21 @@ SROM_API int srom_band_pivot_report(const srom_handle *h, int64_t *factorisation
                                     double *min_pivot_ratio);
 
 /*
+ * The handle keeps the full symmetric pattern and reverse Cuthill-McKee order of its last
+ * srom_krylov_basis / srom_fom_sweep call on the device (about 12 bytes per stored entry and
+ * 12 per row), and a later call whose pattern is the same (sizes, base, storage and a 64-bit hash
+ * of rowptr and colind) reuses them instead of symmetrising, ordering and uploading again; a
+ * different pattern replaces them.  The reference instead repeats PARDISO's analysis (phase 11)
+ * before every factorisation (src/analysis/KrylovROMSubstructure.cpp:647, per expansion point
+ * at :408 and per frequency of the full-order sweep at :1380).
+ * srom_band_cache_report: reused = 1 if the last such call found its pattern in the cache;
+ * cached_rows / bandwidth describe the cached pattern (0 when none).  Any pointer may be NULL.
+ * srom_band_cache_release: frees the cached pattern's device memory (synchronises the stream).
+ */
+SROM_API int srom_band_cache_report(const srom_handle *h, int *reused, int64_t *cached_rows, int64_t *bandwidth);
+SROM_API int srom_band_cache_release(srom_handle *h);
+
+/*
  * Host-only: the reverse Cuthill-McKee ordering srom_krylov_basis uses for a pattern (HOST
  * rowptr/colind, as above).  perm (n_rows ints, may be NULL): perm[k] = original row of row k;
  * *bandwidth = max |new i - new j| over the entries; *band_bytes = device bytes of the band

@@ -39,6 +39,7 @@ EXPORTS = [
     "srom_graph_create", "srom_graph_launch", "srom_graph_destroy", "srom_tune",
     "srom_mtx_read_dense", "srom_mtx_write_dense", "srom_write_solution",
     "srom_krylov_basis", "srom_band_order", "srom_fom_sweep", "srom_zgemm_batched", "srom_band_pivot_report",
+    "srom_band_cache_report", "srom_band_cache_release",
 ]
 
 SROM_OP_N = 0
@@ -133,6 +134,10 @@ def lib() -> C.CDLL:
         L.srom_zgemm_batched.restype = i
         L.srom_band_pivot_report.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_double)]
         L.srom_band_pivot_report.restype = i
+        L.srom_band_cache_report.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.srom_band_cache_report.restype = i
+        L.srom_band_cache_release.argtypes = [vp]
+        L.srom_band_cache_release.restype = i
         L.srom_orthonormalize.argtypes = [vp, vp, C.c_int64, i, C.c_int64, i]
         L.srom_orthonormalize.restype = i
         L.srom_graph_create.argtypes = [vp, C.POINTER(RomDesc), i, C.POINTER(SweepOpts), pp]

@@ -55,6 +55,8 @@ struct srom_handle {
     size_t d_zwork_bytes = 0;
     // pivots of the band factorisations of the last srom_krylov_basis / srom_fom_sweep call
     srom::kry::PivotStats band_stats;
+    // full pattern and RCM order of the last band factorisation, reused by a call on the same pattern
+    srom::kry::PatternCache band_cache;
     // per-launch profiling
     struct ProfRec {
         std::string name;
@@ -303,6 +305,7 @@ int srom_destroy(srom_handle *h) {
     if (h->d_adj) cudaFree(h->d_adj);
     if (h->d_zero) cudaFree(h->d_zero);
     if (h->d_zwork) cudaFree(h->d_zwork);
+    h->band_cache.release();
     if (h->h_meta) cudaFreeHost(h->h_meta);
     if (h->h_flag) cudaFreeHost(h->h_flag);
     if (h->meta_done) cudaEventDestroy(h->meta_done);
@@ -828,6 +831,23 @@ int srom_band_pivot_report(const srom_handle *h, int64_t *factorisations, int64_
     return SROM_OK;
 }
 
+int srom_band_cache_report(const srom_handle *h, int *reused, int64_t *cached_rows, int64_t *bandwidth) {
+    if (!h) return SROM_ERR_INVALID;
+    const srom::kry::PatternCache &c = h->band_cache;
+    if (reused) *reused = c.last_reused ? 1 : 0;
+    if (cached_rows) *cached_rows = c.d_frp ? c.n : 0;
+    if (bandwidth) *bandwidth = c.d_frp ? c.bw : 0;
+    return SROM_OK;
+}
+
+int srom_band_cache_release(srom_handle *h) {
+    if (!h) return SROM_ERR_INVALID;
+    DeviceGuard g(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->band_cache.release();
+    return SROM_OK;
+}
+
 int srom_zgemm_batched(srom_handle *h, int opa, int opb, int m, int n, int k, srom_complex alpha, const srom_complex *A,
                        int64_t lda, int64_t stride_a, const srom_complex *B, int64_t ldb, int64_t stride_b,
                        srom_complex beta, srom_complex *C, int64_t ldc, int64_t stride_c, int batch) {
@@ -1136,6 +1156,8 @@ int srom_krylov_basis(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t
     a.max_cols = max_cols;
     h->band_stats = srom::kry::PivotStats{};
     a.stats = &h->band_stats;
+    a.cache = &h->band_cache;
+    h->band_cache.last_reused = false;
     std::string msg;
     ProfScope ps(h, "krylov_basis", n_points, 0.0, 0.0);
     const int s = srom::kry::krylov_basis(a, &msg, n_cols, nullptr);
@@ -1182,6 +1204,8 @@ int srom_fom_sweep(srom_handle *h, int64_t n_rows, int64_t nnz, const int64_t *r
     a.ldx = ldx;
     h->band_stats = srom::kry::PivotStats{};
     a.stats = &h->band_stats;
+    a.cache = &h->band_cache;
+    h->band_cache.last_reused = false;
     std::string msg;
     ProfScope ps(h, "fom_sweep", n_freq, 0.0, 0.0);
     const int s = srom::kry::fom_sweep(a, &msg);

@@ -787,7 +787,38 @@ int pivoted_qr(cudaStream_t st, double2 *A, int64_t n, int m, double tol, double
 
 }  // namespace
 
+void PatternCache::release() {
+    if (d_frp) cudaFree(d_frp);
+    if (d_fci) cudaFree(d_fci);
+    if (d_fmap) cudaFree(d_fmap);
+    if (d_iperm) cudaFree(d_iperm);
+    d_frp = d_fmap = nullptr;
+    d_fci = d_iperm = nullptr;
+    n = nnz = -1;
+    base = upper = -1;
+    hash = 0;
+    bw = nfull = 0;
+    last_reused = false;
+}
+
 namespace {
+
+// 64-bit hash of a CSR pattern (rowptr words, then colind in pairs): a multiply-xorshift step per
+// 64-bit word.  Equal patterns give equal hashes; the cache also compares the sizes, base and
+// storage.
+uint64_t pattern_hash(const std::vector<int64_t> &rp, const std::vector<int> &ci) {
+    uint64_t h = 0x243F6A8885A308D3ull;
+    auto step = [&](uint64_t w) {
+        h = (h ^ w) * 0xBF58476D1CE4E5B9ull;
+        h ^= h >> 29;
+    };
+    for (int64_t v : rp) step((uint64_t)v);
+    size_t i = 0;
+    for (; i + 1 < ci.size(); i += 2) step((uint64_t)(uint32_t)ci[i] | ((uint64_t)(uint32_t)ci[i + 1] << 32));
+    if (i < ci.size()) step((uint64_t)(uint32_t)ci[i] | (1ull << 63));
+    step((uint64_t)ci.size());
+    return h;
+}
 
 // The factorisation context shared by the Krylov basis and the full-order sweep: the pattern
 // (full symmetric, on host and device), its RCM order, the band factor and its panels, and the
@@ -804,8 +835,10 @@ struct BandContext {
     double *d_nrm = nullptr;
     BandLDLT F;
 
+    // The pattern's full symmetric form and RCM order: from the handle's cache when it holds
+    // this pattern, else computed on the host and uploaded (into the cache when there is one).
     int init(cudaStream_t stream, int64_t n_rows, int64_t nnz, const int64_t *rowptr, const int *colind, int base,
-             int upper, Err &E) {
+             int upper, PatternCache *cache, Err &E) {
         st = stream;
         n = n_rows;
         B.st = st;
@@ -816,12 +849,22 @@ struct BandContext {
         KCU(cudaStreamSynchronize(st));
         if (rp[0] != base || rp[n] - base != nnz)
             return E.set(SROM_ERR_INVALID, "rowptr does not start at base or does not end at base + nnz");
-        std::string err;
-        int s = full_pattern(n, nnz, rp.data(), ci.data(), base, upper, frp, fci, fmap, &err);
-        if (s) return E.set(s, err);
-        const int64_t bw = rcm_order(n, frp, fci, perm);
-        iperm.assign(n, 0);
-        for (int64_t k = 0; k < n; ++k) iperm[perm[k]] = (int)k;
+        const uint64_t hsh = pattern_hash(rp, ci);
+        const bool reuse = cache && cache->matches(n, nnz, base, upper, hsh);
+        int64_t bw = 0, nfull = 0;
+        if (reuse) {
+            bw = cache->bw;
+            nfull = cache->nfull;
+        } else {
+            std::string err;
+            int s = full_pattern(n, nnz, rp.data(), ci.data(), base, upper, frp, fci, fmap, &err);
+            if (s) return E.set(s, err);
+            bw = rcm_order(n, frp, fci, perm);
+            iperm.assign(n, 0);
+            for (int64_t k = 0; k < n; ++k) iperm[perm[k]] = (int)k;
+            nfull = frp[n];
+        }
+        if (cache) cache->last_reused = reuse;
         F.n = n;
         F.bw = bw;
         F.ldab = bw + 2 * NB + 1;
@@ -836,10 +879,40 @@ struct BandContext {
         };
         if (!need(B.alloc(&F.band, (size_t)(n + 2 * NB) * F.ldab), "the band factor") ||
             !need(B.alloc(&F.W, (size_t)F.ldw * NB), "the panel") ||
-            !need(B.alloc(&F.Lp, (size_t)F.ldw * NB), "the panel") || !need(B.alloc(&F.d_info, 1), "info") ||
-            !need(B.alloc(&d_frp, n + 1), "the pattern") || !need(B.alloc(&d_fci, frp[n]), "the pattern") ||
-            !need(B.alloc(&d_fmap, frp[n]), "the pattern") || !need(B.alloc(&d_iperm, n), "the ordering"))
+            !need(B.alloc(&F.Lp, (size_t)F.ldw * NB), "the panel") || !need(B.alloc(&F.d_info, 1), "info"))
             return E.code;
+        if (reuse) {
+            d_frp = cache->d_frp;
+            d_fci = cache->d_fci;
+            d_fmap = cache->d_fmap;
+            d_iperm = cache->d_iperm;
+        } else if (cache) {
+            // a different pattern replaces the cached one (the previous call has drained the stream)
+            cache->release();
+            auto dev = [&](void **p, size_t bytes, const char *what) {
+                const cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 1));
+                if (e != cudaSuccess) {
+                    *p = nullptr;
+                    E.set(e == cudaErrorMemoryAllocation ? SROM_ERR_ALLOC : SROM_ERR_CUDA,
+                          std::string("allocating ") + what + ": " + cudaGetErrorString(e));
+                }
+                return e == cudaSuccess;
+            };
+            if (!dev(reinterpret_cast<void **>(&cache->d_frp), sizeof(int64_t) * (n + 1), "the pattern") ||
+                !dev(reinterpret_cast<void **>(&cache->d_fci), sizeof(int) * nfull, "the pattern") ||
+                !dev(reinterpret_cast<void **>(&cache->d_fmap), sizeof(int64_t) * nfull, "the pattern") ||
+                !dev(reinterpret_cast<void **>(&cache->d_iperm), sizeof(int) * n, "the ordering")) {
+                cache->release();
+                return E.code;
+            }
+            d_frp = cache->d_frp;
+            d_fci = cache->d_fci;
+            d_fmap = cache->d_fmap;
+            d_iperm = cache->d_iperm;
+        } else if (!need(B.alloc(&d_frp, n + 1), "the pattern") || !need(B.alloc(&d_fci, nfull), "the pattern") ||
+                   !need(B.alloc(&d_fmap, nfull), "the pattern") || !need(B.alloc(&d_iperm, n), "the ordering")) {
+            return E.code;
+        }
         {
             int dev = 0;
             KCU(cudaGetDevice(&dev));
@@ -857,10 +930,21 @@ struct BandContext {
         KCU(cudaFuncSetAttribute(ldlt_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(smem + sizeof(double2) * NB)));
         KCU(cudaFuncSetAttribute(trsv_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        KCU(cudaMemcpyAsync(d_frp, frp.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
-        KCU(cudaMemcpyAsync(d_fci, fci.data(), sizeof(int) * frp[n], cudaMemcpyHostToDevice, st));
-        KCU(cudaMemcpyAsync(d_fmap, fmap.data(), sizeof(int64_t) * frp[n], cudaMemcpyHostToDevice, st));
-        KCU(cudaMemcpyAsync(d_iperm, iperm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+        if (!reuse) {
+            KCU(cudaMemcpyAsync(d_frp, frp.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
+            KCU(cudaMemcpyAsync(d_fci, fci.data(), sizeof(int) * nfull, cudaMemcpyHostToDevice, st));
+            KCU(cudaMemcpyAsync(d_fmap, fmap.data(), sizeof(int64_t) * nfull, cudaMemcpyHostToDevice, st));
+            KCU(cudaMemcpyAsync(d_iperm, iperm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+            if (cache) {
+                cache->n = n;
+                cache->nnz = nnz;
+                cache->base = base;
+                cache->upper = upper;
+                cache->hash = hsh;
+                cache->bw = bw;
+                cache->nfull = nfull;
+            }
+        }
         KCU(cudaMemsetAsync(F.W, 0, sizeof(double2) * F.ldw * NB, st));
         KCU(cudaMemsetAsync(F.Lp, 0, sizeof(double2) * F.ldw * NB, st));
         return SROM_OK;
@@ -896,7 +980,7 @@ int krylov_basis(const KrylovArgs &a, std::string *msg, int *n_cols, KrylovLog *
     if (log) log->blocks.clear();
     if (a.n_rows == 0 || a.n_in == 0 || a.n_points == 0) return SROM_OK;
     BandContext X;
-    if (X.init(a.stream, a.n_rows, a.nnz, a.rowptr, a.colind, a.base, a.upper, E)) {
+    if (X.init(a.stream, a.n_rows, a.nnz, a.rowptr, a.colind, a.base, a.upper, a.cache, E)) {
         *msg = E.msg;
         return E.code;
     }
@@ -965,7 +1049,7 @@ int fom_sweep(const FomArgs &a, std::string *msg) {
     Err E;
     if (a.n_rows == 0 || a.r == 0 || a.n_freq == 0) return SROM_OK;
     BandContext X;
-    if (X.init(a.stream, a.n_rows, a.nnz, a.rowptr, a.colind, a.base, a.upper, E)) {
+    if (X.init(a.stream, a.n_rows, a.nnz, a.rowptr, a.colind, a.base, a.upper, a.cache, E)) {
         *msg = E.msg;
         return E.code;
     }

@@ -18,6 +18,28 @@ struct PivotStats {
     double min_pivot_ratio = 1.0 / 0.0;
 };
 
+// The full symmetric pattern of the last band factorisation on a handle and its RCM order, on
+// the device, kept between calls: a call whose pattern matches (sizes, base, storage and a 64-bit
+// hash of rowptr and colind) skips the symmetrisation, the ordering and their uploads.  (The
+// reference redoes PARDISO's analysis, phase 11, before every factorisation:
+// src/analysis/KrylovROMSubstructure.cpp:647, per expansion point at :408 and per frequency of
+// the full-order sweep at :1380.)
+struct PatternCache {
+    int64_t n = -1, nnz = -1;
+    int base = -1, upper = -1;
+    uint64_t hash = 0;
+    int64_t bw = 0;
+    int64_t nfull = 0;  // entries of the full pattern
+    int64_t *d_frp = nullptr, *d_fmap = nullptr;
+    int *d_fci = nullptr, *d_iperm = nullptr;
+    bool last_reused = false;  // the last call found its pattern here
+    bool matches(int64_t n_, int64_t nnz_, int base_, int upper_, uint64_t hash_) const {
+        return d_frp && n == n_ && nnz == nnz_ && base == base_ && upper == upper_ && hash == hash_;
+    }
+    // frees the device arrays (after the caller's stream has drained) and forgets the key
+    void release();
+};
+
 struct KrylovArgs {
     cudaStream_t stream;
     int64_t n_rows, nnz;
@@ -34,7 +56,8 @@ struct KrylovArgs {
     void *V;  // device n_rows x max_cols output, leading dimension ldv
     int64_t ldv;
     int max_cols;
-    PivotStats *stats;  // may be null
+    PivotStats *stats;     // may be null
+    PatternCache *cache;   // may be null (no reuse between calls)
 };
 
 struct KrylovBlock {
@@ -64,7 +87,8 @@ struct FomArgs {
     int n_freq;
     void *X;  // device: n_freq blocks of n_rows x r (leading dimension ldx, block stride ldx * r)
     int64_t ldx;
-    PivotStats *stats;  // may be null
+    PivotStats *stats;     // may be null
+    PatternCache *cache;   // may be null (no reuse between calls)
 };
 
 // (K - w^2 M + i w D) X_f = F for every frequency: band LDL^T per frequency.

@@ -77,6 +77,20 @@ def band_pivot_report(handle: _capi.Handle):
     return int(nf.value), int(npert.value), float(mr.value)
 
 
+def band_cache_report(handle: _capi.Handle):
+    """(reused, cached_rows, bandwidth): whether the handle's last krylov_basis / fom_sweep call
+    reused the cached full pattern and RCM order of an earlier call on the same pattern, and the
+    size of the cached pattern (``srom_band_cache_report``)."""
+    ru, rows, bw = C.c_int(0), C.c_int64(0), C.c_int64(0)
+    check(handle.ptr, _capi.lib().srom_band_cache_report(handle.ptr, C.byref(ru), C.byref(rows), C.byref(bw)))
+    return bool(ru.value), int(rows.value), int(bw.value)
+
+
+def band_cache_release(handle: _capi.Handle) -> None:
+    """Free the handle's cached band pattern (``srom_band_cache_release``)."""
+    check(handle.ptr, _capi.lib().srom_band_cache_release(handle.ptr))
+
+
 def band_order(indptr, indices, base: int = 0, upper: bool = False):
     """(perm, bandwidth, band_bytes) of the reverse Cuthill-McKee ordering of a host CSR pattern:
     perm[k] = original row of row k."""

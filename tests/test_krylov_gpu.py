@@ -258,3 +258,59 @@ def test_band_small_pivot_perturbed_like_pardiso(handle):
     fom_sweep(handle, csr, Kv, torch.zeros_like(Kv), None, F, [10.0])
     nf, npert, ratio = band_pivot_report(handle)
     assert nf == 1 and npert == 0 and 0.0 < ratio <= 1.0
+
+
+def test_pattern_cache_reuse_is_exact(problem):
+    """A second call on the same pattern reuses the handle's cached full pattern and RCM order
+    (srom_band_cache_report) and gives bit-identical results, the full-order sweep included; a
+    different pattern of the same sizes replaces the cache and gives what a fresh handle gives;
+    srom_band_cache_release frees it."""
+    import torch
+
+    from staccato_b200.krylov import band_cache_release, band_cache_report, fom_sweep
+
+    K, M, D, f1 = problem
+    N = K.shape[0]
+    B = _inputs(N, seed=7)
+    pts = [0.5 * f1, 2.0 * f1]
+    rng = np.random.default_rng(8)
+    F = rng.standard_normal((N, 2)) + 1j * rng.standard_normal((N, 2))
+    freqs = [0.4 * f1, 1.3 * f1]
+
+    def fom(h, K_, M_, D_):
+        csr = DeviceCsr.from_host(K_.indptr, K_.indices)
+        X = fom_sweep(h, csr, _dev(torch, K_.data), _dev(torch, M_.data), _dev(torch, D_.data), _dev(torch, F.T), freqs)
+        torch.cuda.synchronize()
+        return X.cpu().numpy()
+
+    h, fresh = _capi.Handle(0), _capi.Handle(0)
+    try:
+        assert band_cache_report(h) == (False, 0, 0)
+        V1 = _run(h, K, M, D, B, pts, 2)
+        reused, rows, bw = band_cache_report(h)
+        assert not reused and rows == N and bw > 0
+        V2 = _run(h, K, M, D, B, pts, 2)
+        assert band_cache_report(h) == (True, N, bw)
+        assert np.array_equal(V1, V2)
+        X1 = fom(h, K, M, D)
+        assert band_cache_report(h)[0]
+        assert np.array_equal(X1, fom(fresh, K, M, D))
+        # the same sizes, another pattern: a symmetric permutation of the matrices
+        p = rng.permutation(N)
+        Kp, Mp, Dp = (A[p][:, p].tocsr() for A in (K, M, D))
+        for A in (Kp, Mp, Dp):
+            A.sort_indices()
+        assert np.array_equal(Mp.indices, Kp.indices) and np.array_equal(Dp.indices, Kp.indices)
+        assert Kp.nnz == K.nnz and not np.array_equal(Kp.indices, K.indices)
+        Xp = fom(h, Kp, Mp, Dp)
+        assert not band_cache_report(h)[0]
+        band_cache_release(fresh)
+        assert np.array_equal(Xp, fom(fresh, Kp, Mp, Dp))
+        assert not band_cache_report(fresh)[0]
+        band_cache_release(h)
+        assert band_cache_report(h) == (False, 0, 0)
+        V3 = _run(h, K, M, D, B, pts, 2)
+        assert not band_cache_report(h)[0] and np.array_equal(V1, V3)
+    finally:
+        h.close()
+        fresh.close()
