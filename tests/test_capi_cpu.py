@@ -17,7 +17,8 @@ def _declared():
     names = []
     for f in sorted(os.listdir(HDR_DIR)):
         if f.endswith(".h"):
-            txt = open(os.path.join(HDR_DIR, f)).read()
+            with open(os.path.join(HDR_DIR, f)) as fh:
+                txt = fh.read()
             names += re.findall(r"SROM_API\s+[\w\s\*]+?\b(srom_\w+)\s*\(", txt)
     return names
 
@@ -53,7 +54,8 @@ int main(void) {
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "t.c")
         exe = os.path.join(d, "t")
-        open(c, "w").write(src)
+        with open(c, "w") as fh:
+            fh.write(src)
         subprocess.run(["gcc", "-I", HDR_DIR, c, "-o", exe], check=True)
         got = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
     R, S = _capi.RomDesc, _capi.SweepOpts

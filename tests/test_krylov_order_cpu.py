@@ -11,8 +11,8 @@ from staccato_b200.krylov import band_order
 
 
 def _grid(nx, ny, seed=None):
-    A = sp.kron(sp.eye(ny), sp.diags([1, 4, 1], [-1, 0, 1], shape=(nx, nx))) + sp.kron(
-        sp.diags([1, 1], [-1, 1], shape=(ny, ny)), sp.eye(nx))
+    A = sp.kron(sp.eye(ny), sp.diags([1.0, 4.0, 1.0], [-1, 0, 1], shape=(nx, nx))) + sp.kron(
+        sp.diags([1.0, 1.0], [-1, 1], shape=(ny, ny)), sp.eye(nx))
     A = sp.csr_matrix(A)
     if seed is not None:
         p = np.random.default_rng(seed).permutation(A.shape[0])
